@@ -1,0 +1,174 @@
+/*
+ * esrrf.h -- C ABI of libesrrf, a B200 (sm_100a) engine for the eSRRF hot path of
+ * NanoJ-eSRRF: Fourier interpolation of each frame, gradient field, radial gradient
+ * convergence (RGC) with Gaussian distance weighting and a sensitivity exponent, intensity
+ * weighting, and AVG/VAR/TAC2 temporal cumulants over frame blocks, in 2-D and 3-D.
+ *
+ * The entry points replace the members of the reference's device-engine class
+ * nanoj.liveSRRF.LiveSRRF_CL (src/nanoj/liveSRRF/LiveSRRF_CL.java); each declaration cites
+ * the member it replaces.  Conventions:
+ *   - plain pointers and sizes only; images are row-major float32 or uint16, frames contiguous;
+ *   - every call returns an esrrf_status; esrrf_last_error() gives the message of the last
+ *     failure on a handle (the reference logs and carries on, or throws RuntimeException on
+ *     device-initialisation failure, LiveSRRF_CL.java:115-119);
+ *   - one handle owns one CUDA stream and its device buffers; handles are independent (the
+ *     reference keeps its OpenCL context in static fields, LiveSRRF_CL.java:70-88, so it has
+ *     one engine per JVM); calls on one handle must not overlap, except
+ *     esrrf_request_cancel(), which is thread-safe;
+ *   - host buffers may be pageable or pinned; the *_device variants take device pointers.
+ */
+#ifndef ESRRF_H
+#define ESRRF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ESRRF_VERSION_MAJOR 0
+#define ESRRF_VERSION_MINOR 1
+
+typedef enum {
+    ESRRF_OK = 0,
+    ESRRF_CANCELLED = 1,       /* calculateSRRF returned true (user pressed Escape) */
+    ESRRF_ERR_INVALID = -1,    /* bad argument or inconsistent parameters */
+    ESRRF_ERR_CUDA = -2,       /* a CUDA runtime call failed; see esrrf_last_error() */
+    ESRRF_ERR_NOMEM = -3,      /* device or pinned-host allocation failed */
+    ESRRF_ERR_STATE = -4,      /* call out of order (e.g. frames pushed past the block) */
+    ESRRF_ERR_TIMEOUT = -5,    /* a bounded device wait gave up */
+    ESRRF_ERR_NODEVICE = -6    /* no CUDA device */
+} esrrf_status;
+
+/* Interpolation mode of the 2-D path (LiveSRRF_CL.java:159-264): FHT loads
+ * liveSRRF_noInterpolation.cl on Fourier-interpolated frames, BIC loads liveSRRF.cl. */
+typedef enum { ESRRF_INTERP_FHT = 0, ESRRF_INTERP_BIC = 1 } esrrf_interp;
+
+/* Scale of the inverse Hartley transform in the Fourier interpolation.  The reference's
+ * transform (nanoj.core2.NanoJFHT, not vendored) does not say which it uses. */
+typedef enum {
+    ESRRF_FHT_SCALE_MEAN_PRESERVING = 0, /* interpolated mean equals the raw mean */
+    ESRRF_FHT_SCALE_UNITARY_BIG = 1      /* inverse scaled by 1/(N*M)^2: mean divided by M^2 */
+} esrrf_fht_scale;
+
+/* Parameters of LiveSRRF_CL.initialise (LiveSRRF_CL.java:159) as a POD struct.
+ * width/height: raw frame size (3-D: the full MFM camera frame, split 3x3 into planes).
+ * fwhm: the GUI's "Radius" (sigma = fwhm / 2.354).  n_frames_on_gpu: frames per push.
+ * n_frame_for_srrf: frames per SR block.  block_length: accepted for API fidelity; the CUDA
+ * kernels do not need the reference's 1-D work splitting (LiveSRRF_CL.java:707-742).
+ * 3-D (n_planes > 0): per-plane calibration of the .njt table the reference loads
+ * (LiveSRRF_CL.java:210-227): roi index, theta (degrees), x/y shift, intensity scaling,
+ * background; axial_offset_nm and pixel_size_um give the (unused by the kernel) dimRatio. */
+typedef struct {
+    int width, height;
+    int magnification;
+    float fwhm;
+    int sensitivity;
+    int n_frames_on_gpu;
+    int n_frame_for_srrf;
+    int block_length;
+    int device;           /* CUDA ordinal; -1 = the device with most SMs x clock */
+    int int_weighting;    /* 1: weight CGLH by the interpolated intensity */
+    int mp_correction;    /* 1: macro-pixel correction (BIC and 3-D paths only, as in the reference) */
+    int interp;           /* esrrf_interp; forced to BIC in 3-D (LiveSRRF_CL.java:166-168) */
+    int fht_scale;        /* esrrf_fht_scale */
+    int kernel;           /* 0: fused tile kernel where applicable, 1: plain per-pixel kernel */
+    int frames_per_launch;/* frames interpolated and reduced per fused launch; 0 = autotuned */
+    /* 3-D calibration, all arrays of length n_planes (NULL in 2-D). */
+    int n_planes;
+    const float* roi;
+    const float* theta_deg;
+    const float* shift_x;
+    const float* shift_y;
+    const float* intensity_coeff;
+    float background;
+    float axial_offset_nm;
+    float pixel_size_um;
+} esrrf_params;
+
+typedef struct esrrf_handle esrrf_handle;
+
+/* Library version "major.minor". */
+const char* esrrf_get_version(void);
+
+/* Number of CUDA devices; replaces the platform scan of LiveSRRF_CL.checkDevices
+ * (LiveSRRF_CL.java:111-155). */
+esrrf_status esrrf_device_count(int* count);
+
+/* Name, SM count and max clock (MHz) of one device (checkDevices' per-device log). */
+esrrf_status esrrf_device_info(int device, char* name, size_t name_len, int* sm_count,
+                               int* clock_mhz);
+
+/* Fill *p with the reference GUI defaults (LiveSRRF_optimised_.java:128-134): M 5,
+ * radius 2, sensitivity 1, 100 frames/block, 20000 block length, FHT on, intensity weighting
+ * on, MP correction off. */
+void esrrf_default_params(esrrf_params* p);
+
+/* Replaces LiveSRRF_CL.initialise (LiveSRRF_CL.java:159-264) and its buffer/program set-up
+ * (prepareBuffersFHTinterpolation :462-579, prepareBuffersBICinterpolation :266-459). */
+esrrf_status esrrf_create(const esrrf_params* params, esrrf_handle** out);
+
+/* Replaces LiveSRRF_CL.release (LiveSRRF_CL.java:939-951). */
+esrrf_status esrrf_destroy(esrrf_handle* h);
+
+/* Replaces LiveSRRF_CL.loadDriftXYGPUbuffer (LiveSRRF_CL.java:583-595): per-frame drift of
+ * the current block in raw pixels, n = n_frame_for_srrf values each (NULL = zero drift). */
+esrrf_status esrrf_set_drift(esrrf_handle* h, const float* drift_x, const float* drift_y, int n);
+
+/* Replaces LiveSRRF_CL.resetFramePosition (LiveSRRF_CL.java:955-960): starts a new block. */
+esrrf_status esrrf_reset_frame_position(esrrf_handle* h);
+
+/* Replaces LiveSRRF_CL.calculateSRRF (LiveSRRF_CL.java:636-746): accumulates n_frames
+ * consecutive frames (host memory, [n][height][width]) into the current block.  Returns
+ * ESRRF_CANCELLED if esrrf_request_cancel() was called. */
+esrrf_status esrrf_calculate_srrf_u16(esrrf_handle* h, const uint16_t* frames, int n_frames);
+esrrf_status esrrf_calculate_srrf_f32(esrrf_handle* h, const float* frames, int n_frames);
+/* Same, frames already in device memory of the handle's device. */
+esrrf_status esrrf_calculate_srrf_u16_device(esrrf_handle* h, const uint16_t* d_frames,
+                                             int n_frames);
+esrrf_status esrrf_calculate_srrf_f32_device(esrrf_handle* h, const float* d_frames,
+                                             int n_frames);
+
+/* Replaces LiveSRRF_CL.readSRRFbuffer (LiveSRRF_CL.java:749-794): finalises VAR/TAC2 (and the
+ * MP correction on the BIC/3-D paths) and copies [4][planesM][heightM][widthM] float slices,
+ * in the order AVG, VAR, TAC2, INT, NaN replaced by 0, to host memory `out`. */
+esrrf_status esrrf_read_srrf(esrrf_handle* h, float* out);
+/* Same into device memory. */
+esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* d_out);
+
+/* Output geometry (public fields widthS/heightS/nPlanes/nPlanesM, LiveSRRF_CL.java:41-45). */
+esrrf_status esrrf_output_shape(const esrrf_handle* h, int* width_m, int* height_m,
+                                int* planes_m);
+
+/* Replaces readGradientBuffers (LiveSRRF_CL.java:797-879): gradient components of the first
+ * frame of the last push ([2 or 3][planes][h'][w'] float, h'/w' as in the reference). */
+esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len);
+
+/* Replaces finishQueue (LiveSRRF_CL.java:1009-1015): waits for the handle's stream. */
+esrrf_status esrrf_finish_queue(esrrf_handle* h);
+
+/* Thread-safe cancellation (replaces the IJ.escapePressed() polling, LiveSRRF_CL.java:731-734). */
+esrrf_status esrrf_request_cancel(esrrf_handle* h);
+
+/* Message of the last failure on h (or of the last failed esrrf_create when h is NULL). */
+const char* esrrf_last_error(const esrrf_handle* h);
+
+/* Runs the handle's kernels on a caller-owned CUDA stream (cudaStream_t passed as void*; NULL
+ * restores a private stream).  Calls still return only when their work on it is done. */
+esrrf_status esrrf_set_stream(esrrf_handle* h, void* stream);
+
+/* Enables per-launch CUDA-event timing of the interpolation and RGC kernels (off by default).  The reference's NanoJProfiler timings
+ * (LiveSRRF_CL.java:67, 609-631, 727-741) are the counterpart.  Events are read back once,
+ * after the call's final stream synchronisation, so timing adds no intermediate waits. */
+esrrf_status esrrf_set_timing(esrrf_handle* h, int enable);
+
+/* Device time (ms) of the last calculate call's interpolation and RGC kernels (timing on) and
+ * the number of kernels it launched (always). */
+esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* rgc_ms,
+                               int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ESRRF_H */

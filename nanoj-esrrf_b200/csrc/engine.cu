@@ -1,0 +1,559 @@
+// engine.cu -- host engine behind the C ABI (include/esrrf.h).  One handle mirrors one
+// nanoj.liveSRRF.LiveSRRF_CL instance (src/nanoj/liveSRRF/LiveSRRF_CL.java): it owns a CUDA
+// stream, the device buffers and the block bookkeeping that the reference keeps in the
+// two-int nCurrentFrame buffer (LiveSRRF_CL.java:296-299, 738-741, 955-960).
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/esrrf.h"
+#include "engine.h"
+#include "esrrf_internal.h"
+
+using namespace esrrf;
+
+namespace {
+std::mutex g_err_mu;
+std::string g_create_error;
+
+const char* kVersion = "0.1";
+}  // namespace
+
+#define CK(call)                                                                     \
+    do {                                                                             \
+        cudaError_t _e = (call);                                                     \
+        if (_e != cudaSuccess) return h->fail_cuda(_e, #call, __LINE__);             \
+    } while (0)
+
+esrrf_status esrrf_handle::fail(esrrf_status s, const std::string& msg) {
+    err = msg;
+    return s;
+}
+
+esrrf_status esrrf_handle::fail_cuda(cudaError_t e, const char* what, int line) {
+    err = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
+          ") in " + what + " at engine.cu:" + std::to_string(line);
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? ESRRF_ERR_NOMEM : ESRRF_ERR_CUDA;
+}
+
+namespace {
+
+esrrf_status validate(const esrrf_params& p, std::string& msg) {
+    if (p.width < 4 || p.height < 4) return msg = "width and height must be >= 4", ESRRF_ERR_INVALID;
+    if (p.magnification < 1 || p.magnification > 16)
+        return msg = "magnification must be in [1, 16]", ESRRF_ERR_INVALID;
+    if (!(p.fwhm > 0.f) || p.fwhm > 20.f) return msg = "fwhm (radius) must be in (0, 20]", ESRRF_ERR_INVALID;
+    if (p.sensitivity < 0 || p.sensitivity > 64) return msg = "sensitivity must be in [0, 64]", ESRRF_ERR_INVALID;
+    if (p.n_frame_for_srrf < 1) return msg = "n_frame_for_srrf must be >= 1", ESRRF_ERR_INVALID;
+    if (p.n_frames_on_gpu < 1) return msg = "n_frames_on_gpu must be >= 1", ESRRF_ERR_INVALID;
+    if (p.frames_per_launch < 0) return msg = "frames_per_launch must be >= 0", ESRRF_ERR_INVALID;
+    if (p.n_planes < 0) return msg = "n_planes must be >= 0", ESRRF_ERR_INVALID;
+    if (p.n_planes > 0) {
+        if (!p.roi || !p.theta_deg || !p.shift_x || !p.shift_y || !p.intensity_coeff)
+            return msg = "3-D calibration arrays must all be given", ESRRF_ERR_INVALID;
+        if (p.n_planes < 2 || p.n_planes > 9) return msg = "n_planes must be in [2, 9]", ESRRF_ERR_INVALID;
+    }
+    if (p.interp != ESRRF_INTERP_FHT && p.interp != ESRRF_INTERP_BIC)
+        return msg = "interp must be ESRRF_INTERP_FHT or ESRRF_INTERP_BIC", ESRRF_ERR_INVALID;
+    return ESRRF_OK;
+}
+
+int pick_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return -1;
+    int best = 0;
+    double best_score = -1;
+    for (int d = 0; d < n; ++d) {
+        int sms = 0, clk = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
+        cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, d);
+        const double score = (double)sms * clk;  // checkDevices' CU x clock rule
+        if (score > best_score) {
+            best_score = score;
+            best = d;
+        }
+    }
+    return best;
+}
+
+}  // namespace
+
+esrrf_status esrrf_handle::init(const esrrf_params& params) {
+    esrrf_handle* h = this;
+    p = params;
+    if (p.n_planes > 0) {
+        mode = Mode::k3D;
+        roi.assign(p.roi, p.roi + p.n_planes);
+        theta.assign(p.theta_deg, p.theta_deg + p.n_planes);
+        shx.assign(p.shift_x, p.shift_x + p.n_planes);
+        shy.assign(p.shift_y, p.shift_y + p.n_planes);
+        coeff.assign(p.intensity_coeff, p.intensity_coeff + p.n_planes);
+        p.roi = p.theta_deg = p.shift_x = p.shift_y = p.intensity_coeff = nullptr;
+    } else {
+        mode = p.interp == ESRRF_INTERP_FHT ? Mode::kFHT : Mode::kBIC;
+    }
+    device = p.device >= 0 ? p.device : pick_device();
+    if (device < 0) return fail(ESRRF_ERR_NODEVICE, "no CUDA device");
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev_a));
+    CK(cudaEventCreate(&ev_b));
+    CK(cudaEventCreate(&ev_c));
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaEventCreateWithFlags(&ev_host_free[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_copied[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_dev_free[b], cudaEventDisableTiming));
+    }
+    drift_x.assign(p.n_frame_for_srrf, 0.f);
+    drift_y.assign(p.n_frame_for_srrf, 0.f);
+    F = p.frames_per_launch > 0 ? p.frames_per_launch : 8;
+
+    if (mode == Mode::kFHT) return init_fht();
+    return fail(ESRRF_ERR_INVALID, "the bicubic 2-D and 3-D paths are not available in this build");
+}
+
+esrrf_status esrrf_handle::init_fht() {
+    esrrf_handle* h = this;
+    const int M = p.magnification;
+    W = p.width;
+    H = p.height;
+    WM = W * M;
+    HM = H * M;
+    PM = 1;
+    CK(interp_plan_create(plan, W, H, M, p.fht_scale));
+    geo = fht_geometry(M, p.fwhm, p.sensitivity);
+    use_fused = (p.kernel == 0) && geo.S <= 32;
+    if (use_fused) CK(fht_fused_tables(geo, WM, HM, tables, stream));
+    const long whM = (long)WM * HM;
+    scratch.capacity = F;
+    CK(cudaMalloc(&scratch.rowT, sizeof(float) * (size_t)F * plan.N * WM));
+    CK(cudaMalloc(&scratch.alt, sizeof(float) * (size_t)F * (2 * plan.N + 1)));
+    CK(cudaMalloc(&scratch.vec, sizeof(float) * (size_t)F * (2 * HM + 2 * WM)));
+    CK(cudaMalloc(&d_interp, sizeof(float) * (size_t)F * whM));
+    CK(cudaMalloc(&d_gx, sizeof(float) * (size_t)F * whM));
+    CK(cudaMalloc(&d_gy, sizeof(float) * (size_t)F * whM));
+    CK(cudaMalloc(&d_shift, sizeof(float) * 2 * (size_t)F));
+    raw_frame_bytes = sizeof(float) * (size_t)W * H;  // holds a float or a uint16 frame
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaMalloc(&d_raw[b], raw_frame_bytes * F));
+        CK(cudaMallocHost(&h_stage[b], raw_frame_bytes * F));
+    }
+    st.pixels = whM;
+    CK(cudaMalloc(&st.acc, sizeof(double) * 4 * whM));
+    CK(cudaMalloc(&st.prev, sizeof(float) * whM));
+    CK(cudaMalloc(&d_out, sizeof(float) * 4 * whM));
+    CK(zero_block(st, stream));
+    CK(cudaStreamSynchronize(stream));
+    frame_in_block = 0;
+    return ESRRF_OK;
+}
+
+void esrrf_handle::release() {
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
+    interp_plan_destroy(plan);
+    fht_fused_tables_free(tables);
+    cudaFree(scratch.rowT);
+    cudaFree(scratch.alt);
+    cudaFree(scratch.vec);
+    cudaFree(d_interp);
+    cudaFree(d_gx);
+    cudaFree(d_gy);
+    cudaFree(d_shift);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(d_raw[b]);
+        cudaFreeHost(h_stage[b]);
+        if (ev_host_free[b]) cudaEventDestroy(ev_host_free[b]);
+        if (ev_copied[b]) cudaEventDestroy(ev_copied[b]);
+        if (ev_dev_free[b]) cudaEventDestroy(ev_dev_free[b]);
+    }
+    cudaFree(st.acc);
+    cudaFree(st.prev);
+    cudaFree(d_out);
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
+    if (ev_a) cudaEventDestroy(ev_a);
+    if (ev_b) cudaEventDestroy(ev_b);
+    if (ev_c) cudaEventDestroy(ev_c);
+    if (stream && own_stream) cudaStreamDestroy(stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    stream = copy_stream = nullptr;
+}
+
+esrrf_status esrrf_handle::reset_block() {
+    esrrf_handle* h = this;
+    CK(cudaSetDevice(device));
+    CK(zero_block(st, stream));
+    frame_in_block = 0;
+    return ESRRF_OK;
+}
+
+// Runs interpolation + RGC for F_now frames that are already in device memory at `src`.
+esrrf_status esrrf_handle::process_chunk(const void* src, bool is_u16, int F_now) {
+    esrrf_handle* h = this;
+    if (mode != Mode::kFHT) return fail(ESRRF_ERR_INVALID, "mode not available");
+    const int M = p.magnification;
+    // per-frame drift of this chunk, in magnified pixels (loadDriftXYGPUbuffer, LiveSRRF_CL.java:586-589)
+    std::vector<float> sh(2 * F_now);
+    bool any_drift = false;
+    for (int f = 0; f < F_now; ++f) {
+        sh[f] = M * drift_x[frame_in_block + f];
+        sh[F_now + f] = M * drift_y[frame_in_block + f];
+        any_drift |= (sh[f] != 0.f || sh[F_now + f] != 0.f);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    if (timing) {
+        esrrf_status r;
+        if ((r = timing_event(&e0)) != ESRRF_OK || (r = timing_event(&e1)) != ESRRF_OK ||
+            (r = timing_event(&e2)) != ESRRF_OK)
+            return r;
+        CK(cudaEventRecord(e0, stream));
+    }
+    CK(interp_run(plan, scratch, src, is_u16, F_now, d_interp, stream, &launches));
+    if (timing) CK(cudaEventRecord(e1, stream));
+    FhtRgcArgs a{};
+    a.interp = d_interp;
+    a.W = WM;
+    a.H = HM;
+    a.F = F_now;
+    a.t0 = frame_in_block;
+    a.int_weighting = p.int_weighting;
+    a.st = st;
+    if (use_fused && !any_drift) {
+        CK(fht_rgc_fused(geo, tables, a, stream));
+        launches += 1;
+    } else {
+        CK(cudaMemcpyAsync(d_shift, sh.data(), sizeof(float) * 2 * F_now, cudaMemcpyHostToDevice, stream));
+        CK(fht_robx(d_interp, WM, HM, F_now, d_gx, d_gy, stream));
+        a.gx = d_gx;
+        a.gy = d_gy;
+        a.shift = d_shift;
+        CK(fht_rgc_plain(geo, a, stream));
+        launches += 2;
+        CK(cudaStreamSynchronize(stream));  // `sh` is a host temporary
+    }
+    if (timing) CK(cudaEventRecord(e2, stream));
+    frame_in_block += F_now;
+    return ESRRF_OK;
+}
+
+// Events come from a pool so per-launch timing needs no synchronisation until the end of the
+// calculate call; triples (interp start, RGC start, RGC end) are read back by collect_timing().
+esrrf_status esrrf_handle::timing_event(cudaEvent_t* out) {
+    esrrf_handle* h = this;
+    if (ev_used == (int)ev_pool.size()) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ev_pool.push_back(e);
+    }
+    *out = ev_pool[ev_used++];
+    return ESRRF_OK;
+}
+
+void esrrf_handle::collect_timing() {
+    for (int i = 0; i + 2 < ev_used; i += 3) {
+        float t1 = 0.f, t2 = 0.f;
+        if (cudaEventElapsedTime(&t1, ev_pool[i], ev_pool[i + 1]) == cudaSuccess) t_interp += t1;
+        if (cudaEventElapsedTime(&t2, ev_pool[i + 1], ev_pool[i + 2]) == cudaSuccess) t_rgc += t2;
+        ++n_rgc_launches;
+    }
+    cudaGetLastError();
+    ev_used = 0;
+}
+
+esrrf_status esrrf_handle::calculate(const void* frames, bool is_u16, int n, bool on_device) {
+    esrrf_handle* h = this;
+    if (n < 0 || (n > 0 && !frames)) return fail(ESRRF_ERR_INVALID, "frames must be non-null");
+    if (frame_in_block + n > p.n_frame_for_srrf)
+        return fail(ESRRF_ERR_STATE, "more frames pushed than n_frame_for_srrf in this block");
+    CK(cudaSetDevice(device));
+    launches = 0;
+    t_interp = t_rgc = 0.f;
+    n_rgc_launches = 0;
+    ev_used = 0;
+    const size_t fbytes = is_u16 ? sizeof(uint16_t) * (size_t)W * H : sizeof(float) * (size_t)W * H;
+    if (on_device) {
+        for (int s = 0; s < n; s += F) {
+            if (cancel.exchange(0)) return ESRRF_CANCELLED;
+            const int F_now = std::min(F, n - s);
+            esrrf_status r = process_chunk((const char*)frames + fbytes * s, is_u16, F_now);
+            if (r != ESRRF_OK) return r;
+        }
+        CK(cudaStreamSynchronize(stream));
+        if (timing) collect_timing();
+        return ESRRF_OK;
+    }
+    // Host frames: double-buffered pinned staging; the copy of chunk s+1 overlaps the kernels of
+    // chunk s (copy stream + events).
+    cudaPointerAttributes attr{};
+    const bool pinned = cudaPointerGetAttributes(&attr, frames) == cudaSuccess &&
+                        attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    int chunk = 0;
+    for (int s = 0; s < n; s += F, ++chunk) {
+        if (cancel.exchange(0)) {
+            cudaStreamSynchronize(copy_stream);
+            cudaStreamSynchronize(stream);
+            return ESRRF_CANCELLED;
+        }
+        const int b = chunk & 1;
+        const int F_now = std::min(F, n - s);
+        const char* src = (const char*)frames + fbytes * s;
+        if (chunk >= 2) CK(cudaStreamWaitEvent(copy_stream, ev_dev_free[b], 0));
+        if (pinned) {
+            CK(cudaMemcpyAsync(d_raw[b], src, fbytes * F_now, cudaMemcpyHostToDevice, copy_stream));
+        } else {
+            if (chunk >= 2) CK(cudaEventSynchronize(ev_host_free[b]));
+            memcpy(h_stage[b], src, fbytes * F_now);
+            CK(cudaMemcpyAsync(d_raw[b], h_stage[b], fbytes * F_now, cudaMemcpyHostToDevice, copy_stream));
+            CK(cudaEventRecord(ev_host_free[b], copy_stream));
+        }
+        CK(cudaEventRecord(ev_copied[b], copy_stream));
+        CK(cudaStreamWaitEvent(stream, ev_copied[b], 0));
+        esrrf_status r = process_chunk(d_raw[b], is_u16, F_now);
+        if (r != ESRRF_OK) return r;
+        CK(cudaEventRecord(ev_dev_free[b], stream));
+    }
+    CK(cudaStreamSynchronize(stream));
+    if (timing) collect_timing();
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_handle::read(float* out, bool on_device) {
+    esrrf_handle* h = this;
+    CK(cudaSetDevice(device));
+    if (frame_in_block == 0) return fail(ESRRF_ERR_STATE, "no frames accumulated in this block");
+    // kernelCalculateVar + NaN->0 (LiveSRRF_CL.java:749-794) on the block accumulated so far.
+    CK(finalize_block(st, p.n_frame_for_srrf, 0, d_out, stream));
+    const size_t bytes = sizeof(float) * 4 * (size_t)st.pixels;
+    CK(cudaMemcpyAsync(out, d_out, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       stream));
+    CK(cudaStreamSynchronize(stream));
+    return ESRRF_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+extern "C" {
+
+const char* esrrf_get_version(void) { return kVersion; }
+
+esrrf_status esrrf_device_count(int* count) {
+    if (!count) return ESRRF_ERR_INVALID;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        return ESRRF_ERR_NODEVICE;
+    }
+    *count = n;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_device_info(int device, char* name, size_t name_len, int* sm_count,
+                               int* clock_mhz) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        cudaGetLastError();
+        return ESRRF_ERR_INVALID;
+    }
+    if (name && name_len) {
+        strncpy(name, prop.name, name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    int clk = 0;
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, device);
+    if (sm_count) *sm_count = prop.multiProcessorCount;
+    if (clock_mhz) *clock_mhz = clk / 1000;
+    return ESRRF_OK;
+}
+
+void esrrf_default_params(esrrf_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->magnification = 5;
+    p->fwhm = 2.0f;
+    p->sensitivity = 1;
+    p->n_frames_on_gpu = 100;
+    p->n_frame_for_srrf = 100;
+    p->block_length = 20000;
+    p->device = -1;
+    p->int_weighting = 1;
+    p->mp_correction = 0;
+    p->interp = ESRRF_INTERP_FHT;
+    p->fht_scale = ESRRF_FHT_SCALE_MEAN_PRESERVING;
+    p->kernel = 0;
+    p->frames_per_launch = 0;
+    p->pixel_size_um = 0.1f;
+}
+
+esrrf_status esrrf_create(const esrrf_params* params, esrrf_handle** out) {
+    if (!params || !out) return ESRRF_ERR_INVALID;
+    *out = nullptr;
+    std::string msg;
+    esrrf_status s = validate(*params, msg);
+    if (s != ESRRF_OK) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_create_error = msg;
+        return s;
+    }
+    esrrf_handle* h = new (std::nothrow) esrrf_handle();
+    if (!h) return ESRRF_ERR_NOMEM;
+    s = h->init(*params);
+    if (s != ESRRF_OK) {
+        {
+            std::lock_guard<std::mutex> lk(g_err_mu);
+            g_create_error = h->err;
+        }
+        h->release();
+        delete h;
+        return s;
+    }
+    *out = h;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_destroy(esrrf_handle* h) {
+    if (!h) return ESRRF_ERR_INVALID;
+    h->release();
+    delete h;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_set_drift(esrrf_handle* h, const float* dx, const float* dy, int n) {
+    if (!h) return ESRRF_ERR_INVALID;
+    if (n != h->p.n_frame_for_srrf && !(n == 0 && !dx && !dy))
+        return h->fail(ESRRF_ERR_INVALID, "drift arrays must hold n_frame_for_srrf values");
+    for (int i = 0; i < h->p.n_frame_for_srrf; ++i) {
+        h->drift_x[i] = dx ? dx[i] : 0.f;
+        h->drift_y[i] = dy ? dy[i] : 0.f;
+    }
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_reset_frame_position(esrrf_handle* h) {
+    if (!h) return ESRRF_ERR_INVALID;
+    return h->reset_block();
+}
+
+esrrf_status esrrf_calculate_srrf_u16(esrrf_handle* h, const uint16_t* frames, int n) {
+    if (!h) return ESRRF_ERR_INVALID;
+    return h->calculate(frames, true, n, false);
+}
+esrrf_status esrrf_calculate_srrf_f32(esrrf_handle* h, const float* frames, int n) {
+    if (!h) return ESRRF_ERR_INVALID;
+    return h->calculate(frames, false, n, false);
+}
+esrrf_status esrrf_calculate_srrf_u16_device(esrrf_handle* h, const uint16_t* frames, int n) {
+    if (!h) return ESRRF_ERR_INVALID;
+    return h->calculate(frames, true, n, true);
+}
+esrrf_status esrrf_calculate_srrf_f32_device(esrrf_handle* h, const float* frames, int n) {
+    if (!h) return ESRRF_ERR_INVALID;
+    return h->calculate(frames, false, n, true);
+}
+
+esrrf_status esrrf_read_srrf(esrrf_handle* h, float* out) {
+    if (!h || !out) return ESRRF_ERR_INVALID;
+    return h->read(out, false);
+}
+esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* out) {
+    if (!h || !out) return ESRRF_ERR_INVALID;
+    return h->read(out, true);
+}
+
+esrrf_status esrrf_output_shape(const esrrf_handle* h, int* wm, int* hm, int* pm) {
+    if (!h) return ESRRF_ERR_INVALID;
+    if (wm) *wm = h->WM;
+    if (hm) *hm = h->HM;
+    if (pm) *pm = h->PM;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len) {
+    if (!h || !out) return ESRRF_ERR_INVALID;
+    if (h->mode != esrrf_handle::Mode::kFHT) return h->fail(ESRRF_ERR_INVALID, "mode not available");
+    const size_t plane = (size_t)h->WM * h->HM;
+    if (out_len < 2 * plane) return h->fail(ESRRF_ERR_INVALID, "output buffer too small");
+    if (cudaSetDevice(h->device) != cudaSuccess) return ESRRF_ERR_CUDA;
+    // The interpolated frames of the last chunk are still resident: recompute the gradient of
+    // the first one (readGradientBuffers reads frame 0 of the last load).
+    if (fht_robx(h->d_interp, h->WM, h->HM, 1, h->d_gx, h->d_gy, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(out, h->d_gx, sizeof(float) * plane, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(out + plane, h->d_gy, sizeof(float) * plane, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return h->fail(ESRRF_ERR_CUDA, "gradient read-back failed");
+    }
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_finish_queue(esrrf_handle* h) {
+    if (!h) return ESRRF_ERR_INVALID;
+    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return h->fail(ESRRF_ERR_CUDA, "stream synchronisation failed");
+    }
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_request_cancel(esrrf_handle* h) {
+    if (!h) return ESRRF_ERR_INVALID;
+    h->cancel.store(1);
+    return ESRRF_OK;
+}
+
+const char* esrrf_last_error(const esrrf_handle* h) {
+    if (!h) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        return g_create_error.c_str();
+    }
+    return h->err.c_str();
+}
+
+esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* rgc_ms, int* launches) {
+    if (!h) return ESRRF_ERR_INVALID;
+    if (interp_ms) *interp_ms = h->t_interp;
+    if (rgc_ms) *rgc_ms = h->t_rgc;
+    if (launches) *launches = h->launches;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_set_stream(esrrf_handle* h, void* stream) {
+    if (!h) return ESRRF_ERR_INVALID;
+    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return h->fail(ESRRF_ERR_CUDA, "could not drain the current stream");
+    }
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    if (stream) {
+        h->stream = (cudaStream_t)stream;
+        h->own_stream = false;
+    } else {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return h->fail(ESRRF_ERR_CUDA, "stream creation failed");
+        }
+        h->own_stream = true;
+    }
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_set_timing(esrrf_handle* h, int enable) {
+    if (!h) return ESRRF_ERR_INVALID;
+    h->timing = enable != 0;
+    return ESRRF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,72 @@
+// engine.h -- the esrrf_handle behind the C ABI: one per LiveSRRF_CL-equivalent engine.
+#pragma once
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/esrrf.h"
+#include "esrrf_internal.h"
+
+struct esrrf_handle {
+    enum class Mode { kFHT, kBIC, k3D };
+
+    esrrf_params p{};
+    Mode mode = Mode::kFHT;
+    std::vector<float> roi, theta, shx, shy, coeff;  // 3-D calibration copies
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;
+
+    int W = 0, H = 0;           // raw frame size handled by the kernels
+    int WM = 0, HM = 0, PM = 1; // output plane size and number of output planes
+    int F = 8;                  // frames per interpolation + RGC launch
+
+    // FHT path
+    esrrf::InterpPlan plan;
+    esrrf::InterpScratch scratch;
+    esrrf::FhtGeometry geo;
+    esrrf::FhtFusedTables tables;
+    bool use_fused = false;
+    float* d_interp = nullptr;
+    float* d_gx = nullptr;
+    float* d_gy = nullptr;
+    float* d_shift = nullptr;
+
+    // input staging (double-buffered)
+    size_t raw_frame_bytes = 0;
+    void* d_raw[2] = {nullptr, nullptr};
+    void* h_stage[2] = {nullptr, nullptr};
+    cudaEvent_t ev_host_free[2] = {nullptr, nullptr};
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr};
+    cudaEvent_t ev_dev_free[2] = {nullptr, nullptr};
+
+    // block accumulators and output
+    esrrf::BlockState st;
+    float* d_out = nullptr;
+    int frame_in_block = 0;     // nCurrentFrame[0] of the reference
+    std::vector<float> drift_x, drift_y;
+
+    // control, errors, timing
+    std::atomic<int> cancel{0};
+    std::string err;
+    bool timing = false;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr;
+    std::vector<cudaEvent_t> ev_pool;  // [3 per chunk] interp start, RGC start, RGC end
+    int ev_used = 0;
+    float t_interp = 0.f, t_rgc = 0.f;
+    int launches = 0, n_rgc_launches = 0;
+    bool own_stream = true;
+
+    esrrf_status timing_event(cudaEvent_t* out);
+    void collect_timing();
+
+    esrrf_status init(const esrrf_params& params);
+    esrrf_status init_fht();
+    void release();
+    esrrf_status reset_block();
+    esrrf_status calculate(const void* frames, bool is_u16, int n, bool on_device);
+    esrrf_status process_chunk(const void* src, bool is_u16, int F_now);
+    esrrf_status read(float* out, bool on_device);
+    esrrf_status fail(esrrf_status s, const std::string& msg);
+    esrrf_status fail_cuda(cudaError_t e, const char* what, int line);
+};

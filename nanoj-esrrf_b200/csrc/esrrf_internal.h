@@ -1,0 +1,117 @@
+// esrrf_internal.h -- shared declarations of the libesrrf CUDA kernels and host engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace esrrf {
+
+// ------------------------------------------------------------------------------------------
+// Fourier interpolation plan.
+//
+// FourierInterpolation.fhtSpaceInterpolation (FourierInterpolation.java:12-58) mirror-pads a
+// frame to an N x N square (N a power of two), takes its 2-D Hartley transform, moves every
+// spectral index p >= N/2 to p + (M-1) N on an NM x NM canvas, inverts, and crops.  The whole
+// map is linear in the frame and, written out, equals
+//     I' = s [ Dy X Dx^T + P (x) c_x + c_y (x) Q - u_y (x) R - T (x) u_x ]
+// where X is the padded frame, D the N-1-term Dirichlet kernel sampled at
+// 2 pi (m M - n)/(N M), c(n) = cos(pi n / M), u(n) = sin(pi n / M), and P, Q, R, T are per-frame
+// vectors built from the alternating row/column sums of X (the unpaired Nyquist row/column of
+// the Hartley spectrum).  The dense part runs as two batched GEMMs; the rank-one part is
+// folded into the second GEMM's epilogue.
+// ------------------------------------------------------------------------------------------
+struct InterpPlan {
+    int w = 0, h = 0, M = 0;  // raw frame size and magnification
+    int N = 0;                // padded square size
+    int WM = 0, HM = 0;       // output size
+    int xroi = 0, yroi = 0;   // crop offsets on the NM canvas
+    bool identity_pad = true; // no mirror padding needed (power-of-two square input)
+    double s_axis = 0;        // per-axis scale folded into Dx, Dy
+    double s = 0;             // total scale
+    // device arrays
+    float* dxT = nullptr;     // [N][WM]   (Dx transposed, scaled)
+    float* dy = nullptr;      // [HM][N]   (scaled)
+    float* dyT = nullptr;     // [N][HM]   (scaled, transposed copy for the vector kernel)
+    float* cx = nullptr;      // [WM]
+    float* ux = nullptr;      // [WM]
+    float* cy = nullptr;      // [HM]
+    float* uy = nullptr;      // [HM]
+    int* srcx = nullptr;      // [N] source column of padded column
+    int* srcy = nullptr;      // [N] source row of padded row
+};
+
+// Per-frame interpolation scratch for a chunk of F frames.
+struct InterpScratch {
+    int capacity = 0;
+    float* rowT = nullptr;    // [F][N][WM]  first-pass output
+    float* alt = nullptr;     // [F][2N+1]   alternating row sums, column sums, q
+    float* vec = nullptr;     // [F][2HM+2WM] P, T (rows) and Q, R (columns)
+};
+
+cudaError_t interp_plan_create(InterpPlan& plan, int w, int h, int M, int scale_mode);
+void interp_plan_destroy(InterpPlan& plan);
+
+// raw: [F][h][w] uint16 (is_u16) or float; out: [F][HM][WM]
+cudaError_t interp_run(const InterpPlan& plan, InterpScratch& scratch, const void* raw,
+                       bool is_u16, int F, float* out, cudaStream_t stream, int* launches);
+
+// ------------------------------------------------------------------------------------------
+// RGC geometry of the FHT path (liveSRRF_noInterpolation.cl:245-393, constants from
+// LiveSRRF_CL.java:491-500).  Taps are integer offsets (i, j) in [r0, r1]^2.
+// ------------------------------------------------------------------------------------------
+constexpr int kMaxBox = 48;  // max tap box side r1 - r0 + 1 supported by the fused kernel
+
+struct FhtGeometry {
+    float sigma = 0, tSS = 0, tSO = 0, radius = 0;
+    int r0 = 0, r1 = 0, S = 0;   // S = r1 - r0 + 1
+    float sensitivity = 1;
+    // host tables [S][S] indexed [(j - r0) * S + (i - r0)]
+    std::vector<float> w, wd;    // weight and weight / distance (0 outside the tap disc)
+    std::vector<int> jlo, jhi;   // per column i: valid j range (jlo > jhi if none)
+    float wsum_interior = 0;     // sum of weights in the reference's (j, i) order
+};
+FhtGeometry fht_geometry(int M, float fwhm, int sensitivity);
+
+// Accumulator state for one SR block on the device.
+struct BlockState {
+    long pixels = 0;
+    double* acc = nullptr;  // [4][pixels]: sum X, sum X^2, sum X_t X_{t-1}, sum v
+    float* prev = nullptr;  // [pixels]
+};
+
+struct FhtRgcArgs {
+    const float* interp;   // [F][H][W]
+    const float* gx;       // plain path: [F][H][W] Roberts-cross gradients
+    const float* gy;
+    int W, H, F;
+    int t0;                // frame index within the block of the first frame
+    const float* shift;    // [2][F] drift in magnified pixels (plain path)
+    int int_weighting;
+    BlockState st;
+};
+
+cudaError_t fht_robx(const float* interp, int W, int H, int F, float* gx, float* gy,
+                     cudaStream_t stream);
+cudaError_t fht_rgc_plain(const FhtGeometry& g, const FhtRgcArgs& a, cudaStream_t stream);
+
+struct FhtFusedTables {
+    float* wtab = nullptr;     // device [S*S] weights
+    float* wdtab = nullptr;    // device [S*S] weight / distance
+    int* jrange = nullptr;     // device [2*S]
+    float* wsum = nullptr;     // device [H*W] per-pixel weight sums
+};
+cudaError_t fht_fused_tables(const FhtGeometry& g, int W, int H, FhtFusedTables& t,
+                             cudaStream_t stream);
+void fht_fused_tables_free(FhtFusedTables& t);
+cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
+                          cudaStream_t stream);
+
+// AVG/VAR/TAC2/INT from the block accumulators (kernelCalculateVar and the readback's NaN->0).
+// tac_div2: the 2-D bicubic path's double division of TAC2 by (n-1).
+cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out,
+                           cudaStream_t stream);
+cudaError_t zero_block(BlockState& st, cudaStream_t stream);
+
+}  // namespace esrrf

@@ -1,0 +1,401 @@
+// interp.cu -- Fourier (Hartley) interpolation of frames by the magnification on the GPU.
+//
+// Replaces the per-frame CPU loop FourierInterpolation.fhtSpaceInterpolation
+// (FourierInterpolation.java:12-73) that LiveSRRF_CL.prepareDataFHT_SRRF runs before every
+// upload (LiveSRRF_CL.java:598-617).  The reference's transform is nanoj.core2.NanoJFHT
+// (NanoJ-Core, not vendored); this file implements the map that its call sites define -- mirror
+// padding to a power-of-two square (FourierInterpolation.java:118-172), forward 2-D Hartley
+// transform, spectral index remap p -> p (p < N/2) or p + (M-1) N (:33-42), inverse transform on
+// the magnified canvas, crop (:49-56) -- in closed form: a separable Dirichlet-kernel product
+// (two batched GEMMs) plus four rank-one terms from the Hartley spectrum's unpaired Nyquist row
+// and column.
+#include <math.h>
+
+#include <algorithm>
+
+#include "esrrf_internal.h"
+
+namespace esrrf {
+
+namespace {
+
+// Power-of-two size that mirrorPaddingEvenSquare pads to (FourierInterpolation.java:125-130).
+int pow2_ceil_java(int n) {
+    int b = (int)std::ceil(std::log((double)n) / std::log(2.0));
+    return (int)std::pow(2.0, (double)b);
+}
+
+// Source index along one axis of padded position c (mirror tiling with an odd number of tiles,
+// centre tile unflipped, then a centred crop of length out_dim; FourierInterpolation.java:138-171).
+int mirror_src(int c, int n, int out_dim) {
+    int scale = (int)std::ceil((double)out_dim / n);
+    if (scale % 2 == 0) scale += 1;
+    const int roi = (scale * n - out_dim) / 2;
+    const int pos = c + roi;
+    const int tile = pos / n;
+    const int i = pos - tile * n;
+    const int rel = tile - (scale - 1) / 2;
+    return (rel % 2 == 0) ? i : n - 1 - i;
+}
+
+// N-1-term Dirichlet kernel sum_{|k| < N/2} cos(k a), a = 2 pi j / NM, j in [0, NM).
+double dirichlet(long j, int N, long NM) {
+    if (j == 0) return (double)(N - 1);
+    const double a = 2.0 * M_PI * (double)j / (double)NM;
+    return std::sin((N - 1) * a / 2.0) / std::sin(a / 2.0);
+}
+
+template <class T>
+cudaError_t upload(T** dptr, const std::vector<T>& host) {
+    cudaError_t e = cudaMalloc((void**)dptr, sizeof(T) * host.size());
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*dptr, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice);
+}
+
+__device__ __forceinline__ float load_raw(const void* raw, bool is_u16, long idx) {
+    return is_u16 ? (float)__ldg((const unsigned short*)raw + idx) : __ldg((const float*)raw + idx);
+}
+
+// Alternating sums of the padded frame: wy[y] = sum_x (-1)^x X[y][x], wx[x] = sum_y (-1)^y X[y][x],
+// q = sum_y (-1)^y wy[y].  One CTA per frame.
+__global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u16, int w, int h,
+                                                       int N, const int* __restrict__ srcx,
+                                                       const int* __restrict__ srcy,
+                                                       float* __restrict__ alt) {
+    const int f = blockIdx.x;
+    const void* frame = is_u16 ? (const void*)((const unsigned short*)raw + (long)f * w * h)
+                               : (const void*)((const float*)raw + (long)f * w * h);
+    float* out = alt + (long)f * (2 * N + 1);
+    __shared__ double red[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double qpart = 0.0;
+    // rows: one warp per row
+    for (int y = warp; y < N; y += 8) {
+        const long rowoff = (long)srcy[y] * w;
+        double s = 0.0;
+        for (int x = lane; x < N; x += 32) {
+            const float v = load_raw(frame, is_u16, rowoff + srcx[x]);
+            s += (x & 1) ? -(double)v : (double)v;
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            out[y] = (float)s;
+            qpart += (y & 1) ? -s : s;
+        }
+    }
+    // columns: one thread per column
+    for (int x = threadIdx.x; x < N; x += blockDim.x) {
+        const int sx = srcx[x];
+        double s = 0.0;
+        for (int y = 0; y < N; ++y) {
+            const float v = load_raw(frame, is_u16, (long)srcy[y] * w + sx);
+            s += (y & 1) ? -(double)v : (double)v;
+        }
+        out[N + x] = (float)s;
+    }
+    if (lane == 0) red[warp] = qpart;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double q = 0.0;
+        for (int i = 0; i < 8; ++i) q += red[i];
+        out[2 * N] = (float)q;
+    }
+}
+
+// Rank-one correction vectors per frame:
+//   P = s_axis Dy wy,  T = s_axis Dy flip(wy) + s q cy,
+//   Q = s_axis Dx wx + s q cx,  R = s_axis Dx flip(wx) + s q (cx + ux),
+// flip(w)[m] = w[(N - m) mod N].  Dy, Dx already carry s_axis.
+__global__ void __launch_bounds__(256) rank1_vectors_kernel(
+    const float* __restrict__ alt, const float* __restrict__ dyT, const float* __restrict__ dxT,
+    const float* __restrict__ cx, const float* __restrict__ ux, const float* __restrict__ cy,
+    int N, int HM, int WM, float s_axis, float s, float* __restrict__ vec) {
+    extern __shared__ float wsh[];  // [2N]: wy then wx
+    const int f = blockIdx.y;
+    const float* a = alt + (long)f * (2 * N + 1);
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) wsh[i] = a[i];
+    __syncthreads();
+    const float q = a[2 * N];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    float* v = vec + (long)f * (2 * HM + 2 * WM);
+    if (e < HM) {
+        float d0 = 0.f, d1 = 0.f;
+        for (int y = 0; y < N; ++y) {
+            const float dv = dyT[(long)y * HM + e];
+            d0 = fmaf(dv, wsh[y], d0);
+            d1 = fmaf(dv, wsh[(N - y) & (N - 1)], d1);
+        }
+        v[e] = s_axis * d0;
+        v[HM + e] = s_axis * d1 + s * q * cy[e];
+    } else if (e < HM + WM) {
+        const int n = e - HM;
+        float d0 = 0.f, d1 = 0.f;
+        for (int x = 0; x < N; ++x) {
+            const float dv = dxT[(long)x * WM + n];
+            d0 = fmaf(dv, wsh[N + x], d0);
+            d1 = fmaf(dv, wsh[N + ((N - x) & (N - 1))], d1);
+        }
+        v[2 * HM + n] = s_axis * d0 + s * q * cx[n];
+        v[2 * HM + WM + n] = s_axis * d1 + s * q * (cx[n] + ux[n]);
+    }
+}
+
+// --------------------------------------------------------------------------------------------
+// Batched FP32 GEMM, 128x128x8 CTA tile, 256 threads, 8x8 outputs per thread (two 4x4 quads
+// 64 apart in each direction so that shared-memory reads are conflict free).
+//   PASS 1: C[f] (N x WM)  = X_f (N x N, gathered through the padding tables) . dxT (N x WM)
+//   PASS 2: C[f] (HM x WM) = dy (HM x N) . rowT[f] (N x WM) + rank-one epilogue
+// --------------------------------------------------------------------------------------------
+struct GemmArgs {
+    int Mr, Nc, K;
+    const void* raw;  // pass 1
+    int is_u16, w, h;
+    const int* srcx;
+    const int* srcy;
+    const float* A;   // pass 2: dy
+    const float* B;   // pass 1: dxT; pass 2: rowT
+    float* C;
+    const float* vec; // pass 2 epilogue
+    const float* cx;
+    const float* ux;
+    const float* cy;
+    const float* uy;
+    int HM, WM;
+};
+
+template <int PASS>
+__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+    __shared__ __align__(16) float As[2][8][128];
+    __shared__ __align__(16) float Bs[2][8][128];
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int f = blockIdx.z;
+    const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
+    const float* Bf = (PASS == 1) ? g.B : g.B + (long)f * g.K * g.Nc;
+    const void* rawf = nullptr;
+    if (PASS == 1)
+        rawf = g.is_u16 ? (const void*)((const unsigned short*)g.raw + (long)f * g.w * g.h)
+                        : (const void*)((const float*)g.raw + (long)f * g.w * g.h);
+
+    // global-load mapping
+    const int a_row = tid >> 1, a_k = (tid & 1) * 4;   // A: 128 rows x 8 k
+    const int b_k = tid >> 5, b_col = (tid & 31) * 4;  // B: 8 k x 128 cols
+    float ra[4], rb[4];
+
+    auto load_tiles = [&](int k0) {
+        const int m = m0 + a_row;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int k = k0 + a_k + i;
+            float v = 0.f;
+            if (m < g.Mr && k < g.K) {
+                if (PASS == 1)
+                    v = load_raw(rawf, g.is_u16, (long)__ldg(g.srcy + m) * g.w + __ldg(g.srcx + k));
+                else
+                    v = __ldg(g.A + (long)m * g.K + k);
+            }
+            ra[i] = v;
+        }
+        const int kb = k0 + b_k;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int n = n0 + b_col + i;
+            rb[i] = (kb < g.K && n < g.Nc) ? __ldg(Bf + (long)kb * g.Nc + n) : 0.f;
+        }
+    };
+    auto store_tiles = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) As[buf][a_k + i][a_row] = ra[i];
+        *reinterpret_cast<float4*>(&Bs[buf][b_k][b_col]) = make_float4(rb[0], rb[1], rb[2], rb[3]);
+    };
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+    load_tiles(0);
+    store_tiles(0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < g.K; k0 += 8) {
+        const bool more = k0 + 8 < g.K;
+        if (more) load_tiles(k0 + 8);
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            float a[8], b[8];
+            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][64 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
+            a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
+            a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
+            b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
+            b[4] = b1.x; b[5] = b1.y; b[6] = b1.z; b[7] = b1.w;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        if (more) {
+            store_tiles(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
+        }
+    }
+
+    float* Cf = g.C + (long)f * g.Mr * g.Nc;
+    const float* vec = (PASS == 2) ? g.vec + (long)f * (2 * g.HM + 2 * g.WM) : nullptr;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+        if (m >= g.Mr) continue;
+        float pm = 0.f, tm = 0.f, cym = 0.f, uym = 0.f;
+        if (PASS == 2) {
+            pm = vec[m];
+            tm = vec[g.HM + m];
+            cym = g.cy[m];
+            uym = g.uy[m];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+            if (n >= g.Nc) continue;
+            float v = acc[i][j];
+            if (PASS == 2) {
+                const float qn = vec[2 * g.HM + n], rn = vec[2 * g.HM + g.WM + n];
+                v += pm * g.cx[n] + cym * qn - uym * rn - tm * g.ux[n];
+            }
+            Cf[(long)m * g.Nc + n] = v;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t interp_plan_create(InterpPlan& p, int w, int h, int M, int scale_mode) {
+    p.w = w;
+    p.h = h;
+    p.M = M;
+    const int bw = pow2_ceil_java(w), bh = pow2_ceil_java(h);
+    p.N = std::max(bw, bh);
+    const int N = p.N;
+    const long NM = (long)N * M;
+    p.WM = w * M;
+    p.HM = h * M;
+    p.xroi = (int)((NM - p.WM) / 2);
+    p.yroi = (int)((NM - p.HM) / 2);
+    p.identity_pad = (w == N && h == N);
+    p.s_axis = scale_mode == 0 ? 1.0 / N : 1.0 / (double)NM;
+    p.s = p.s_axis * p.s_axis;
+
+    std::vector<int> sx(N), sy(N);
+    for (int c = 0; c < N; ++c) {
+        sx[c] = mirror_src(c, w, N);
+        sy[c] = mirror_src(c, h, N);
+    }
+    std::vector<float> dxT((size_t)N * p.WM), dy((size_t)p.HM * N), dyT((size_t)N * p.HM);
+    for (int n = 0; n < p.WM; ++n)
+        for (int m = 0; m < N; ++m) {
+            long j = ((long)m * M - (n + p.xroi)) % NM;
+            if (j < 0) j += NM;
+            dxT[(size_t)m * p.WM + n] = (float)(dirichlet(j, N, NM) * p.s_axis);
+        }
+    for (int n = 0; n < p.HM; ++n)
+        for (int m = 0; m < N; ++m) {
+            long j = ((long)m * M - (n + p.yroi)) % NM;
+            if (j < 0) j += NM;
+            const float v = (float)(dirichlet(j, N, NM) * p.s_axis);
+            dy[(size_t)n * N + m] = v;
+            dyT[(size_t)m * p.HM + n] = v;
+        }
+    std::vector<float> cx(p.WM), ux(p.WM), cy(p.HM), uy(p.HM);
+    for (int n = 0; n < p.WM; ++n) {
+        const double a = M_PI * (double)(n + p.xroi) / M;
+        cx[n] = (float)std::cos(a);
+        ux[n] = (float)std::sin(a);
+    }
+    for (int n = 0; n < p.HM; ++n) {
+        const double a = M_PI * (double)(n + p.yroi) / M;
+        cy[n] = (float)std::cos(a);
+        uy[n] = (float)std::sin(a);
+    }
+    cudaError_t e;
+    if ((e = upload(&p.dxT, dxT)) != cudaSuccess) return e;
+    if ((e = upload(&p.dy, dy)) != cudaSuccess) return e;
+    if ((e = upload(&p.dyT, dyT)) != cudaSuccess) return e;
+    if ((e = upload(&p.cx, cx)) != cudaSuccess) return e;
+    if ((e = upload(&p.ux, ux)) != cudaSuccess) return e;
+    if ((e = upload(&p.cy, cy)) != cudaSuccess) return e;
+    if ((e = upload(&p.uy, uy)) != cudaSuccess) return e;
+    if ((e = upload(&p.srcx, sx)) != cudaSuccess) return e;
+    if ((e = upload(&p.srcy, sy)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+void interp_plan_destroy(InterpPlan& p) {
+    cudaFree(p.dxT);
+    cudaFree(p.dy);
+    cudaFree(p.dyT);
+    cudaFree(p.cx);
+    cudaFree(p.ux);
+    cudaFree(p.cy);
+    cudaFree(p.uy);
+    cudaFree(p.srcx);
+    cudaFree(p.srcy);
+    p = InterpPlan();
+}
+
+cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, bool is_u16, int F,
+                       float* out, cudaStream_t stream, int* launches) {
+    if (F <= 0) return cudaSuccess;
+    if (F > sc.capacity) return cudaErrorInvalidValue;
+    const int N = p.N;
+    alt_sums_kernel<<<F, 256, 0, stream>>>(raw, is_u16 ? 1 : 0, p.w, p.h, N, p.srcx, p.srcy, sc.alt);
+    {
+        dim3 grid((p.HM + p.WM + 255) / 256, F);
+        rank1_vectors_kernel<<<grid, 256, sizeof(float) * 2 * N, stream>>>(
+            sc.alt, p.dyT, p.dxT, p.cx, p.ux, p.cy, N, p.HM, p.WM, (float)p.s_axis, (float)p.s,
+            sc.vec);
+    }
+    GemmArgs g{};
+    g.raw = raw;
+    g.is_u16 = is_u16 ? 1 : 0;
+    g.w = p.w;
+    g.h = p.h;
+    g.srcx = p.srcx;
+    g.srcy = p.srcy;
+    g.HM = p.HM;
+    g.WM = p.WM;
+    // pass 1: rows of the padded frame times dxT
+    g.Mr = N;
+    g.Nc = p.WM;
+    g.K = N;
+    g.B = p.dxT;
+    g.C = sc.rowT;
+    {
+        dim3 grid((g.Nc + 127) / 128, (g.Mr + 127) / 128, F);
+        gemm_kernel<1><<<grid, 256, 0, stream>>>(g);
+    }
+    // pass 2: dy times the first-pass rows, plus the rank-one epilogue
+    g.Mr = p.HM;
+    g.Nc = p.WM;
+    g.K = N;
+    g.A = p.dy;
+    g.B = sc.rowT;
+    g.C = out;
+    g.vec = sc.vec;
+    g.cx = p.cx;
+    g.ux = p.ux;
+    g.cy = p.cy;
+    g.uy = p.uy;
+    {
+        dim3 grid((g.Nc + 127) / 128, (g.Mr + 127) / 128, F);
+        gemm_kernel<2><<<grid, 256, 0, stream>>>(g);
+    }
+    if (launches) *launches += 4;
+    return cudaGetLastError();
+}
+
+}  // namespace esrrf

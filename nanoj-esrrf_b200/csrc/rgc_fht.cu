@@ -1,0 +1,514 @@
+// rgc_fht.cu -- radial gradient convergence on Fourier-interpolated frames (the default 2-D
+// path: LiveSRRF_CL.prepareBuffersFHTinterpolation loads liveSRRF_noInterpolation.cl,
+// LiveSRRF_CL.java:462-579).
+//
+// Two kernels compute the same map:
+//  * fht_rgc_plain_kernel: one thread per output pixel, the reference's per-tap arithmetic
+//    (liveSRRF_noInterpolation.cl:245-393) on a separately computed Roberts-cross gradient
+//    (:138-159); handles frames with drift.  Cumulants are kept in registers across the frames
+//    of one launch instead of the reference's per-frame global read-modify-write.
+//  * fht_rgc_fused_kernel: 32x64-pixel output tiles; per frame it stages the interpolated tile
+//    plus the RGC halo in shared memory, forms the unit gradient field there, and runs the tap
+//    loop with each thread owning 8 vertically adjacent outputs so that one shared-memory load
+//    feeds up to 8 taps.  With zero drift the tap offsets are integers (dx = i, dy = j), so the
+//    distance weights are a per-launch table and the contribution of an inward tap reduces to
+//    w - (w/d) |g_y i - g_x j| on the unit gradient g.
+#include <math.h>
+
+#include <algorithm>
+
+#include "esrrf_internal.h"
+
+namespace esrrf {
+
+FhtGeometry fht_geometry(int M, float fwhm, int sensitivity) {
+    // Java float arithmetic of prepareBuffersFHTinterpolation (LiveSRRF_CL.java:490-500).
+    FhtGeometry g;
+    const float Mf = (float)M;
+    g.sigma = fwhm / 2.354f;
+    float t = 2.0f * g.sigma;
+    t = t * Mf;
+    t = t * g.sigma;
+    t = t * Mf;
+    g.tSS = t;
+    g.tSO = (2.0f * g.sigma + 1.0f) * Mf;
+    g.radius = Mf * ((float)((int)(2.0f * g.sigma)) + 1.0f);
+    g.r0 = -(int)g.radius;
+    g.r1 = (int)(g.radius + 1.0f);
+    g.S = g.r1 - g.r0 + 1;
+    g.sensitivity = (float)sensitivity;
+    const int S = g.S;
+    g.w.assign((size_t)S * S, 0.f);
+    g.wd.assign((size_t)S * S, 0.f);
+    g.jlo.assign(S, S);
+    g.jhi.assign(S, -1);
+    float wsum = 0.f;
+    for (int jj = 0; jj < S; ++jj) {
+        for (int ii = 0; ii < S; ++ii) {
+            const int i = g.r0 + ii, j = g.r0 + jj;
+            const float d = sqrtf((float)(i * i + j * j));
+            if (!(d != 0.f && d <= g.tSO)) continue;
+            const float dd = d * d;
+            float w = d * expf(-dd / g.tSS);
+            w = w * w * w * w;
+            g.w[(size_t)jj * S + ii] = w;
+            g.wd[(size_t)jj * S + ii] = w / d;
+            wsum += w;
+            g.jlo[ii] = std::min(g.jlo[ii], jj);
+            g.jhi[ii] = std::max(g.jhi[ii], jj);
+        }
+    }
+    g.wsum_interior = wsum;
+    return g;
+}
+
+namespace {
+
+__device__ __forceinline__ float cglh_power(float c, float s) {
+    // CGLH >= 0 ? pow(CGLH, S) : 0, NaN -> 0 (liveSRRF_noInterpolation.cl:349-353).
+    if (!(c >= 0.f)) return 0.f;
+    if (s == 1.f) return c;
+    if (s == 2.f) return c * c;
+    if (s == 3.f) return c * c * c;
+    if (s == 4.f) {
+        const float c2 = c * c;
+        return c2 * c2;
+    }
+    return powf(c, s);
+}
+
+// Catmull-Rom kernel and bicubic/bilinear sampler (liveSRRF_noInterpolation.cl:17-75).
+__device__ __forceinline__ float cubic(float x) {
+    const float a = 0.5f;
+    if (x < 0.0f) x = -x;
+    float z = 0.0f;
+    if (x < 1.0f)
+        z = x * x * (x * (-a + 2.0f) + (a - 3.0f)) + 1.0f;
+    else if (x < 2.0f)
+        z = -a * x * x * x + 5.0f * a * x * x - 8.0f * a * x + 4.0f * a;
+    return z;
+}
+
+__device__ float sample2d(const float* __restrict__ a, int w, int h, float x, float y) {
+    const int u0 = (int)floorf(x);
+    const int v0 = (int)floorf(y);
+    if (u0 > 0 && u0 < w - 2 && v0 > 0 && v0 < h - 2) {
+        float q = 0.0f;
+        for (int j = 0; j <= 3; j++) {
+            const int v = min(max(v0 - 1 + j, 0), h - 1);
+            float p = 0.0f;
+            for (int i = 0; i <= 3; i++) {
+                const int u = min(max(u0 - 1 + i, 0), w - 1);
+                p = p + __ldg(a + (long)v * w + u) * cubic(x - (float)u);
+            }
+            q = q + p * cubic(y - (float)v);
+        }
+        return q;
+    }
+    const int xb = (int)fminf((float)w - 2, fmaxf(x, 0.0f));
+    const int yb = (int)fminf((float)h - 2, fmaxf(y, 0.0f));
+    const float xf = x - (float)xb, yf = y - (float)yb;
+    const float ll = __ldg(a + (long)yb * w + xb), lr = __ldg(a + (long)yb * w + xb + 1);
+    const float ur = __ldg(a + (long)(yb + 1) * w + xb + 1), ul = __ldg(a + (long)(yb + 1) * w + xb);
+    const float upper = ul + xf * (ur - ul);
+    const float lower = ll + xf * (lr - ll);
+    return lower + yf * (upper - lower);
+}
+
+__global__ void robx_kernel(const float* __restrict__ p, int W, int H, long plane,
+                            float* __restrict__ gx, float* __restrict__ gy) {
+    const int x1 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y1 = blockIdx.y;
+    const long f = blockIdx.z;
+    if (x1 >= W) return;
+    const int x0 = max(x1 - 1, 0), y0 = max(y1 - 1, 0);
+    const float* q = p + f * plane;
+    const float a = q[(long)y0 * W + x1], b = q[(long)y1 * W + x0];
+    const float c = q[(long)y1 * W + x1], d = q[(long)y0 * W + x0];
+    gx[f * plane + (long)y1 * W + x1] = a - b + c - d;
+    gy[f * plane + (long)y1 * W + x1] = -a + b + c - d;
+}
+
+struct PlainParams {
+    float tSS, tSO, radius, sens;
+};
+
+__global__ void __launch_bounds__(256) fht_rgc_plain_kernel(FhtRgcArgs a, PlainParams pp) {
+    const long pix = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long wh = (long)a.W * a.H;
+    if (pix >= wh) return;
+    const int yM = (int)(pix / a.W), xM = (int)(pix - (long)yM * a.W);
+    const int r0 = -(int)pp.radius, r1 = (int)(pp.radius + 1);
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    float prev = a.st.prev[pix];
+    for (int f = 0; f < a.F; ++f) {
+        const float* fr = a.interp + (long)f * wh;
+        const float* gxf = a.gx + (long)f * wh;
+        const float* gyf = a.gy + (long)f * wh;
+        const float sx = a.shift[f], sy = a.shift[a.F + f];
+        const float xc = (float)((double)xM + 0.5 + (double)sx);
+        const float yc = (float)((double)yM + 0.5 + (double)sy);
+        const int bx = (int)((double)xc - 0.5), by = (int)((double)yc - 0.5);
+        float cglh = 0.f, wsum = 0.f;
+        for (int j = r0; j <= r1; ++j) {
+            const float vy = (float)((double)((float)by + (float)j) + 0.5);
+            if (!(vy > 0 && vy < (float)a.H)) continue;
+            for (int i = r0; i <= r1; ++i) {
+                const float vx = (float)((double)((float)bx + (float)i) + 0.5);
+                if (!(vx > 0 && vx < (float)a.W)) continue;
+                const float dx = vx - xc, dy = vy - yc;
+                const float d = sqrtf(dx * dx + dy * dy);
+                if (!(d != 0.f && d <= pp.tSO)) continue;
+                const int gxx = min(max((int)((double)vx - 0.5 + 1), 0), a.W - 1);
+                const int gxy = min(max((int)((double)vy - 0.5), 0), a.H - 1);
+                const int gyx = min(max((int)((double)vx - 0.5), 0), a.W - 1);
+                const int gyy = min(max((int)((double)vy - 0.5 + 1), 0), a.H - 1);
+                const float Gx = __ldg(gxf + (long)gxy * a.W + gxx);
+                const float Gy = __ldg(gyf + (long)gyy * a.W + gyx);
+                float w = d * expf(-(d * d) / pp.tSS);
+                w = w * w * w * w;
+                wsum += w;
+                if (Gx * dx + Gy * dy < 0) {
+                    const float gm = sqrtf(Gx * Gx + Gy * Gy);
+                    float dk = fabsf(Gy * dx - Gx * dy) / gm;
+                    if (isnan(dk)) dk = d;
+                    dk = 1 - dk / d;
+                    cglh += dk * w;
+                }
+            }
+        }
+        const float cg = cglh_power(cglh / wsum, pp.sens);
+        float v;
+        if (sx == 0.f && sy == 0.f)
+            v = __ldg(fr + pix);
+        else
+            v = sample2d(fr, a.W, a.H, (float)xM + sx, (float)yM + sy);
+        const float x = a.int_weighting ? v * cg : cg;
+        s0 += x;
+        s1 += (double)x * x;
+        if (a.t0 + f > 0) s2 += (double)x * prev;
+        s3 += v;
+        prev = x;
+    }
+    a.st.acc[pix] += s0;
+    a.st.acc[wh + pix] += s1;
+    a.st.acc[2 * wh + pix] += s2;
+    a.st.acc[3 * wh + pix] += s3;
+    a.st.prev[pix] = prev;
+}
+
+// Per-pixel sum of tap weights over in-image taps, in the reference's (j outer, i inner)
+// float order, so interior and border pixels normalise exactly as liveSRRF_noInterpolation.cl.
+__global__ void wsum_kernel(const float* __restrict__ wtab, int r0, int S, int W, int H,
+                            float* __restrict__ wsum) {
+    const long pix = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= (long)W * H) return;
+    const int yM = (int)(pix / W), xM = (int)(pix - (long)yM * W);
+    float s = 0.f;
+    for (int jj = 0; jj < S; ++jj) {
+        const int Y = yM + r0 + jj;
+        if (Y < 0 || Y >= H) continue;
+        for (int ii = 0; ii < S; ++ii) {
+            const int X = xM + r0 + ii;
+            if (X < 0 || X >= W) continue;
+            const float w = wtab[jj * S + ii];
+            if (w != 0.f) s += w;
+        }
+    }
+    wsum[pix] = s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Fused tile kernel.
+// ---------------------------------------------------------------------------------------------
+constexpr int kTX = 32;          // output columns per CTA (one warp wide)
+constexpr int kTYT = 8;          // thread rows per CTA
+constexpr int kK = 8;            // outputs per thread (vertical)
+constexpr int kTH = kTYT * kK;   // output rows per CTA
+
+struct FusedSmem {
+    int EW, EH, IW, IH, S;
+    size_t off_E, off_I, off_w, off_wd, off_jr, off_st, bytes;
+};
+
+__host__ __device__ inline FusedSmem fused_smem_layout(int S) {
+    FusedSmem L;
+    L.S = S;
+    L.EW = kTX + S - 1;
+    L.EH = kTH + S - 1;
+    L.IW = L.EW + 2;
+    L.IH = L.EH + 2;
+    size_t o = 0;
+    L.off_E = o;
+    o += sizeof(float2) * (size_t)L.EW * L.EH;
+    L.off_I = o;
+    o += sizeof(float) * (size_t)L.IW * L.IH;
+    o = (o + 15) & ~size_t(15);
+    L.off_w = o;
+    o += sizeof(float) * (size_t)S * S;
+    L.off_wd = o;
+    o += sizeof(float) * (size_t)S * S;
+    L.off_jr = o;
+    o += sizeof(int) * 2 * (size_t)S;
+    o = (o + 15) & ~size_t(15);
+    L.off_st = o;
+    o += sizeof(float) * 5 * kTX * kTH;
+    L.bytes = o;
+    return L;
+}
+
+struct FusedParams {
+    int r0, S;
+    float sens;
+    const float* wtab;
+    const float* wdtab;
+    const int* jrange;
+    const float* wsum;
+};
+
+template <int SB>
+__global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, FusedParams fp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const FusedSmem L = fused_smem_layout(fp.S);
+    float2* sE = reinterpret_cast<float2*>(smem + L.off_E);
+    float* sI = reinterpret_cast<float*>(smem + L.off_I);
+    float* sw = reinterpret_cast<float*>(smem + L.off_w);
+    float* swd = reinterpret_cast<float*>(smem + L.off_wd);
+    int* sjr = reinterpret_cast<int*>(smem + L.off_jr);
+    float* sst = reinterpret_cast<float*>(smem + L.off_st);  // [5][kTH][kTX]
+
+    const int tid = threadIdx.x;
+    const int tx = tid & 31, ty = tid >> 5;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTH;
+    const int S = fp.S, r0 = fp.r0;
+    const int W = a.W, H = a.H;
+    const long wh = (long)W * H;
+
+    for (int i = tid; i < S * S; i += blockDim.x) {
+        sw[i] = fp.wtab[i];
+        swd[i] = fp.wdtab[i];
+    }
+    for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = fp.jrange[i];
+
+    // per-output constants and block state
+    const int xM = x0 + tx;
+    float wsum[kK];
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const int yM = y0 + ty * kK + k;
+        const bool in = xM < W && yM < H;
+        const long pix = (long)yM * W + xM;
+        wsum[k] = in ? fp.wsum[pix] : 1.f;
+        const int o = (ty * kK + k) * kTX + tx;
+        sst[0 * kTX * kTH + o] = 0.f;
+        sst[1 * kTX * kTH + o] = 0.f;
+        sst[2 * kTX * kTH + o] = 0.f;
+        sst[3 * kTX * kTH + o] = 0.f;
+        sst[4 * kTX * kTH + o] = in ? a.st.prev[pix] : 0.f;
+    }
+
+    const int gX0 = x0 + r0 - 1, gY0 = y0 + r0 - 1;  // global origin of the intensity tile
+    const float fr0 = (float)r0;
+
+    for (int f = 0; f < a.F; ++f) {
+        const float* fr = a.interp + (long)f * wh;
+        __syncthreads();
+        // 1. interpolated tile with a one-pixel margin beyond the gradient halo (clamped reads)
+        for (int idx = tid; idx < L.IW * L.IH; idx += blockDim.x) {
+            const int ly = idx / L.IW, lx = idx - ly * L.IW;
+            const int gy = min(max(gY0 + ly, 0), H - 1), gx = min(max(gX0 + lx, 0), W - 1);
+            sI[idx] = __ldg(fr + (long)gy * W + gx);
+        }
+        __syncthreads();
+        // 2. unit gradient at each tap source: Gx read at min(X+1, W-1), Gy at min(Y+1, H-1),
+        //    Roberts cross with max(.-1, 0) clamps (liveSRRF_noInterpolation.cl:144-155, 291-292)
+        for (int idx = tid; idx < L.EW * L.EH; idx += blockDim.x) {
+            const int ey = idx / L.EW, ex = idx - ey * L.EW;
+            const int X = x0 + r0 + ex, Y = y0 + r0 + ey;
+            float2 e = make_float2(0.f, 0.f);
+            if (X >= 0 && X < W && Y >= 0 && Y < H) {
+                const int xa = min(X + 1, W - 1), xa0 = max(xa - 1, 0), ya0 = max(Y - 1, 0);
+                const float ga = sI[(ya0 - gY0) * L.IW + (xa - gX0)];
+                const float gb = sI[(Y - gY0) * L.IW + (xa0 - gX0)];
+                const float gc = sI[(Y - gY0) * L.IW + (xa - gX0)];
+                const float gd = sI[(ya0 - gY0) * L.IW + (xa0 - gX0)];
+                const float Gx = ga - gb + gc - gd;
+                const int yb = min(Y + 1, H - 1), yb0 = max(yb - 1, 0), xb0 = max(X - 1, 0);
+                const float ha = sI[(yb0 - gY0) * L.IW + (X - gX0)];
+                const float hb = sI[(yb - gY0) * L.IW + (xb0 - gX0)];
+                const float hc = sI[(yb - gY0) * L.IW + (X - gX0)];
+                const float hd = sI[(yb0 - gY0) * L.IW + (xb0 - gX0)];
+                const float Gy = -ha + hb + hc - hd;
+                const float n2 = Gx * Gx + Gy * Gy;
+                if (n2 > 0.f) {
+                    const float inv = rsqrtf(n2);
+                    e = make_float2(Gx * inv, Gy * inv);
+                }
+            }
+            sE[idx] = e;
+        }
+        __syncthreads();
+        // 3. tap loop
+        float acc[kK];
+#pragma unroll
+        for (int k = 0; k < kK; ++k) acc[k] = 0.f;
+        for (int ii = 0; ii < S; ++ii) {
+            const float fi = fr0 + (float)ii;
+            float wr[SB], wdr[SB];
+#pragma unroll
+            for (int jj = 0; jj < SB; ++jj) {
+                wr[jj] = jj < S ? sw[jj * S + ii] : 0.f;
+                wdr[jj] = jj < S ? swd[jj * S + ii] : 0.f;
+            }
+            const int lo = sjr[2 * ii];
+            const int hi = min(sjr[2 * ii + 1] + kK - 1, S + kK - 2);
+            const float2* col = sE + (ty * kK) * L.EW + tx + ii;
+#pragma unroll
+            for (int rr = 0; rr < SB + kK - 1; ++rr) {
+                if (rr < lo || rr > hi) continue;
+                const float2 e = col[rr * L.EW];
+                const float fr = fr0 + (float)rr;  // j + k for this source row
+                float dk = fmaf(e.y, fr, e.x * fi);
+                float ck = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+                for (int k = 0; k < kK; ++k) {
+                    const int jj = rr - k;
+                    if (jj >= 0 && jj < SB) {
+                        const float t = fmaf(-fabsf(ck), wdr[jj], wr[jj]);
+                        if (dk < 0.f) acc[k] += t;
+                    }
+                    dk -= e.y;
+                    ck += e.x;
+                }
+            }
+        }
+        // 4. normalisation, sensitivity, intensity weighting and cumulants
+        const int tglob = a.t0 + f;
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int o = (ty * kK + k) * kTX + tx;
+            const float cg = cglh_power(acc[k] / wsum[k], fp.sens);
+            const float v = sI[(ty * kK + k + 1 - r0) * L.IW + (tx + 1 - r0)];
+            const float x = a.int_weighting ? v * cg : cg;
+            const float pv = sst[4 * kTX * kTH + o];
+            sst[0 * kTX * kTH + o] += x;
+            sst[1 * kTX * kTH + o] += x * x;
+            if (tglob > 0) sst[2 * kTX * kTH + o] += x * pv;
+            sst[3 * kTX * kTH + o] += v;
+            sst[4 * kTX * kTH + o] = x;
+        }
+    }
+    // 5. fold this launch's FP32 partial sums into the block's FP64 accumulators
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const int yM = y0 + ty * kK + k;
+        if (xM >= W || yM >= H) continue;
+        const long pix = (long)yM * W + xM;
+        const int o = (ty * kK + k) * kTX + tx;
+        a.st.acc[pix] += (double)sst[0 * kTX * kTH + o];
+        a.st.acc[wh + pix] += (double)sst[1 * kTX * kTH + o];
+        a.st.acc[2 * wh + pix] += (double)sst[2 * kTX * kTH + o];
+        a.st.acc[3 * wh + pix] += (double)sst[3 * kTX * kTH + o];
+        a.st.prev[pix] = sst[4 * kTX * kTH + o];
+    }
+}
+
+template <int SB>
+cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
+                         cudaStream_t stream) {
+    const FusedSmem L = fused_smem_layout(g.S);
+    cudaError_t e = cudaFuncSetAttribute(fht_rgc_fused_kernel<SB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
+    if (e != cudaSuccess) return e;
+    FusedParams fp{g.r0, g.S, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
+    dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
+    fht_rgc_fused_kernel<SB><<<grid, 256, L.bytes, stream>>>(a, fp);
+    return cudaGetLastError();
+}
+
+__global__ void finalize_kernel(BlockState st, int n, int tac_div2, float* __restrict__ out) {
+    const long pix = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long P = st.pixels;
+    if (pix >= P) return;
+    const double avg = st.acc[pix] / n;
+    const double av2 = avg * avg;
+    double tac = 0.0;
+    if (n > 1) {
+        tac = st.acc[2 * P + pix] / (n - 1);
+        if (tac_div2) tac /= (n - 1);
+    }
+    float o[4] = {(float)avg, (float)(st.acc[P + pix] / n - av2), (float)(tac - av2),
+                  (float)(st.acc[3 * P + pix] / n)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k * P + pix] = isnan(o[k]) ? 0.f : o[k];
+}
+
+}  // namespace
+
+cudaError_t fht_robx(const float* interp, int W, int H, int F, float* gx, float* gy,
+                     cudaStream_t stream) {
+    dim3 grid((W + 127) / 128, H, F);
+    robx_kernel<<<grid, 128, 0, stream>>>(interp, W, H, (long)W * H, gx, gy);
+    return cudaGetLastError();
+}
+
+cudaError_t fht_rgc_plain(const FhtGeometry& g, const FhtRgcArgs& a, cudaStream_t stream) {
+    PlainParams pp{g.tSS, g.tSO, g.radius, g.sensitivity};
+    const long wh = (long)a.W * a.H;
+    fht_rgc_plain_kernel<<<(unsigned)((wh + 255) / 256), 256, 0, stream>>>(a, pp);
+    return cudaGetLastError();
+}
+
+cudaError_t fht_fused_tables(const FhtGeometry& g, int W, int H, FhtFusedTables& t,
+                             cudaStream_t stream) {
+    cudaError_t e;
+    const int S = g.S;
+    std::vector<int> jr(2 * S);
+    for (int ii = 0; ii < S; ++ii) {
+        jr[2 * ii] = g.jlo[ii];
+        jr[2 * ii + 1] = g.jhi[ii];
+    }
+    if ((e = cudaMalloc(&t.wtab, sizeof(float) * S * S)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&t.wdtab, sizeof(float) * S * S)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&t.jrange, sizeof(int) * 2 * S)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&t.wsum, sizeof(float) * (size_t)W * H)) != cudaSuccess) return e;
+    cudaMemcpyAsync(t.wtab, g.w.data(), sizeof(float) * S * S, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(t.wdtab, g.wd.data(), sizeof(float) * S * S, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(t.jrange, jr.data(), sizeof(int) * 2 * S, cudaMemcpyHostToDevice, stream);
+    const long wh = (long)W * H;
+    wsum_kernel<<<(unsigned)((wh + 255) / 256), 256, 0, stream>>>(t.wtab, g.r0, S, W, H, t.wsum);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(stream);  // host tables above are stack temporaries
+}
+
+void fht_fused_tables_free(FhtFusedTables& t) {
+    cudaFree(t.wtab);
+    cudaFree(t.wdtab);
+    cudaFree(t.jrange);
+    cudaFree(t.wsum);
+    t = FhtFusedTables();
+}
+
+cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
+                          cudaStream_t stream) {
+    if (g.S <= 12) return launch_fused<12>(g, t, a, stream);
+    if (g.S <= 18) return launch_fused<18>(g, t, a, stream);
+    if (g.S <= 24) return launch_fused<24>(g, t, a, stream);
+    if (g.S <= 32) return launch_fused<32>(g, t, a, stream);
+    return cudaErrorInvalidValue;  // caller falls back to the plain kernel
+}
+
+cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out,
+                           cudaStream_t stream) {
+    finalize_kernel<<<(unsigned)((st.pixels + 255) / 256), 256, 0, stream>>>(st, n, tac_div2, out);
+    return cudaGetLastError();
+}
+
+cudaError_t zero_block(BlockState& st, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(st.acc, 0, sizeof(double) * 4 * st.pixels, stream);
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(st.prev, 0, sizeof(float) * st.pixels, stream);
+}
+
+}  // namespace esrrf

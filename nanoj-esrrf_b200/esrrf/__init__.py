@@ -1,0 +1,228 @@
+"""Python front end of libesrrf, the B200 eSRRF engine.
+
+``LiveSRRF_CL`` mirrors the reference's device-engine class nanoj.liveSRRF.LiveSRRF_CL
+(src/nanoj/liveSRRF/LiveSRRF_CL.java) member for member, over the C ABI in include/esrrf.h, so
+that code written against the Fiji plugin's engine reads the same here.  ``esrrf_stack`` is a
+one-call functional form used by the benchmark and the parity tests.
+
+There is no CPU fallback: importing this package on a machine without the built library raises,
+and every call that reaches the GPU raises ``EsrrfError`` on failure.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import EsrrfError, EsrrfParams, lib
+
+__all__ = ["LiveSRRF_CL", "EsrrfError", "EsrrfParams", "esrrf_stack", "lib", "default_params"]
+
+# Keys of the 3-D calibration table that LiveSRRF_CL.initialise reads (LiveSRRF_CL.java:212-220).
+CALIB_KEYS = ("X-shift (pixels)", "Y-shift (pixels)", "Theta (degrees)", "Axial positions",
+              "ROI #", "Intensity scaling", "Background level (ADC)")
+
+
+def default_params() -> EsrrfParams:
+    p = EsrrfParams()
+    lib().esrrf_default_params(ctypes.byref(p))
+    return p
+
+
+class LiveSRRF_CL:
+    """Mirror of nanoj.liveSRRF.LiveSRRF_CL over libesrrf (one CUDA stream per instance)."""
+
+    nReconstructions = 3  # AVG, VAR, TAC2 (LiveSRRF_CL.java:51)
+    gradientMag = 2       # 2x gradient grid of the bicubic paths (LiveSRRF_CL.java:45)
+
+    def __init__(self, DEBUG: bool = False):
+        self.DEBUG = DEBUG
+        self._h = ctypes.c_void_p()
+        self._keep = []
+        self.allCLdevices: list[str] = []
+        self.imsSRRF: np.ndarray | None = None
+        self.widthS = self.heightS = 0
+        self.nPlanes = self.nPlanesM = 1
+        self._shape = None
+
+    # -- LiveSRRF_CL.checkDevices (LiveSRRF_CL.java:111-155)
+    def checkDevices(self) -> list[str]:
+        n = ctypes.c_int(0)
+        lib().esrrf_device_count(ctypes.byref(n))
+        names = []
+        for d in range(n.value):
+            buf = ctypes.create_string_buffer(256)
+            sms, clk = ctypes.c_int(), ctypes.c_int()
+            _lib.check(None, lib().esrrf_device_info(d, buf, 256, ctypes.byref(sms),
+                                                     ctypes.byref(clk)))
+            names.append(buf.value.decode())
+        self.allCLdevices = names
+        return names
+
+    # -- LiveSRRF_CL.initialise (LiveSRRF_CL.java:159-264)
+    def initialise(self, width, height, magnification, fwhm, sensitivity, nFramesOnGPU,
+                   nFrameForSRRF, blockLength=20000, chosenDevice=None, intWeighting=True,
+                   doMPmapCorrection=False, doFHTinterpolation=True, calibTable3DSRRF=None,
+                   axialOffset=0.0, pixelSize=0.1, kernel="fused", framesPerLaunch=0,
+                   fhtScale="mean_preserving"):
+        """Same arguments as the reference.  ``calibTable3DSRRF`` replaces the .njt path: a
+        mapping with the table's keys (CALIB_KEYS); ``None`` means 2-D."""
+        self.release()
+        p = default_params()
+        p.width, p.height = int(width), int(height)
+        p.magnification = int(magnification)
+        p.fwhm = float(fwhm)
+        p.sensitivity = int(sensitivity)
+        p.n_frames_on_gpu = int(nFramesOnGPU)
+        p.n_frame_for_srrf = int(nFrameForSRRF)
+        p.block_length = int(blockLength)
+        p.device = -1 if chosenDevice is None else int(chosenDevice)
+        p.int_weighting = int(bool(intWeighting))
+        p.mp_correction = int(bool(doMPmapCorrection))
+        p.interp = 0 if doFHTinterpolation else 1
+        p.fht_scale = {"mean_preserving": 0, "unitary_big": 1}[fhtScale]
+        p.kernel = {"fused": 0, "plain": 1}[kernel]
+        p.frames_per_launch = int(framesPerLaunch)
+        p.axial_offset_nm = float(axialOffset)
+        p.pixel_size_um = float(pixelSize)
+        self._keep = []
+        if calibTable3DSRRF is not None:
+            t = calibTable3DSRRF
+            arrs = {k: np.ascontiguousarray(np.asarray(t[k], np.float32)) for k in CALIB_KEYS
+                    if k in t}
+            n_planes = len(arrs["X-shift (pixels)"])
+            p.n_planes = n_planes
+            fptr = ctypes.POINTER(ctypes.c_float)
+            p.roi = arrs["ROI #"].ctypes.data_as(fptr)
+            p.theta_deg = arrs["Theta (degrees)"].ctypes.data_as(fptr)
+            p.shift_x = arrs["X-shift (pixels)"].ctypes.data_as(fptr)
+            p.shift_y = arrs["Y-shift (pixels)"].ctypes.data_as(fptr)
+            p.intensity_coeff = arrs["Intensity scaling"].ctypes.data_as(fptr)
+            p.background = float(arrs["Background level (ADC)"][0])
+            self._keep = list(arrs.values())
+        h = ctypes.c_void_p()
+        _lib.check(None, lib().esrrf_create(ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self._params = p
+        wm, hm, pm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(h, lib().esrrf_output_shape(h, ctypes.byref(wm), ctypes.byref(hm),
+                                               ctypes.byref(pm)))
+        self._shape = (wm.value, hm.value, pm.value)
+        M = int(magnification)
+        self.widthS, self.heightS = wm.value // M, hm.value // M
+        self.nPlanesM = pm.value
+        self.nPlanes = max(1, pm.value // M) if calibTable3DSRRF is not None else 1
+
+    # -- LiveSRRF_CL.loadDriftXYGPUbuffer (LiveSRRF_CL.java:583-595)
+    def loadDriftXYGPUbuffer(self, driftX, driftY):
+        dx = np.ascontiguousarray(driftX, np.float32)
+        dy = np.ascontiguousarray(driftY, np.float32)
+        fptr = ctypes.POINTER(ctypes.c_float)
+        _lib.check(self._h, lib().esrrf_set_drift(self._h, dx.ctypes.data_as(fptr),
+                                                  dy.ctypes.data_as(fptr), len(dx)))
+
+    # -- LiveSRRF_CL.resetFramePosition (LiveSRRF_CL.java:955-960)
+    def resetFramePosition(self):
+        _lib.check(self._h, lib().esrrf_reset_frame_position(self._h))
+
+    # -- LiveSRRF_CL.calculateSRRF (LiveSRRF_CL.java:636-746); True if cancelled
+    def calculateSRRF(self, imsRawData) -> bool:
+        a = np.asarray(imsRawData)
+        if a.dtype == np.uint16:
+            a = np.ascontiguousarray(a)
+            rc = lib().esrrf_calculate_srrf_u16(self._h, a.ctypes.data_as(ctypes.c_void_p),
+                                                a.shape[0])
+        else:
+            a = np.ascontiguousarray(a, np.float32)
+            rc = lib().esrrf_calculate_srrf_f32(self._h, a.ctypes.data_as(ctypes.c_void_p),
+                                                a.shape[0])
+        if rc == 1:
+            return True
+        _lib.check(self._h, rc)
+        return False
+
+    # -- LiveSRRF_CL.readSRRFbuffer (LiveSRRF_CL.java:749-794)
+    def readSRRFbuffer(self):
+        wm, hm, pm = self._shape
+        out = np.empty((4 * pm, hm, wm), np.float32)
+        _lib.check(self._h, lib().esrrf_read_srrf(self._h, out.ctypes.data_as(ctypes.c_void_p)))
+        self.imsSRRF = out
+        return out
+
+    # -- LiveSRRF_CL.readGradientBuffers (LiveSRRF_CL.java:797-879)
+    def readGradientBuffers(self):
+        wm, hm, pm = self._shape
+        out = np.empty((2, hm, wm), np.float32)
+        _lib.check(self._h, lib().esrrf_read_gradients(self._h, out.ctypes.data_as(ctypes.c_void_p),
+                                                       ctypes.c_size_t(out.size)))
+        return out
+
+    # -- LiveSRRF_CL.finishQueue (LiveSRRF_CL.java:1009-1015)
+    def finishQueue(self):
+        _lib.check(self._h, lib().esrrf_finish_queue(self._h))
+
+    def requestCancel(self):
+        """Thread-safe counterpart of the reference's Escape-key polling."""
+        _lib.check(self._h, lib().esrrf_request_cancel(self._h))
+
+    def lastTiming(self):
+        i, r, n = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+        _lib.check(self._h, lib().esrrf_last_timing(self._h, ctypes.byref(i), ctypes.byref(r),
+                                                    ctypes.byref(n)))
+        return i.value, r.value, n.value
+
+    def setStream(self, stream_ptr):
+        """Run on a caller-owned cudaStream_t (an int pointer value); None restores a private one."""
+        _lib.check(self._h, lib().esrrf_set_stream(self._h, ctypes.c_void_p(stream_ptr or None)))
+
+    def setTiming(self, on: bool):
+        _lib.check(self._h, lib().esrrf_set_timing(self._h, int(bool(on))))
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- LiveSRRF_CL.release (LiveSRRF_CL.java:939-951)
+    def release(self):
+        if self._h:
+            lib().esrrf_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def esrrf_stack(stack, magnification, fwhm, sensitivity, frames_per_block=None, gap=None,
+                int_weighting=True, mp_correction=False, fht=True, drift=None, kernel="fused",
+                frames_per_launch=0, calib3d=None, n_frames_on_gpu=None):
+    """Rolling eSRRF over a stack, the loop of LiveSRRF_optimised_.run
+    (gui/LiveSRRF_optimised_.java:276-389): blocks of ``frames_per_block`` frames starting every
+    ``gap`` frames; returns [blocks][4*planesM][HM][WM] (AVG, VAR, TAC2, INT)."""
+    a = np.asarray(stack)
+    n = a.shape[0]
+    nf = n if frames_per_block is None else min(n, int(frames_per_block))
+    gap = nf if gap is None else int(gap)
+    n_blocks = int((n - nf) / gap) + 1
+    h, w = a.shape[-2], a.shape[-1]
+    eng = LiveSRRF_CL()
+    eng.initialise(w, h, magnification, fwhm, sensitivity, n_frames_on_gpu or nf, nf,
+                   intWeighting=int_weighting, doMPmapCorrection=mp_correction,
+                   doFHTinterpolation=fht, calibTable3DSRRF=calib3d, kernel=kernel,
+                   framesPerLaunch=frames_per_launch)
+    outs = []
+    try:
+        for r in range(n_blocks):
+            eng.resetFramePosition()
+            if drift is not None:
+                eng.loadDriftXYGPUbuffer(drift[0][r * gap:r * gap + nf], drift[1][r * gap:r * gap + nf])
+            if eng.calculateSRRF(a[r * gap:r * gap + nf]):
+                raise EsrrfError("cancelled")
+            outs.append(eng.readSRRFbuffer().copy())
+    finally:
+        eng.release()
+    return np.stack(outs)

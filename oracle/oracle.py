@@ -199,3 +199,45 @@ def ref_3d_block(planes, magnification, fwhm, sensitivity, theta_deg, shift_x, s
                               _ptr(_f32(drift_x)), _ptr(_f32(drift_y)), _ptr(out)),
            "ref_3d_block")
     return out
+
+
+# ------------------------------------------------------------------ FFT form of the interpolation
+
+
+def _mirror_src(c, n, out_dim):
+    scale = int(np.ceil(out_dim / n))
+    if scale % 2 == 0:
+        scale += 1
+    roi = (scale * n - out_dim) // 2
+    pos = c + roi
+    tile = pos // n
+    i = pos - tile * n
+    rel = tile - (scale - 1) // 2
+    return i if rel % 2 == 0 else n - 1 - i
+
+
+def fht_interpolate_fft(raw, magnification: int, scale_mode: int = 0) -> np.ndarray:
+    """Same map as ``fht_interpolate`` (FourierInterpolation.java:12-73) evaluated with numpy's
+    FFT: DHT = Re(F) - Im(F) of the 2-D DFT, spectral remap, inverse DHT on the magnified canvas.
+    Used where the definition-based form is too slow (the bench's CPU baseline)."""
+    raw = np.asarray(raw, np.float64)
+    n, h, w = raw.shape
+    M = magnification
+    N = max(1 << int(np.ceil(np.log2(w))), 1 << int(np.ceil(np.log2(h))))
+    NM = N * M
+    WM, HM = w * M, h * M
+    xroi, yroi = (NM - WM) // 2, (NM - HM) // 2
+    sx = np.array([_mirror_src(c, w, N) for c in range(N)])
+    sy = np.array([_mirror_src(c, h, N) for c in range(N)])
+    kmap = np.array([p if p < N // 2 else p + (M - 1) * N for p in range(N)])
+    s = 1.0 / (N * N) if scale_mode == 0 else 1.0 / (NM * NM)
+    out = np.empty((n, HM, WM), np.float32)
+    for f in range(n):
+        X = raw[f][sy][:, sx]
+        F = np.fft.fft2(X)
+        Hs = F.real - F.imag
+        big = np.zeros((NM, NM))
+        big[np.ix_(kmap, kmap)] = Hs
+        G = np.fft.fft2(big)
+        out[f] = ((G.real - G.imag) * s)[yroi:yroi + HM, xroi:xroi + WM]
+    return out

@@ -1,0 +1,92 @@
+"""CPU tests of the C ABI: the library loads, exports every symbol include/esrrf.h declares,
+and the ctypes view of esrrf_params matches the C layout.  No GPU work is done."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "esrrf.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(esrrf_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(esrrf_mod):
+    from esrrf import _lib
+    L = esrrf_mod.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+        assert n in _lib.SIGNATURES, f"{n} has no ctypes signature"
+
+
+def test_params_layout_matches_c():
+    from esrrf import EsrrfParams
+    fields = [f for f, _ in EsrrfParams._fields_]
+    prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"esrrf.h\"\nint main(){"
+    prog += 'printf("%zu\\n", sizeof(esrrf_params));'
+    for f in fields:
+        prog += f'printf("%zu\\n", offsetof(esrrf_params, {f}));'
+    prog += "return 0;}"
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(prog)
+        subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
+        vals = [int(x) for x in subprocess.run([exe], capture_output=True, text=True,
+                                               check=True).stdout.split()]
+    assert vals[0] == ctypes.sizeof(EsrrfParams)
+    for f, off in zip(fields, vals[1:]):
+        assert getattr(EsrrfParams, f).offset == off, f
+
+
+def test_version_and_defaults(esrrf_mod):
+    L = esrrf_mod.lib()
+    assert L.esrrf_get_version().decode().startswith("0.")
+    p = esrrf_mod.default_params()
+    # reference GUI defaults (gui/LiveSRRF_optimised_.java:128-134)
+    assert (p.magnification, p.sensitivity, p.n_frame_for_srrf, p.block_length) == (5, 1, 100, 20000)
+    assert abs(p.fwhm - 2.0) < 1e-6 and p.int_weighting == 1 and p.interp == 0
+
+
+def test_invalid_parameters_are_rejected_before_device_work(esrrf_mod):
+    """Parameter validation runs on the host and reports through esrrf_last_error(NULL)."""
+    L = esrrf_mod.lib()
+    p = esrrf_mod.default_params()
+    p.width, p.height = 2, 64
+    h = ctypes.c_void_p()
+    rc = L.esrrf_create(ctypes.byref(p), ctypes.byref(h))
+    assert rc == -1 and not h.value
+    assert b"width" in L.esrrf_last_error(None)
+    p.width, p.height, p.magnification = 64, 64, 0
+    assert L.esrrf_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    p.magnification, p.n_frame_for_srrf = 4, 0
+    assert L.esrrf_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    p.n_frame_for_srrf, p.n_planes = 10, 3  # 3-D without calibration arrays
+    assert L.esrrf_create(ctypes.byref(p), ctypes.byref(h)) == -1
+
+
+def test_null_handles_are_rejected(esrrf_mod):
+    L = esrrf_mod.lib()
+    assert L.esrrf_destroy(None) == -1
+    assert L.esrrf_reset_frame_position(None) == -1
+    assert L.esrrf_read_srrf(None, None) == -1
+    assert L.esrrf_request_cancel(None) == -1
+
+
+def test_no_cpu_fallback_without_library(monkeypatch):
+    """The package fails loudly when the CUDA library is missing."""
+    from esrrf import _lib
+    monkeypatch.setattr(_lib, "_LIB", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", "/nonexistent/libesrrf.so")
+    with pytest.raises(_lib.EsrrfError):
+        _lib.lib()

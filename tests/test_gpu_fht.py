@@ -1,0 +1,125 @@
+"""GPU parity tests of the 2-D FHT path (liveSRRF_noInterpolation.cl semantics) through the C ABI.
+
+Tolerance: every output slice (AVG, VAR, TAC2, INT) must agree with the oracle within 1e-4 of
+that slice's dynamic range (max - min), the bar the engine is specified to.  The oracle is the
+FP32 restatement, itself pinned bit-exactly to the reference kernels by tests/test_oracle.py.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def run_engine(esrrf, frames, M, fwhm, S, intw=True, kernel="fused", drift=None,
+               frames_per_launch=0, block=None, chunks=None):
+    eng = esrrf.LiveSRRF_CL()
+    n = frames.shape[0] if block is None else block
+    eng.initialise(frames.shape[-1], frames.shape[-2], M, fwhm, S, n, n, intWeighting=intw,
+                   kernel=kernel, framesPerLaunch=frames_per_launch)
+    try:
+        eng.resetFramePosition()
+        if drift is not None:
+            eng.loadDriftXYGPUbuffer(*drift)
+        if chunks is None:
+            assert not eng.calculateSRRF(frames)
+        else:
+            s = 0
+            for c in chunks:
+                assert not eng.calculateSRRF(frames[s:s + c])
+                s += c
+        return eng.readSRRFbuffer().copy()
+    finally:
+        eng.release()
+
+
+def assert_close(got, ref, tol=TOL, what=""):
+    for k in range(4):
+        e = rel_err(got[k], ref[k])
+        assert e < tol, f"{what} slice {k}: {e:.3g} of range"
+
+
+@pytest.mark.parametrize("kernel", ["fused", "plain"])
+@pytest.mark.parametrize("name", golden_names("fht"))
+def test_fht_golden(esrrf_mod, name, kernel):
+    g = load_golden(name)
+    drift = (g["drift_x"], g["drift_y"]) if "drift_x" in g else None
+    got = run_engine(esrrf_mod, g["raw"], int(g["magnification"]), float(g["fwhm"]),
+                     int(g["sensitivity"]), bool(g["int_weighting"]), kernel=kernel, drift=drift)
+    assert_close(got, g["out"], what=f"{name}/{kernel}")
+
+
+def test_fht_u16_input_and_chunked_pushes(esrrf_mod, oracle_mod):
+    """uint16 frames pushed in uneven GPU loads give the same block as one float push."""
+    from esrrf import synth
+    raw = synth.small_stack(21, 13, 32, 32)
+    ref = oracle_mod.fht_block(oracle_mod.fht_interpolate(raw.astype(np.float32), 4), 4, 1.5, 2)
+    got = run_engine(esrrf_mod, raw, 4, 1.5, 2, chunks=[5, 1, 7], frames_per_launch=3)
+    assert_close(got, ref, what="u16 chunked")
+    got2 = run_engine(esrrf_mod, raw.astype(np.float32), 4, 1.5, 2)
+    assert_close(got2, ref, what="f32 single push")
+
+
+def test_fht_workload_fht64_subset(esrrf_mod, oracle_mod):
+    """The 64x64, M5, radius 1.5, S1 workload on its first 20 frames, fused and plain."""
+    from esrrf import synth
+    raw = synth.make_stack("fht64", frames=20)
+    ref = oracle_mod.fht_block(oracle_mod.fht_interpolate(raw.astype(np.float32), 5), 5, 1.5, 1)
+    for kernel in ("fused", "plain"):
+        got = run_engine(esrrf_mod, raw, 5, 1.5, 1, kernel=kernel)
+        assert_close(got, ref, what=f"fht64/{kernel}")
+
+
+def test_fht_mirror_padded_non_square(esrrf_mod, oracle_mod):
+    from esrrf import synth
+    raw = synth.small_stack(22, 6, 20, 28).astype(np.float32)
+    ref = oracle_mod.fht_block(oracle_mod.fht_interpolate(raw, 3), 3, 2.0, 1)
+    got = run_engine(esrrf_mod, raw, 3, 2.0, 1)
+    assert_close(got, ref, what="non-square")
+
+
+@pytest.mark.parametrize("fwhm,M", [(0.5, 2), (1.0, 4), (2.5, 2), (3.0, 4)])
+def test_fht_radius_range(esrrf_mod, oracle_mod, fwhm, M):
+    """Radii of the parameter sweep (tap boxes from 6 to 26 wide) on both kernels."""
+    from esrrf import synth
+    raw = synth.small_stack(23, 5, 24, 24).astype(np.float32)
+    ref = oracle_mod.fht_block(oracle_mod.fht_interpolate(raw, M), M, fwhm, 2)
+    for kernel in ("fused", "plain"):
+        got = run_engine(esrrf_mod, raw, M, fwhm, 2, kernel=kernel)
+        assert_close(got, ref, what=f"r{fwhm} M{M} {kernel}")
+
+
+def test_intensity_scaling_property_full_size(esrrf_mod):
+    """Size-independent property at the 512x512, M4 workload size: CGLH does not depend on the
+    intensity scale, so scaling the frames by c scales AVG, INT by c and VAR, TAC2 by c^2."""
+    from esrrf import synth
+    raw = synth.make_stack("fht512", frames=12).astype(np.float32)
+    a = run_engine(esrrf_mod, raw, 4, 1.5, 2)
+    b = run_engine(esrrf_mod, raw * 2.0, 4, 1.5, 2)
+    for k, p in zip(range(4), (1, 2, 2, 1)):
+        assert rel_err(b[k], a[k] * 2.0 ** p) < TOL, k
+
+
+def test_constant_frames_full_size(esrrf_mod):
+    c = np.full((4, 512, 512), 300, np.uint16)
+    out = run_engine(esrrf_mod, c, 4, 1.5, 2)
+    assert np.abs(out[:3]).max() == 0.0
+    np.testing.assert_allclose(out[3], 300.0, rtol=1e-5)
+
+
+def test_block_overflow_and_cancel(esrrf_mod):
+    from esrrf import EsrrfError, synth
+    raw = synth.small_stack(24, 6, 16, 16)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(16, 16, 2, 1.5, 1, 4, 4)
+    try:
+        eng.resetFramePosition()
+        with pytest.raises(EsrrfError):
+            eng.calculateSRRF(raw)  # 6 frames into a 4-frame block
+        eng.resetFramePosition()
+        eng.requestCancel()
+        assert eng.calculateSRRF(raw[:4]) is True
+    finally:
+        eng.release()
