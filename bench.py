@@ -220,7 +220,9 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     name, nf = WORKLOADS[args.workload]
     wl = synth.WORKLOADS[name]
-    stack = synth.make_stack(name)
+    stack = synth.make_stack(name, frames=args.frames)
+    if args.block:
+        nf = args.block
     n, h, w = stack.shape
     M, fwhm, S = wl.magnification, wl.fwhm, wl.sensitivity
     n_blocks = n // nf
@@ -326,7 +328,7 @@ def run_ours(args, world, rank, local):
         "value": value, "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1000.0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: 512x512x500 uint16, M4, radius 1.5, S2, "
+        "config": {"workload": f"{args.workload}: {w}x{h}x{n} uint16, M{M}, radius {fwhm}, S{S}, "
                                f"AVG+VAR+TAC2+INT, blocks of {nf}", "kernel": args.kernel,
                    "frames_per_launch": F, "l2": "inputs (262 MB) larger than L2",
                    "parallelism": f"replicas x{world}"},
@@ -359,6 +361,9 @@ def main():
     ap.add_argument("--kernel", default="fused", choices=["fused", "plain"])
     ap.add_argument("--frames-per-launch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--frames", type=int, default=None,
+                    help="shorter stack (profiling runs); default: the workload's length")
+    ap.add_argument("--block", type=int, default=0, help="frames per block override")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
