@@ -168,6 +168,28 @@ esrrf_status esrrf_set_timing(esrrf_handle* h, int enable);
 esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* rgc_ms,
                                int* launches);
 
+/* Allocation-free variant of one FHT-path SR block; it has no counterpart in the reference.
+ * For callers that must not allocate device memory when they reconstruct -- e.g. a
+ * live-acquisition callback, where cudaMalloc/cudaFree can synchronise the device and stall
+ * the camera stream, or a host that owns every device byte through its own pool.  It computes
+ * what esrrf_create + esrrf_calculate_srrf_*_device + esrrf_read_srrf_device compute for one
+ * block (FHT interpolation, mean-preserving scale, zero drift, fused RGC, FP64 cumulants) and
+ * takes every temporary buffer from one 64 MiB static device array that each GPU loading the
+ * library holds until exit; frame sizes whose tables, buffers and accumulators need more than
+ * that (roughly widthM x heightM above 1.3 M pixels) are rejected with ESRRF_ERR_INVALID, as
+ * are radii whose tap box exceeds 32 magnified pixels.
+ * d_frames: device [n_frames][height][width], uint16 (is_u16 = 1) or float.  d_out: device
+ * [4][height*M][width*M] float (AVG, VAR, TAC2, INT).  stream: cudaStream_t or NULL; the call
+ * only enqueues work on it.  err/err_len: optional buffer for a message on failure.
+ * The first call on a device looks up the array's address (cudaGetSymbolAddress, with that
+ * device current) -- make it before any stream capture.  Calls share the array and it keeps
+ * the last call's contents (the accumulators are cleared at the start of each call); calls
+ * whose work overlaps on the GPU race on it. */
+esrrf_status esrrf_fht_block_noalloc(const void* d_frames, int is_u16, int n_frames, int width,
+                                     int height, int magnification, float fwhm, int sensitivity,
+                                     int int_weighting, float* d_out, void* stream, char* err,
+                                     size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

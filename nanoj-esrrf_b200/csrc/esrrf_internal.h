@@ -114,4 +114,11 @@ cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out
                            cudaStream_t stream);
 cudaError_t zero_block(BlockState& st, cudaStream_t stream);
 
+// Variants of the table set-up that place their tables in caller-provided device memory (no
+// allocation); used by the allocation-free entry point.
+cudaError_t interp_plan_place(InterpPlan& plan, int w, int h, int M, int scale_mode,
+                              unsigned char* base, size_t* bytes, cudaStream_t stream);
+cudaError_t fht_fused_tables_place(const FhtGeometry& g, int W, int H, FhtFusedTables& t,
+                                   unsigned char* base, size_t* bytes, cudaStream_t stream);
+
 }  // namespace esrrf

@@ -399,3 +399,93 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
 }
 
 }  // namespace esrrf
+
+namespace esrrf {
+
+// Same tables as interp_plan_create, laid out in caller-provided device memory from `base`
+// (each piece 256-byte aligned) instead of fresh allocations.  With base == nullptr only the
+// byte count is computed.  Host tables are staged by pageable cudaMemcpyAsync on `stream`,
+// which copies them out before returning.
+cudaError_t interp_plan_place(InterpPlan& p, int w, int h, int M, int scale_mode,
+                              unsigned char* base, size_t* bytes, cudaStream_t stream) {
+    p.w = w;
+    p.h = h;
+    p.M = M;
+    p.N = std::max(pow2_ceil_java(w), pow2_ceil_java(h));
+    const int N = p.N;
+    const long NM = (long)N * M;
+    p.WM = w * M;
+    p.HM = h * M;
+    p.xroi = (int)((NM - p.WM) / 2);
+    p.yroi = (int)((NM - p.HM) / 2);
+    p.identity_pad = (w == N && h == N);
+    p.s_axis = scale_mode == 0 ? 1.0 / N : 1.0 / (double)NM;
+    p.s = p.s_axis * p.s_axis;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t n_dxT = (size_t)N * p.WM, n_dy = (size_t)p.HM * N;
+    size_t off = 0;
+    const size_t o_dxT = off; off += al(sizeof(float) * n_dxT);
+    const size_t o_dy = off;  off += al(sizeof(float) * n_dy);
+    const size_t o_dyT = off; off += al(sizeof(float) * n_dy);
+    const size_t o_cx = off;  off += al(sizeof(float) * p.WM);
+    const size_t o_ux = off;  off += al(sizeof(float) * p.WM);
+    const size_t o_cy = off;  off += al(sizeof(float) * p.HM);
+    const size_t o_uy = off;  off += al(sizeof(float) * p.HM);
+    const size_t o_sx = off;  off += al(sizeof(int) * N);
+    const size_t o_sy = off;  off += al(sizeof(int) * N);
+    *bytes = off;
+    if (!base) return cudaSuccess;
+    p.dxT = (float*)(base + o_dxT);
+    p.dy = (float*)(base + o_dy);
+    p.dyT = (float*)(base + o_dyT);
+    p.cx = (float*)(base + o_cx);
+    p.ux = (float*)(base + o_ux);
+    p.cy = (float*)(base + o_cy);
+    p.uy = (float*)(base + o_uy);
+    p.srcx = (int*)(base + o_sx);
+    p.srcy = (int*)(base + o_sy);
+    std::vector<int> sx(N), sy(N);
+    for (int c = 0; c < N; ++c) {
+        sx[c] = mirror_src(c, w, N);
+        sy[c] = mirror_src(c, h, N);
+    }
+    std::vector<float> dxT(n_dxT), dy(n_dy), dyT(n_dy);
+    for (int n = 0; n < p.WM; ++n)
+        for (int m = 0; m < N; ++m) {
+            long j = ((long)m * M - (n + p.xroi)) % NM;
+            if (j < 0) j += NM;
+            dxT[(size_t)m * p.WM + n] = (float)(dirichlet(j, N, NM) * p.s_axis);
+        }
+    for (int n = 0; n < p.HM; ++n)
+        for (int m = 0; m < N; ++m) {
+            long j = ((long)m * M - (n + p.yroi)) % NM;
+            if (j < 0) j += NM;
+            const float v = (float)(dirichlet(j, N, NM) * p.s_axis);
+            dy[(size_t)n * N + m] = v;
+            dyT[(size_t)m * p.HM + n] = v;
+        }
+    std::vector<float> cx(p.WM), ux(p.WM), cy(p.HM), uy(p.HM);
+    for (int n = 0; n < p.WM; ++n) {
+        const double a = M_PI * (double)(n + p.xroi) / M;
+        cx[n] = (float)std::cos(a);
+        ux[n] = (float)std::sin(a);
+    }
+    for (int n = 0; n < p.HM; ++n) {
+        const double a = M_PI * (double)(n + p.yroi) / M;
+        cy[n] = (float)std::cos(a);
+        uy[n] = (float)std::sin(a);
+    }
+    cudaError_t e;
+    const cudaMemcpyKind k = cudaMemcpyHostToDevice;
+    if ((e = cudaMemcpyAsync(p.dxT, dxT.data(), sizeof(float) * n_dxT, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.dy, dy.data(), sizeof(float) * n_dy, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.dyT, dyT.data(), sizeof(float) * n_dy, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.cx, cx.data(), sizeof(float) * p.WM, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.ux, ux.data(), sizeof(float) * p.WM, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.cy, cy.data(), sizeof(float) * p.HM, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.uy, uy.data(), sizeof(float) * p.HM, k, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(p.srcx, sx.data(), sizeof(int) * N, k, stream)) != cudaSuccess) return e;
+    return cudaMemcpyAsync(p.srcy, sy.data(), sizeof(int) * N, k, stream);
+}
+
+}  // namespace esrrf

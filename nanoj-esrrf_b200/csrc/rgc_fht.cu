@@ -512,3 +512,38 @@ cudaError_t zero_block(BlockState& st, cudaStream_t stream) {
 }
 
 }  // namespace esrrf
+
+namespace esrrf {
+
+// Same tables as fht_fused_tables, laid out in caller-provided device memory from `base` (each
+// piece 256-byte aligned).  With base == nullptr only the byte count is computed.
+cudaError_t fht_fused_tables_place(const FhtGeometry& g, int W, int H, FhtFusedTables& t,
+                                   unsigned char* base, size_t* bytes, cudaStream_t stream) {
+    const int S = g.S;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    size_t off = 0;
+    const size_t o_w = off;  off += al(sizeof(float) * S * S);
+    const size_t o_wd = off; off += al(sizeof(float) * S * S);
+    const size_t o_jr = off; off += al(sizeof(int) * 2 * S);
+    const size_t o_ws = off; off += al(sizeof(float) * (size_t)W * H);
+    *bytes = off;
+    if (!base) return cudaSuccess;
+    t.wtab = (float*)(base + o_w);
+    t.wdtab = (float*)(base + o_wd);
+    t.jrange = (int*)(base + o_jr);
+    t.wsum = (float*)(base + o_ws);
+    std::vector<int> jr(2 * S);
+    for (int ii = 0; ii < S; ++ii) {
+        jr[2 * ii] = g.jlo[ii];
+        jr[2 * ii + 1] = g.jhi[ii];
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(t.wtab, g.w.data(), sizeof(float) * S * S, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(t.wdtab, g.wd.data(), sizeof(float) * S * S, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(t.jrange, jr.data(), sizeof(int) * 2 * S, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    const long wh = (long)W * H;
+    wsum_kernel<<<(unsigned)((wh + 255) / 256), 256, 0, stream>>>(t.wtab, g.r0, S, W, H, t.wsum);
+    return cudaGetLastError();
+}
+
+}  // namespace esrrf

@@ -72,6 +72,9 @@ SIGNATURES = {
     "esrrf_set_stream": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
     "esrrf_last_timing": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_float), _c.POINTER(_c.c_float),
                                      _c.POINTER(_c.c_int)]),
+    "esrrf_fht_block_noalloc": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int, _c.c_int,
+                                           _c.c_int, _c.c_float, _c.c_int, _c.c_int, _c.c_void_p,
+                                           _c.c_void_p, _c.c_char_p, _c.c_size_t]),
 }
 
 _LIB = None
