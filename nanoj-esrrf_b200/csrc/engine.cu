@@ -130,7 +130,7 @@ esrrf_status esrrf_handle::init_fht() {
     PM = 1;
     CK(interp_plan_create(plan, W, H, M, p.fht_scale));
     geo = fht_geometry(M, p.fwhm, p.sensitivity);
-    use_fused = (p.kernel == 0) && geo.S <= 32;
+    use_fused = (p.kernel == 0) && fht_fused_supported(geo);
     if (use_fused) CK(fht_fused_tables(geo, WM, HM, tables, stream));
     const long whM = (long)WM * HM;
     scratch.capacity = F;

@@ -107,6 +107,7 @@ cudaError_t fht_fused_tables(const FhtGeometry& g, int W, int H, FhtFusedTables&
 void fht_fused_tables_free(FhtFusedTables& t);
 cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                           cudaStream_t stream);
+bool fht_fused_supported(const FhtGeometry& g);
 
 // AVG/VAR/TAC2/INT from the block accumulators (kernelCalculateVar and the readback's NaN->0).
 // tac_div2: the 2-D bicubic path's double division of TAC2 by (n-1).

@@ -56,49 +56,48 @@ __device__ __forceinline__ float load_raw(const void* raw, bool is_u16, long idx
     return is_u16 ? (float)__ldg((const unsigned short*)raw + idx) : __ldg((const float*)raw + idx);
 }
 
-// Alternating sums of the padded frame: wy[y] = sum_x (-1)^x X[y][x], wx[x] = sum_y (-1)^y X[y][x],
-// q = sum_y (-1)^y wy[y].  One CTA per frame.
+// Alternating sums of the padded frame: wy[y] = sum_x (-1)^x X[y][x] and
+// wx[x] = sum_y (-1)^y X[y][x].  Grid (ceil(N/32), frames): each CTA owns 32 rows and 32 columns.
 __global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u16, int w, int h,
                                                        int N, const int* __restrict__ srcx,
                                                        const int* __restrict__ srcy,
                                                        float* __restrict__ alt) {
-    const int f = blockIdx.x;
+    const int f = blockIdx.y;
     const void* frame = is_u16 ? (const void*)((const unsigned short*)raw + (long)f * w * h)
                                : (const void*)((const float*)raw + (long)f * w * h);
     float* out = alt + (long)f * (2 * N + 1);
-    __shared__ double red[8];
+    __shared__ double red[8][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double qpart = 0.0;
-    // rows: one warp per row
-    for (int y = warp; y < N; y += 8) {
+    const int base = blockIdx.x * 32;
+    // rows base .. base+31: four per warp, lanes across the row
+    for (int r = 0; r < 4; ++r) {
+        const int y = base + warp * 4 + r;
+        if (y >= N) break;
         const long rowoff = (long)srcy[y] * w;
-        double s = 0.0;
+        double acc = 0.0;
         for (int x = lane; x < N; x += 32) {
             const float v = load_raw(frame, is_u16, rowoff + srcx[x]);
-            s += (x & 1) ? -(double)v : (double)v;
+            acc += (x & 1) ? -(double)v : (double)v;
         }
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) {
-            out[y] = (float)s;
-            qpart += (y & 1) ? -s : s;
-        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[y] = (float)acc;
     }
-    // columns: one thread per column
-    for (int x = threadIdx.x; x < N; x += blockDim.x) {
+    // columns base .. base+31: lane = column, warps stride the rows
+    const int x = base + lane;
+    double acc = 0.0;
+    if (x < N) {
         const int sx = srcx[x];
-        double s = 0.0;
-        for (int y = 0; y < N; ++y) {
+        for (int y = warp; y < N; y += 8) {
             const float v = load_raw(frame, is_u16, (long)srcy[y] * w + sx);
-            s += (y & 1) ? -(double)v : (double)v;
+            acc += (y & 1) ? -(double)v : (double)v;
         }
-        out[N + x] = (float)s;
     }
-    if (lane == 0) red[warp] = qpart;
+    red[warp][lane] = acc;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double q = 0.0;
-        for (int i = 0; i < 8; ++i) q += red[i];
-        out[2 * N] = (float)q;
+    if (warp == 0 && x < N) {
+        double t = 0.0;
+        for (int i = 0; i < 8; ++i) t += red[i][lane];
+        out[N + x] = (float)t;
     }
 }
 
@@ -111,11 +110,20 @@ __global__ void __launch_bounds__(256) rank1_vectors_kernel(
     const float* __restrict__ cx, const float* __restrict__ ux, const float* __restrict__ cy,
     int N, int HM, int WM, float s_axis, float s, float* __restrict__ vec) {
     extern __shared__ float wsh[];  // [2N]: wy then wx
+    __shared__ float qred[8];
     const int f = blockIdx.y;
     const float* a = alt + (long)f * (2 * N + 1);
-    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) wsh[i] = a[i];
+    float qp = 0.f;  // q = sum_y (-1)^y wy[y]
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) {
+        const float v = a[i];
+        wsh[i] = v;
+        if (i < N) qp += (i & 1) ? -v : v;
+    }
+    for (int o = 16; o > 0; o >>= 1) qp += __shfl_xor_sync(0xffffffffu, qp, o);
+    if ((threadIdx.x & 31) == 0) qred[threadIdx.x >> 5] = qp;
     __syncthreads();
-    const float q = a[2 * N];
+    float q = 0.f;
+    for (int i = 0; i < 8; ++i) q += qred[i];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     float* v = vec + (long)f * (2 * HM + 2 * WM);
     if (e < HM) {
@@ -352,7 +360,8 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
     if (F <= 0) return cudaSuccess;
     if (F > sc.capacity) return cudaErrorInvalidValue;
     const int N = p.N;
-    alt_sums_kernel<<<F, 256, 0, stream>>>(raw, is_u16 ? 1 : 0, p.w, p.h, N, p.srcx, p.srcy, sc.alt);
+    alt_sums_kernel<<<dim3((N + 31) / 32, F), 256, 0, stream>>>(raw, is_u16 ? 1 : 0, p.w, p.h, N,
+                                                               p.srcx, p.srcy, sc.alt);
     {
         dim3 grid((p.HM + p.WM + 255) / 256, F);
         rank1_vectors_kernel<<<grid, 256, sizeof(float) * 2 * N, stream>>>(

@@ -100,7 +100,7 @@ esrrf_status esrrf_fht_block_noalloc(const void* d_frames, int is_u16, int n_fra
     size_t plan_bytes = 0;
     interp_plan_place(plan, width, height, magnification, 0, nullptr, &plan_bytes, stream);
     const FhtGeometry geo = fht_geometry(magnification, fwhm, sensitivity);
-    if (geo.S > 32)
+    if (!fht_fused_supported(geo))
         return es.fail(ESRRF_ERR_INVALID, "radius too large for the allocation-free entry point "
                                        "(tap box wider than 32 magnified pixels)");
     FhtFusedTables tables;

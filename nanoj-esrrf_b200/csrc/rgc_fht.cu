@@ -226,39 +226,21 @@ constexpr int kTYT = 8;          // thread rows per CTA
 constexpr int kK = 8;            // outputs per thread (vertical)
 constexpr int kTH = kTYT * kK;   // output rows per CTA
 
-struct FusedSmem {
-    int EW, EH, IW, IH, S;
-    size_t off_E, off_I, off_w, off_wd, off_jr, off_st, bytes;
+// Shared-memory layout for a tap box of side S (S = r1 - r0 + 1, always even).
+template <int S>
+struct FusedLayout {
+    static constexpr int EW = kTX + S - 1, EH = kTH + S - 1;  // unit-gradient tile
+    static constexpr int IW = EW + 2, IH = EH + 2;            // intensity tile (+1 px margin)
+    static constexpr size_t off_E = 0;
+    static constexpr size_t off_I = off_E + sizeof(float2) * EW * EH;
+    static constexpr size_t off_wt = (off_I + sizeof(float) * IW * IH + 15) & ~size_t(15);
+    static constexpr size_t off_jr = off_wt + sizeof(float2) * S * S;
+    static constexpr size_t off_st = (off_jr + sizeof(int) * 2 * S + 15) & ~size_t(15);
+    static constexpr size_t bytes = off_st + sizeof(float) * 5 * kTX * kTH;
 };
 
-__host__ __device__ inline FusedSmem fused_smem_layout(int S) {
-    FusedSmem L;
-    L.S = S;
-    L.EW = kTX + S - 1;
-    L.EH = kTH + S - 1;
-    L.IW = L.EW + 2;
-    L.IH = L.EH + 2;
-    size_t o = 0;
-    L.off_E = o;
-    o += sizeof(float2) * (size_t)L.EW * L.EH;
-    L.off_I = o;
-    o += sizeof(float) * (size_t)L.IW * L.IH;
-    o = (o + 15) & ~size_t(15);
-    L.off_w = o;
-    o += sizeof(float) * (size_t)S * S;
-    L.off_wd = o;
-    o += sizeof(float) * (size_t)S * S;
-    L.off_jr = o;
-    o += sizeof(int) * 2 * (size_t)S;
-    o = (o + 15) & ~size_t(15);
-    L.off_st = o;
-    o += sizeof(float) * 5 * kTX * kTH;
-    L.bytes = o;
-    return L;
-}
-
 struct FusedParams {
-    int r0, S;
+    int r0;
     float sens;
     const float* wtab;
     const float* wdtab;
@@ -266,31 +248,59 @@ struct FusedParams {
     const float* wsum;
 };
 
-template <int SB>
+// One column offset i of the tap box for a thread's 8 outputs: source rows rr = 0 .. S+6 of the
+// unit-gradient tile column; row rr feeds output k with tap row jj = rr - k.  CHECK skips rows
+// outside [lo, hi] (columns whose disc chord is shorter than the box).
+template <int S, bool CHECK>
+__device__ __forceinline__ void tap_column(const float2* __restrict__ col, float fi, float fr0,
+                                           int lo, int hi, const float (&w)[S],
+                                           const float (&wd)[S], float (&acc)[kK]) {
+    constexpr int EW = FusedLayout<S>::EW;
+#pragma unroll
+    for (int rr = 0; rr < S + kK - 1; ++rr) {
+        if (CHECK && (rr < lo || rr > hi)) continue;
+        const float2 e = col[rr * EW];
+        const float fr = fr0 + (float)rr;       // tap row j of output k = 0
+        const float dot0 = fmaf(e.y, fr, e.x * fi);
+        const float cr0 = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;
+            if (jj >= 0 && jj < S) {
+                // j = fr - k: dot = dot0 - k g_y, cross = cr0 + k g_x (independent of k - 1)
+                const float dk = k == 0 ? dot0 : fmaf(-(float)k, e.y, dot0);
+                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
+                if (dk < 0.f) acc[k] += t;
+            }
+        }
+    }
+}
+
+template <int S>
 __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, FusedParams fp) {
+    using L = FusedLayout<S>;
+    constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
     extern __shared__ __align__(16) unsigned char smem[];
-    const FusedSmem L = fused_smem_layout(fp.S);
-    float2* sE = reinterpret_cast<float2*>(smem + L.off_E);
-    float* sI = reinterpret_cast<float*>(smem + L.off_I);
-    float* sw = reinterpret_cast<float*>(smem + L.off_w);
-    float* swd = reinterpret_cast<float*>(smem + L.off_wd);
-    int* sjr = reinterpret_cast<int*>(smem + L.off_jr);
-    float* sst = reinterpret_cast<float*>(smem + L.off_st);  // [5][kTH][kTX]
+    float2* sE = reinterpret_cast<float2*>(smem + L::off_E);
+    float* sI = reinterpret_cast<float*>(smem + L::off_I);
+    float2* swt = reinterpret_cast<float2*>(smem + L::off_wt);  // [ii][jj] = (w, w/d)
+    int* sjr = reinterpret_cast<int*>(smem + L::off_jr);
+    float* sst = reinterpret_cast<float*>(smem + L::off_st);    // [5][kTH][kTX]
 
     const int tid = threadIdx.x;
     const int tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTH;
-    const int S = fp.S, r0 = fp.r0;
+    const int r0 = fp.r0;
     const int W = a.W, H = a.H;
     const long wh = (long)W * H;
 
-    for (int i = tid; i < S * S; i += blockDim.x) {
-        sw[i] = fp.wtab[i];
-        swd[i] = fp.wdtab[i];
+    for (int idx = tid; idx < S * S; idx += blockDim.x) {
+        const int ii = idx / S, jj = idx - ii * S;
+        swt[idx] = make_float2(fp.wtab[jj * S + ii], fp.wdtab[jj * S + ii]);
     }
     for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = fp.jrange[i];
 
-    // per-output constants and block state
     const int xM = x0 + tx;
     float wsum[kK];
 #pragma unroll
@@ -314,73 +324,66 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         const float* fr = a.interp + (long)f * wh;
         __syncthreads();
         // 1. interpolated tile with a one-pixel margin beyond the gradient halo (clamped reads)
-        for (int idx = tid; idx < L.IW * L.IH; idx += blockDim.x) {
-            const int ly = idx / L.IW, lx = idx - ly * L.IW;
-            const int gy = min(max(gY0 + ly, 0), H - 1), gx = min(max(gX0 + lx, 0), W - 1);
-            sI[idx] = __ldg(fr + (long)gy * W + gx);
+        for (int ly = ty; ly < IH; ly += kTYT) {
+            const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
+            for (int lx = tx; lx < IW; lx += kTX)
+                sI[ly * IW + lx] = __ldg(fr + grow + min(max(gX0 + lx, 0), W - 1));
         }
         __syncthreads();
         // 2. unit gradient at each tap source: Gx read at min(X+1, W-1), Gy at min(Y+1, H-1),
         //    Roberts cross with max(.-1, 0) clamps (liveSRRF_noInterpolation.cl:144-155, 291-292)
-        for (int idx = tid; idx < L.EW * L.EH; idx += blockDim.x) {
-            const int ey = idx / L.EW, ex = idx - ey * L.EW;
-            const int X = x0 + r0 + ex, Y = y0 + r0 + ey;
-            float2 e = make_float2(0.f, 0.f);
-            if (X >= 0 && X < W && Y >= 0 && Y < H) {
-                const int xa = min(X + 1, W - 1), xa0 = max(xa - 1, 0), ya0 = max(Y - 1, 0);
-                const float ga = sI[(ya0 - gY0) * L.IW + (xa - gX0)];
-                const float gb = sI[(Y - gY0) * L.IW + (xa0 - gX0)];
-                const float gc = sI[(Y - gY0) * L.IW + (xa - gX0)];
-                const float gd = sI[(ya0 - gY0) * L.IW + (xa0 - gX0)];
-                const float Gx = ga - gb + gc - gd;
-                const int yb = min(Y + 1, H - 1), yb0 = max(yb - 1, 0), xb0 = max(X - 1, 0);
-                const float ha = sI[(yb0 - gY0) * L.IW + (X - gX0)];
-                const float hb = sI[(yb - gY0) * L.IW + (xb0 - gX0)];
-                const float hc = sI[(yb - gY0) * L.IW + (X - gX0)];
-                const float hd = sI[(yb0 - gY0) * L.IW + (xb0 - gX0)];
-                const float Gy = -ha + hb + hc - hd;
-                const float n2 = Gx * Gx + Gy * Gy;
-                if (n2 > 0.f) {
-                    const float inv = rsqrtf(n2);
-                    e = make_float2(Gx * inv, Gy * inv);
+        for (int ey = ty; ey < EH; ey += kTYT) {
+            const int Y = y0 + r0 + ey;
+            const bool yin = Y >= 0 && Y < H;
+            const int ya0 = max(Y - 1, 0), yb = min(Y + 1, H - 1), yb0 = max(yb - 1, 0);
+            for (int ex = tx; ex < EW; ex += kTX) {
+                const int X = x0 + r0 + ex;
+                float2 e = make_float2(0.f, 0.f);
+                if (yin && X >= 0 && X < W) {
+                    const int xa = min(X + 1, W - 1), xa0 = max(xa - 1, 0), xb0 = max(X - 1, 0);
+                    const float ga = sI[(ya0 - gY0) * IW + (xa - gX0)];
+                    const float gb = sI[(Y - gY0) * IW + (xa0 - gX0)];
+                    const float gc = sI[(Y - gY0) * IW + (xa - gX0)];
+                    const float gd = sI[(ya0 - gY0) * IW + (xa0 - gX0)];
+                    const float Gx = ga - gb + gc - gd;
+                    const float ha = sI[(yb0 - gY0) * IW + (X - gX0)];
+                    const float hb = sI[(yb - gY0) * IW + (xb0 - gX0)];
+                    const float hc = sI[(yb - gY0) * IW + (X - gX0)];
+                    const float hd = sI[(yb0 - gY0) * IW + (xb0 - gX0)];
+                    const float Gy = -ha + hb + hc - hd;
+                    const float n2 = Gx * Gx + Gy * Gy;
+                    if (n2 > 0.f) {
+                        const float inv = rsqrtf(n2);
+                        e = make_float2(Gx * inv, Gy * inv);
+                    }
                 }
+                sE[ey * EW + ex] = e;
             }
-            sE[idx] = e;
         }
         __syncthreads();
-        // 3. tap loop
+        // 3. tap loop, one box column at a time with its weights in registers
         float acc[kK];
 #pragma unroll
         for (int k = 0; k < kK; ++k) acc[k] = 0.f;
         for (int ii = 0; ii < S; ++ii) {
             const float fi = fr0 + (float)ii;
-            float wr[SB], wdr[SB];
+            float w[S], wd[S];
+            const float4* wc = reinterpret_cast<const float4*>(swt + ii * S);
 #pragma unroll
-            for (int jj = 0; jj < SB; ++jj) {
-                wr[jj] = jj < S ? sw[jj * S + ii] : 0.f;
-                wdr[jj] = jj < S ? swd[jj * S + ii] : 0.f;
+            for (int q = 0; q < S / 2; ++q) {
+                const float4 v = wc[q];
+                w[2 * q] = v.x;
+                wd[2 * q] = v.y;
+                w[2 * q + 1] = v.z;
+                wd[2 * q + 1] = v.w;
             }
             const int lo = sjr[2 * ii];
-            const int hi = min(sjr[2 * ii + 1] + kK - 1, S + kK - 2);
-            const float2* col = sE + (ty * kK) * L.EW + tx + ii;
-#pragma unroll
-            for (int rr = 0; rr < SB + kK - 1; ++rr) {
-                if (rr < lo || rr > hi) continue;
-                const float2 e = col[rr * L.EW];
-                const float fr = fr0 + (float)rr;  // j + k for this source row
-                float dk = fmaf(e.y, fr, e.x * fi);
-                float ck = fmaf(-e.x, fr, e.y * fi);
-#pragma unroll
-                for (int k = 0; k < kK; ++k) {
-                    const int jj = rr - k;
-                    if (jj >= 0 && jj < SB) {
-                        const float t = fmaf(-fabsf(ck), wdr[jj], wr[jj]);
-                        if (dk < 0.f) acc[k] += t;
-                    }
-                    dk -= e.y;
-                    ck += e.x;
-                }
-            }
+            const int hi = sjr[2 * ii + 1] + kK - 1;
+            const float2* col = sE + (ty * kK) * EW + tx + ii;
+            if (lo == 0 && hi == S + kK - 2)
+                tap_column<S, false>(col, fi, fr0, lo, hi, w, wd, acc);
+            else
+                tap_column<S, true>(col, fi, fr0, lo, hi, w, wd, acc);
         }
         // 4. normalisation, sensitivity, intensity weighting and cumulants
         const int tglob = a.t0 + f;
@@ -388,7 +391,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         for (int k = 0; k < kK; ++k) {
             const int o = (ty * kK + k) * kTX + tx;
             const float cg = cglh_power(acc[k] / wsum[k], fp.sens);
-            const float v = sI[(ty * kK + k + 1 - r0) * L.IW + (tx + 1 - r0)];
+            const float v = sI[(ty * kK + k + 1 - r0) * IW + (tx + 1 - r0)];
             const float x = a.int_weighting ? v * cg : cg;
             const float pv = sst[4 * kTX * kTH + o];
             sst[0 * kTX * kTH + o] += x;
@@ -413,16 +416,16 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
     }
 }
 
-template <int SB>
+template <int S>
 cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                          cudaStream_t stream) {
-    const FusedSmem L = fused_smem_layout(g.S);
-    cudaError_t e = cudaFuncSetAttribute(fht_rgc_fused_kernel<SB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
+    constexpr size_t bytes = FusedLayout<S>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    FusedParams fp{g.r0, g.S, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
+    FusedParams fp{g.r0, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
     dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
-    fht_rgc_fused_kernel<SB><<<grid, 256, L.bytes, stream>>>(a, fp);
+    fht_rgc_fused_kernel<S><<<grid, 256, bytes, stream>>>(a, fp);
     return cudaGetLastError();
 }
 
@@ -492,12 +495,29 @@ void fht_fused_tables_free(FhtFusedTables& t) {
 
 cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                           cudaStream_t stream) {
-    if (g.S <= 12) return launch_fused<12>(g, t, a, stream);
-    if (g.S <= 18) return launch_fused<18>(g, t, a, stream);
-    if (g.S <= 24) return launch_fused<24>(g, t, a, stream);
-    if (g.S <= 32) return launch_fused<32>(g, t, a, stream);
-    return cudaErrorInvalidValue;  // caller falls back to the plain kernel
+    // The tap box side S = 2 * loop radius + 2 is even; one instantiation per size keeps the
+    // weight offsets and the tile geometry compile-time constants.
+    switch (g.S) {
+        case 4: return launch_fused<4>(g, t, a, stream);
+        case 6: return launch_fused<6>(g, t, a, stream);
+        case 8: return launch_fused<8>(g, t, a, stream);
+        case 10: return launch_fused<10>(g, t, a, stream);
+        case 12: return launch_fused<12>(g, t, a, stream);
+        case 14: return launch_fused<14>(g, t, a, stream);
+        case 16: return launch_fused<16>(g, t, a, stream);
+        case 18: return launch_fused<18>(g, t, a, stream);
+        case 20: return launch_fused<20>(g, t, a, stream);
+        case 22: return launch_fused<22>(g, t, a, stream);
+        case 24: return launch_fused<24>(g, t, a, stream);
+        case 26: return launch_fused<26>(g, t, a, stream);
+        case 28: return launch_fused<28>(g, t, a, stream);
+        case 30: return launch_fused<30>(g, t, a, stream);
+        case 32: return launch_fused<32>(g, t, a, stream);
+        default: return cudaErrorInvalidValue;  // caller uses the plain kernel
+    }
 }
+
+bool fht_fused_supported(const FhtGeometry& g) { return g.S >= 4 && g.S <= 32 && g.S % 2 == 0; }
 
 cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out,
                            cudaStream_t stream) {
