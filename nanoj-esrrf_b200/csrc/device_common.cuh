@@ -1,0 +1,69 @@
+// device_common.cuh -- device helpers shared by the RGC kernels of the three paths.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace esrrf {
+namespace dev {
+
+// CGLH >= 0 ? pow(CGLH, S) : 0, NaN -> 0 (liveSRRF_noInterpolation.cl:349-353,
+// liveSRRF.cl:357-359, live3DSRRF.cl:429-431); small integer S by repeated products.
+__device__ __forceinline__ float cglh_power(float c, float s) {
+    if (!(c >= 0.f)) return 0.f;
+    if (s == 1.f) return c;
+    if (s == 2.f) return c * c;
+    if (s == 3.f) return c * c * c;
+    if (s == 4.f) {
+        const float c2 = c * c;
+        return c2 * c2;
+    }
+    return powf(c, s);
+}
+
+// Catmull-Rom kernel, a = 0.5 (liveSRRF.cl:26-35).
+__device__ __forceinline__ float cubic(float x) {
+    const float a = 0.5f;
+    if (x < 0.0f) x = -x;
+    float z = 0.0f;
+    if (x < 1.0f)
+        z = x * x * (x * (-a + 2.0f) + (a - 3.0f)) + 1.0f;
+    else if (x < 2.0f)
+        z = -a * x * x * x + 5.0f * a * x * x - 8.0f * a * x + 4.0f * a;
+    return z;
+}
+
+// Bicubic sample when the 4x4 support is interior, else bilinear with extrapolation
+// (getInterpolatedValue, liveSRRF.cl:39-133).
+__device__ __forceinline__ float sample2d(const float* __restrict__ a, int w, int h, float x, float y) {
+    const int u0 = (int)floorf(x);
+    const int v0 = (int)floorf(y);
+    if (u0 > 0 && u0 < w - 2 && v0 > 0 && v0 < h - 2) {
+        float q = 0.0f;
+#pragma unroll
+        for (int j = 0; j <= 3; j++) {
+            const int v = min(max(v0 - 1 + j, 0), h - 1);
+            float p = 0.0f;
+#pragma unroll
+            for (int i = 0; i <= 3; i++) {
+                const int u = min(max(u0 - 1 + i, 0), w - 1);
+                p = p + __ldg(a + (long)v * w + u) * cubic(x - (float)u);
+            }
+            q = q + p * cubic(y - (float)v);
+        }
+        return q;
+    }
+    const int xb = (int)fminf((float)w - 2, fmaxf(x, 0.0f));
+    const int yb = (int)fminf((float)h - 2, fmaxf(y, 0.0f));
+    const float xf = x - (float)xb, yf = y - (float)yb;
+    const float ll = __ldg(a + (long)yb * w + xb), lr = __ldg(a + (long)yb * w + xb + 1);
+    const float ur = __ldg(a + (long)(yb + 1) * w + xb + 1), ul = __ldg(a + (long)(yb + 1) * w + xb);
+    const float upper = ul + xf * (ur - ul);
+    const float lower = ll + xf * (lr - ll);
+    return lower + yf * (upper - lower);
+}
+
+__device__ __forceinline__ float load_px(const void* raw, int is_u16, long idx) {
+    return is_u16 ? (float)__ldg((const unsigned short*)raw + idx) : __ldg((const float*)raw + idx);
+}
+
+}  // namespace dev
+}  // namespace esrrf

@@ -117,7 +117,89 @@ esrrf_status esrrf_handle::init(const esrrf_params& params) {
     F = p.frames_per_launch > 0 ? p.frames_per_launch : 8;
 
     if (mode == Mode::kFHT) return init_fht();
-    return fail(ESRRF_ERR_INVALID, "the bicubic 2-D and 3-D paths are not available in this build");
+    return init_bic3d();
+}
+
+// Staging buffers, block accumulators and output, shared by the three paths.
+esrrf_status esrrf_handle::alloc_common(size_t frame_bytes, long out_pixels) {
+    esrrf_handle* h = this;
+    raw_frame_bytes = frame_bytes;
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaMalloc(&d_raw[b], raw_frame_bytes * F));
+        CK(cudaMallocHost(&h_stage[b], raw_frame_bytes * F));
+    }
+    st.pixels = out_pixels;
+    CK(cudaMalloc(&st.acc, sizeof(double) * 4 * out_pixels));
+    CK(cudaMalloc(&st.prev, sizeof(float) * out_pixels));
+    CK(cudaMalloc(&d_out, sizeof(float) * 4 * out_pixels));
+    CK(zero_block(st, stream));
+    CK(cudaMalloc(&d_shift, sizeof(float) * 2 * (size_t)F));
+    CK(cudaStreamSynchronize(stream));
+    frame_in_block = 0;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_handle::init_bic3d() {
+    esrrf_handle* h = this;
+    const int M = p.magnification;
+    W = p.width;
+    H = p.height;
+    bgeo = bic_geometry(p.fwhm, p.sensitivity);
+    if (mode == Mode::k3D) {
+        P = p.n_planes;
+        ws = W / 3;  // nSplits = 3 (LiveSRRF_CL.java:37, 229-230)
+        hs = H / 3;
+        if (ws < 4 || hs < 4) return fail(ESRRF_ERR_INVALID, "MFM planes must be at least 4x4 pixels");
+        std::vector<int> tx0(P), ty0(P);
+        std::vector<float> ct(P), sn(P);
+        for (int z = 0; z < P; ++z) {
+            // ROI index -> tile origin, Math.round((float) W / 3 * i) (LiveSRRF_CL.java:973-978)
+            const int i = ((int)roi[z]) % 3;
+            const int j = ((int)(roi[z] - (float)i)) / 3;
+            tx0[z] = (int)floorf((float)W / 3 * i + 0.5f);
+            ty0[z] = (int)floorf((float)H / 3 * j + 0.5f);
+            if (roi[z] < 0 || roi[z] > 8 || tx0[z] + ws > W || ty0[z] + hs > H)
+                return fail(ESRRF_ERR_INVALID, "calibration ROI outside the camera frame");
+            if (!(coeff[z] != 0.f)) return fail(ESRRF_ERR_INVALID, "intensity scaling must be non-zero");
+            // -theta in radians as the Java host uploads it (LiveSRRF_CL.java:441)
+            const float th = (float)(-(double)theta[z] * M_PI / 180.0);
+            ct[z] = cosf(th);
+            sn[z] = sinf(th);
+        }
+        auto up = [&](auto** d, const auto& v) -> cudaError_t {
+            cudaError_t e = cudaMalloc((void**)d, sizeof(v[0]) * v.size());
+            if (e != cudaSuccess) return e;
+            return cudaMemcpy(*d, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice);
+        };
+        CK(up(&mfm.tile_x0, tx0));
+        CK(up(&mfm.tile_y0, ty0));
+        CK(up(&mfm.coeff, coeff));
+        CK(up(&mfm.cos_t, ct));
+        CK(up(&mfm.sin_t, sn));
+        CK(up(&mfm.shx, shx));
+        CK(up(&mfm.shy, shy));
+        PM = P * M;
+    } else {
+        P = 1;
+        ws = W;
+        hs = H;
+        PM = 1;
+    }
+    WM = ws * M;
+    HM = hs * M;
+    const size_t plane = (size_t)ws * hs;
+    CK(cudaMalloc(&d_fraw, sizeof(float) * F * P * plane));
+    CK(cudaMalloc(&d_gx, sizeof(float) * F * P * plane));
+    CK(cudaMalloc(&d_gy, sizeof(float) * F * P * plane));
+    CK(cudaMalloc(&d_gxi, sizeof(float) * F * P * 4 * plane));
+    CK(cudaMalloc(&d_gyi, sizeof(float) * F * P * 4 * plane));
+    if (mode == Mode::k3D) {
+        CK(cudaMalloc(&d_planes, sizeof(float) * F * P * plane));
+        CK(cudaMalloc(&d_gz, sizeof(float) * F * P * plane));
+        CK(cudaMalloc(&d_gzi, sizeof(float) * F * P * 4 * plane));
+    }
+    CK(cudaMalloc(&d_mpmap, sizeof(float) * 3 * M * M * M));
+    return alloc_common(sizeof(float) * (size_t)W * H, (long)WM * HM * PM);
 }
 
 esrrf_status esrrf_handle::init_fht() {
@@ -140,20 +222,7 @@ esrrf_status esrrf_handle::init_fht() {
     CK(cudaMalloc(&d_interp, sizeof(float) * (size_t)F * whM));
     CK(cudaMalloc(&d_gx, sizeof(float) * (size_t)F * whM));
     CK(cudaMalloc(&d_gy, sizeof(float) * (size_t)F * whM));
-    CK(cudaMalloc(&d_shift, sizeof(float) * 2 * (size_t)F));
-    raw_frame_bytes = sizeof(float) * (size_t)W * H;  // holds a float or a uint16 frame
-    for (int b = 0; b < 2; ++b) {
-        CK(cudaMalloc(&d_raw[b], raw_frame_bytes * F));
-        CK(cudaMallocHost(&h_stage[b], raw_frame_bytes * F));
-    }
-    st.pixels = whM;
-    CK(cudaMalloc(&st.acc, sizeof(double) * 4 * whM));
-    CK(cudaMalloc(&st.prev, sizeof(float) * whM));
-    CK(cudaMalloc(&d_out, sizeof(float) * 4 * whM));
-    CK(zero_block(st, stream));
-    CK(cudaStreamSynchronize(stream));
-    frame_in_block = 0;
-    return ESRRF_OK;
+    return alloc_common(sizeof(float) * (size_t)W * H, whM);  // a float or a uint16 frame
 }
 
 void esrrf_handle::release() {
@@ -179,6 +248,11 @@ void esrrf_handle::release() {
     cudaFree(st.acc);
     cudaFree(st.prev);
     cudaFree(d_out);
+    for (float* b : {d_fraw, d_planes, d_gz, d_gxi, d_gyi, d_gzi, d_mpmap, mfm.coeff, mfm.cos_t,
+                     mfm.sin_t, mfm.shx, mfm.shy})
+        cudaFree(b);
+    cudaFree(mfm.tile_x0);
+    cudaFree(mfm.tile_y0);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
     ev_pool.clear();
     if (ev_a) cudaEventDestroy(ev_a);
@@ -200,9 +274,8 @@ esrrf_status esrrf_handle::reset_block() {
 // Runs interpolation + RGC for F_now frames that are already in device memory at `src`.
 esrrf_status esrrf_handle::process_chunk(const void* src, bool is_u16, int F_now) {
     esrrf_handle* h = this;
-    if (mode != Mode::kFHT) return fail(ESRRF_ERR_INVALID, "mode not available");
     const int M = p.magnification;
-    // per-frame drift of this chunk, in magnified pixels (loadDriftXYGPUbuffer, LiveSRRF_CL.java:586-589)
+    // per-frame drift of this chunk, x magnification (loadDriftXYGPUbuffer, LiveSRRF_CL.java:586-589)
     std::vector<float> sh(2 * F_now);
     bool any_drift = false;
     for (int f = 0; f < F_now; ++f) {
@@ -210,6 +283,7 @@ esrrf_status esrrf_handle::process_chunk(const void* src, bool is_u16, int F_now
         sh[F_now + f] = M * drift_y[frame_in_block + f];
         any_drift |= (sh[f] != 0.f || sh[F_now + f] != 0.f);
     }
+    if (mode != Mode::kFHT) return process_chunk_bic3d(src, is_u16, F_now, sh);
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     if (timing) {
         esrrf_status r;
@@ -268,6 +342,73 @@ void esrrf_handle::collect_timing() {
     }
     cudaGetLastError();
     ev_used = 0;
+}
+
+esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int F_now,
+                                               const std::vector<float>& sh) {
+    esrrf_handle* h = this;
+    CK(cudaMemcpyAsync(d_shift, sh.data(), sizeof(float) * 2 * F_now, cudaMemcpyHostToDevice, stream));
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    if (timing) {
+        esrrf_status r;
+        if ((r = timing_event(&e0)) != ESRRF_OK || (r = timing_event(&e1)) != ESRRF_OK ||
+            (r = timing_event(&e2)) != ESRRF_OK)
+            return r;
+        CK(cudaEventRecord(e0, stream));
+    }
+    if (mode == Mode::kBIC) {
+        CK(bic_prepare(src, is_u16 ? 1 : 0, W, H, F_now, d_fraw, d_gx, d_gy, d_gxi, d_gyi, stream));
+        launches += 3;
+    } else {
+        CK(mfm_prepare(src, is_u16 ? 1 : 0, W, H, P, ws, hs, F_now, mfm, p.background, d_planes,
+                       d_fraw, d_gx, d_gy, d_gz, d_gxi, d_gyi, d_gzi, stream));
+        launches += 6;
+    }
+    if (timing) CK(cudaEventRecord(e1, stream));
+    if (mode == Mode::kBIC) {
+        BicRgcArgs a{};
+        a.fraw = d_fraw;
+        a.gxi = d_gxi;
+        a.gyi = d_gyi;
+        a.w = ws;
+        a.h = hs;
+        a.M = p.magnification;
+        a.F = F_now;
+        a.t0 = frame_in_block;
+        a.tSS = bgeo.tSS;
+        a.tSO = bgeo.tSO;
+        a.radius = bgeo.radius;
+        a.sens = bgeo.sensitivity;
+        a.shift = d_shift;
+        a.int_weighting = p.int_weighting;
+        a.st = st;
+        CK(bic_rgc(a, stream));
+    } else {
+        Rgc3dArgs a{};
+        a.apx = d_fraw;
+        a.gxi = d_gxi;
+        a.gyi = d_gyi;
+        a.gzi = d_gzi;
+        a.w = ws;
+        a.h = hs;
+        a.P = P;
+        a.M = p.magnification;
+        a.F = F_now;
+        a.t0 = frame_in_block;
+        a.tSS = bgeo.tSS;
+        a.tSO = bgeo.tSO;
+        a.radius = bgeo.radius;
+        a.sens = bgeo.sensitivity;
+        a.shift = d_shift;
+        a.int_weighting = p.int_weighting;
+        a.st = st;
+        CK(rgc_3d(a, stream));
+    }
+    launches += 1;
+    if (timing) CK(cudaEventRecord(e2, stream));
+    CK(cudaStreamSynchronize(stream));  // `sh` is a host temporary
+    frame_in_block += F_now;
+    return ESRRF_OK;
 }
 
 esrrf_status esrrf_handle::calculate(const void* frames, bool is_u16, int n, bool on_device) {
@@ -333,7 +474,10 @@ esrrf_status esrrf_handle::read(float* out, bool on_device) {
     CK(cudaSetDevice(device));
     if (frame_in_block == 0) return fail(ESRRF_ERR_STATE, "no frames accumulated in this block");
     // kernelCalculateVar + NaN->0 (LiveSRRF_CL.java:749-794) on the block accumulated so far.
-    CK(finalize_block(st, p.n_frame_for_srrf, 0, d_out, stream));
+    CK(finalize_block(st, p.n_frame_for_srrf, mode == Mode::kBIC ? 1 : 0, d_out, stream));
+    // MP map correction runs on the bicubic and 3-D paths only (LiveSRRF_CL.java:762-770)
+    if (p.mp_correction && mode != Mode::kFHT)
+        CK(mp_correct(d_out, ws, hs, P, p.magnification, mode == Mode::k3D ? 1 : 0, d_mpmap, stream));
     const size_t bytes = sizeof(float) * 4 * (size_t)st.pixels;
     CK(cudaMemcpyAsync(out, d_out, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                        stream));
@@ -483,10 +627,24 @@ esrrf_status esrrf_output_shape(const esrrf_handle* h, int* wm, int* hm, int* pm
 
 esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len) {
     if (!h || !out) return ESRRF_ERR_INVALID;
-    if (h->mode != esrrf_handle::Mode::kFHT) return h->fail(ESRRF_ERR_INVALID, "mode not available");
+    if (cudaSetDevice(h->device) != cudaSuccess) return ESRRF_ERR_CUDA;
+    if (h->mode != esrrf_handle::Mode::kFHT) {
+        // 2x-resampled gradient components of the first frame of the last push
+        const size_t plane = (size_t)4 * h->ws * h->hs * h->P;
+        const int nc = h->mode == esrrf_handle::Mode::k3D ? 3 : 2;
+        if (out_len < nc * plane) return h->fail(ESRRF_ERR_INVALID, "output buffer too small");
+        const float* src[3] = {h->d_gxi, h->d_gyi, h->d_gzi};
+        for (int c = 0; c < nc; ++c)
+            if (cudaMemcpyAsync(out + c * plane, src[c], sizeof(float) * plane, cudaMemcpyDeviceToHost,
+                                h->stream) != cudaSuccess) {
+                cudaGetLastError();
+                return h->fail(ESRRF_ERR_CUDA, "gradient read-back failed");
+            }
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) return h->fail(ESRRF_ERR_CUDA, "sync failed");
+        return ESRRF_OK;
+    }
     const size_t plane = (size_t)h->WM * h->HM;
     if (out_len < 2 * plane) return h->fail(ESRRF_ERR_INVALID, "output buffer too small");
-    if (cudaSetDevice(h->device) != cudaSuccess) return ESRRF_ERR_CUDA;
     // The interpolated frames of the last chunk are still resident: recompute the gradient of
     // the first one (readGradientBuffers reads frame 0 of the last load).
     if (fht_robx(h->d_interp, h->WM, h->HM, 1, h->d_gx, h->d_gy, h->stream) != cudaSuccess ||

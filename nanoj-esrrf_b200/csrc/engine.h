@@ -32,6 +32,18 @@ struct esrrf_handle {
     float* d_gy = nullptr;
     float* d_shift = nullptr;
 
+    // 2-D bicubic and 3-D paths
+    esrrf::BicGeometry bgeo;
+    esrrf::Mfm3dTables mfm;
+    int P = 1, ws = 0, hs = 0;  // planes and per-plane size (3-D); ws = W, hs = H in 2-D
+    float* d_fraw = nullptr;    // [F][P][hs][ws] float frames / aligned planes
+    float* d_planes = nullptr;  // [F][P][hs][ws] split planes before alignment (3-D)
+    float* d_gz = nullptr;
+    float* d_gxi = nullptr;     // [F][P][2hs][2ws]
+    float* d_gyi = nullptr;
+    float* d_gzi = nullptr;
+    float* d_mpmap = nullptr;   // [3][M^2 or M^3]
+
     // input staging (double-buffered)
     size_t raw_frame_bytes = 0;
     void* d_raw[2] = {nullptr, nullptr};
@@ -62,10 +74,14 @@ struct esrrf_handle {
 
     esrrf_status init(const esrrf_params& params);
     esrrf_status init_fht();
+    esrrf_status init_bic3d();
+    esrrf_status alloc_common(size_t raw_frame_bytes, long out_pixels);
     void release();
     esrrf_status reset_block();
     esrrf_status calculate(const void* frames, bool is_u16, int n, bool on_device);
     esrrf_status process_chunk(const void* src, bool is_u16, int F_now);
+    esrrf_status process_chunk_bic3d(const void* src, bool is_u16, int F_now,
+                                     const std::vector<float>& sh);
     esrrf_status read(float* out, bool on_device);
     esrrf_status fail(esrrf_status s, const std::string& msg);
     esrrf_status fail_cuda(cudaError_t e, const char* what, int line);

@@ -115,6 +115,63 @@ cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out
                            cudaStream_t stream);
 cudaError_t zero_block(BlockState& st, cudaStream_t stream);
 
+// ------------------------------------------------------------------------------------------
+// 2-D bicubic path (liveSRRF.cl) and 3-D path (live3DSRRF.cl): constants as
+// prepareBuffersBICinterpolation computes them (LiveSRRF_CL.java:301-342).
+// ------------------------------------------------------------------------------------------
+struct BicGeometry {
+    float sigma = 0, tSS = 0, tSO = 0, radius = 0;
+    float sensitivity = 1;
+};
+BicGeometry bic_geometry(float fwhm, int sensitivity);
+
+struct BicRgcArgs {
+    const float* fraw;   // [F][h][w] raw frames as float (intensity source)
+    const float* gxi;    // [F][2h][2w] 2x-resampled 2-point gradient
+    const float* gyi;
+    int w, h, M, F, t0;
+    float tSS, tSO, radius, sens;
+    const float* shift;  // [2][F] drift x magnification (used in raw pixels, as the reference)
+    int int_weighting;
+    BlockState st;
+};
+
+cudaError_t bic_prepare(const void* raw, int is_u16, int w, int h, int F, float* fraw, float* gx,
+                        float* gy, float* gxi, float* gyi, cudaStream_t stream);
+cudaError_t grad2x(const float* g, int w, int h, int planes, float* gi, cudaStream_t stream);
+cudaError_t bic_rgc(const BicRgcArgs& a, cudaStream_t stream);
+// MP map of AVG/VAR/TAC2 and division (then NaN->0) on a finalized output [4][PM][HM][WM].
+cudaError_t mp_correct(float* out, int w, int h, int P, int M, int is3d, float* map,
+                       cudaStream_t stream);
+
+struct Rgc3dArgs {
+    const float* apx;    // [F][P][h][w] aligned planes
+    const float* gxi;    // [F][P][2h][2w]
+    const float* gyi;
+    const float* gzi;
+    int w, h, P, M, F, t0;
+    float tSS, tSO, radius, sens;
+    const float* shift;  // [2][F] drift x magnification (used in raw pixels, as the reference)
+    int int_weighting;
+    BlockState st;
+};
+struct Mfm3dTables {
+    int* tile_x0 = nullptr;   // [P] crop origin of each plane in the camera frame
+    int* tile_y0 = nullptr;
+    float* coeff = nullptr;   // [P] intensity scaling
+    float* cos_t = nullptr;   // [P] cos / sin of -theta (radians, float)
+    float* sin_t = nullptr;
+    float* shx = nullptr;     // [P]
+    float* shy = nullptr;
+};
+// camera frames [F][H][W] -> planes [F][P][hs][ws] ((p - background) / coeff), aligned planes,
+// 3-D 2-point gradient and its 2x lateral resampling.
+cudaError_t mfm_prepare(const void* raw, int is_u16, int W, int H, int P, int ws, int hs, int F,
+                        const Mfm3dTables& t, float background, float* planes, float* apx,
+                        float* gx, float* gy, float* gz, float* gxi, float* gyi, float* gzi,
+                        cudaStream_t stream);
+cudaError_t rgc_3d(const Rgc3dArgs& a, cudaStream_t stream);
+
 // Variants of the table set-up that place their tables in caller-provided device memory (no
 // allocation); used by the allocation-free entry point.
 cudaError_t interp_plan_place(InterpPlan& plan, int w, int h, int M, int scale_mode,
