@@ -168,6 +168,44 @@ esrrf_status esrrf_set_timing(esrrf_handle* h, int enable);
 esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* rgc_ms,
                                int* launches);
 
+/* ---- Batched parameter sweep and rolling analysis over uneven blocks -----------------------
+ * Replaces the per-combination loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519:
+ * initialise + resetFramePosition + calculateSRRF + readSRRFbuffer for every radius x
+ * sensitivity) and the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:
+ * 276-389), on the 2-D FHT path with zero drift.  All frames are interpolated once per
+ * magnification and the RGC tap loop runs once per (magnification, radius) for all
+ * sensitivities and blocks; the whole sweep is one captured CUDA graph replayed per run.
+ * Blocks are arbitrary [start, start + length) frame ranges (uneven and overlapping allowed). */
+typedef struct {
+    int width, height, n_frames;
+    int n_mag;
+    const int* magnifications;
+    int n_radius;
+    const float* radii;        /* the GUI's "Radius" (fwhm) values */
+    int n_sens;
+    const int* sensitivities;
+    int n_blocks;
+    const int* block_start;
+    const int* block_length;
+    int int_weighting;
+    int device;                /* CUDA ordinal; -1 = device 0 */
+} esrrf_sweep_params;
+
+typedef struct esrrf_sweep esrrf_sweep;
+
+esrrf_status esrrf_sweep_create(const esrrf_sweep_params* params, esrrf_sweep** out);
+/* Output layout: for magnification m, radius r the floats from offsets[m * n_radius + r] hold
+ * [n_sens][n_blocks][4][HM_m][WM_m] (AVG, VAR, TAC2, INT; NaN -> 0), HM_m = height * M_m. */
+esrrf_status esrrf_sweep_output_layout(const esrrf_sweep* s, size_t* total_floats, size_t* offsets);
+/* frames: [n_frames][height][width] uint16 (is_u16 = 1) or float; device pointers here, host
+ * pointers in esrrf_sweep_run.  The first run with given pointers captures the graph. */
+esrrf_status esrrf_sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out);
+esrrf_status esrrf_sweep_run(esrrf_sweep* s, const void* frames, int is_u16, float* out);
+/* Kernels in one run (the graph's node count). */
+esrrf_status esrrf_sweep_launch_count(const esrrf_sweep* s, int* launches);
+const char* esrrf_sweep_last_error(const esrrf_sweep* s);
+esrrf_status esrrf_sweep_destroy(esrrf_sweep* s);
+
 /* Allocation-free variant of one FHT-path SR block; it has no counterpart in the reference.
  * For callers that must not allocate device memory when they reconstruct -- e.g. a
  * live-acquisition callback, where cudaMalloc/cudaFree can synchronise the device and stall

@@ -90,6 +90,8 @@ struct FhtRgcArgs {
     const float* shift;    // [2][F] drift in magnified pixels (plain path)
     int int_weighting;
     BlockState st;
+    float* cg_out = nullptr;  // fused kernel only: if set, write CGLH / sum of weights per frame
+                              // [F][H][W] (before the sensitivity power) instead of accumulating
 };
 
 cudaError_t fht_robx(const float* interp, int W, int H, int F, float* gx, float* gy,

@@ -255,6 +255,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
     for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = fp.jrange[i];
 
     const int xM = x0 + tx;
+    const bool emit = a.cg_out != nullptr;
     float wsum[kK];
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         const bool in = xM < W && yM < H;
         const long pix = (long)yM * W + xM;
         wsum[k] = in ? fp.wsum[pix] : 1.f;
+        if (emit) continue;
         const int o = (ty * kK + k) * kTX + tx;
         sst[0 * kTX * kTH + o] = 0.f;
         sst[1 * kTX * kTH + o] = 0.f;
@@ -339,6 +341,14 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
                 tap_column<S, true>(col, fi, fr0, lo, hi, w, wd, acc);
         }
         // 4. normalisation, sensitivity, intensity weighting and cumulants
+        if (emit) {
+#pragma unroll
+            for (int k = 0; k < kK; ++k) {
+                const int yM = y0 + ty * kK + k;
+                if (xM < W && yM < H) a.cg_out[(long)f * wh + (long)yM * W + xM] = acc[k] / wsum[k];
+            }
+            continue;
+        }
         const int tglob = a.t0 + f;
 #pragma unroll
         for (int k = 0; k < kK; ++k) {
@@ -355,6 +365,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         }
     }
     // 5. fold this launch's FP32 partial sums into the block's FP64 accumulators
+    if (emit) return;
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
         const int yM = y0 + ty * kK + k;
@@ -373,9 +384,18 @@ template <int S>
 cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                          cudaStream_t stream) {
     constexpr size_t bytes = FusedLayout<S>::bytes;
-    cudaError_t e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // The opt-in shared-memory size is a per-device function attribute: set it once per device
+    // (also keeps the call out of CUDA-graph captures after the first, uncaptured launch).
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    if (dev >= 64 || !(configured & (1ull << dev))) {
+        e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes);
+        if (e != cudaSuccess) return e;
+        if (dev < 64) configured |= 1ull << dev;
+    }
     FusedParams fp{g.r0, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
     dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
     fht_rgc_fused_kernel<S><<<grid, 256, bytes, stream>>>(a, fp);

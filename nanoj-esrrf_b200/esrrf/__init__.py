@@ -226,3 +226,97 @@ def esrrf_stack(stack, magnification, fwhm, sensitivity, frames_per_block=None, 
     finally:
         eng.release()
     return np.stack(outs)
+
+
+class Sweep:
+    """Batched parameter sweep / rolling analysis (esrrf_sweep_*): every (magnification, radius,
+    sensitivity, block) reconstruction of a stack in one captured CUDA graph.  Replaces the
+    per-combination engine loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519) and
+    the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:276-389)."""
+
+    def __init__(self, width, height, n_frames, magnifications, radii, sensitivities, blocks,
+                 int_weighting=True, device=-1):
+        from ._lib import EsrrfSweepParams
+
+        self.width, self.height, self.n_frames = int(width), int(height), int(n_frames)
+        self.mags = np.ascontiguousarray(magnifications, np.int32)
+        self.radii = np.ascontiguousarray(radii, np.float32)
+        self.sens = np.ascontiguousarray(sensitivities, np.int32)
+        blocks = np.asarray(blocks, np.int64).reshape(-1, 2)
+        self.bstart = np.ascontiguousarray(blocks[:, 0], np.int32)
+        self.blen = np.ascontiguousarray(blocks[:, 1], np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        fp = ctypes.POINTER(ctypes.c_float)
+        p = EsrrfSweepParams(self.width, self.height, self.n_frames, len(self.mags),
+                             self.mags.ctypes.data_as(ip), len(self.radii), self.radii.ctypes.data_as(fp),
+                             len(self.sens), self.sens.ctypes.data_as(ip), len(self.bstart),
+                             self.bstart.ctypes.data_as(ip), self.blen.ctypes.data_as(ip),
+                             int(bool(int_weighting)), int(device))
+        h = ctypes.c_void_p()
+        _lib.check(None, lib().esrrf_sweep_create(ctypes.byref(p), ctypes.byref(h)), sweep=True)
+        self._h = h
+        total = ctypes.c_size_t()
+        offs = (ctypes.c_size_t * (len(self.mags) * len(self.radii)))()
+        _lib.check(h, lib().esrrf_sweep_output_layout(h, ctypes.byref(total), offs), sweep=True)
+        self.total = total.value
+        self.offsets = list(offs)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def launch_count(self) -> int:
+        n = ctypes.c_int()
+        _lib.check(self._h, lib().esrrf_sweep_launch_count(self._h, ctypes.byref(n)), sweep=True)
+        return n.value
+
+    def unpack(self, flat):
+        """{(M, radius, S, (start, length)): [4][HM][WM]} views of a flat output buffer."""
+        out = {}
+        nS, nB = len(self.sens), len(self.bstart)
+        for mi, M in enumerate(self.mags):
+            P = self.height * M * self.width * M
+            for ri, r in enumerate(self.radii):
+                base = self.offsets[mi * len(self.radii) + ri]
+                blk = flat[base:base + nS * nB * 4 * P].reshape(nS, nB, 4, self.height * M, self.width * M)
+                for si, S in enumerate(self.sens):
+                    for bi in range(nB):
+                        out[(int(M), float(r), int(S), (int(self.bstart[bi]), int(self.blen[bi])))] = blk[si, bi]
+        return out
+
+    def run(self, stack):
+        a = np.asarray(stack)
+        if a.dtype == np.uint16:
+            a = np.ascontiguousarray(a)
+            is_u16 = 1
+        else:
+            a = np.ascontiguousarray(a, np.float32)
+            is_u16 = 0
+        flat = np.empty(self.total, np.float32)
+        _lib.check(self._h, lib().esrrf_sweep_run(self._h, a.ctypes.data_as(ctypes.c_void_p), is_u16,
+                                                  flat.ctypes.data_as(ctypes.c_void_p)), sweep=True)
+        return self.unpack(flat)
+
+    def release(self):
+        if self._h:
+            lib().esrrf_sweep_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def rolling(stack, magnification, fwhm, sensitivity, blocks, int_weighting=True):
+    """Rolling analysis over arbitrary (start, length) blocks, each frame interpolated and run
+    through the RGC once: {(start, length): [4][HM][WM]}."""
+    a = np.asarray(stack)
+    sw = Sweep(a.shape[-1], a.shape[-2], a.shape[0], [magnification], [fwhm], [sensitivity],
+               blocks, int_weighting)
+    try:
+        res = sw.run(a)
+        return {k[3]: v.copy() for k, v in res.items()}
+    finally:
+        sw.release()

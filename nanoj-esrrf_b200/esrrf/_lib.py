@@ -77,6 +77,32 @@ SIGNATURES = {
                                            _c.c_void_p, _c.c_char_p, _c.c_size_t]),
 }
 
+
+class EsrrfSweepParams(ctypes.Structure):
+    """esrrf_sweep_params (include/esrrf.h)."""
+
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("n_frames", ctypes.c_int),
+        ("n_mag", ctypes.c_int), ("magnifications", ctypes.POINTER(ctypes.c_int)),
+        ("n_radius", ctypes.c_int), ("radii", _f32p),
+        ("n_sens", ctypes.c_int), ("sensitivities", ctypes.POINTER(ctypes.c_int)),
+        ("n_blocks", ctypes.c_int), ("block_start", ctypes.POINTER(ctypes.c_int)),
+        ("block_length", ctypes.POINTER(ctypes.c_int)),
+        ("int_weighting", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+SIGNATURES.update({
+    "esrrf_sweep_create": (_c.c_int, [_c.POINTER(EsrrfSweepParams), _c.POINTER(_c.c_void_p)]),
+    "esrrf_sweep_output_layout": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_size_t),
+                                             _c.POINTER(_c.c_size_t)]),
+    "esrrf_sweep_run_device": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_int, _c.c_void_p]),
+    "esrrf_sweep_run": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_int, _c.c_void_p]),
+    "esrrf_sweep_launch_count": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
+    "esrrf_sweep_last_error": (_c.c_char_p, [_c.c_void_p]),
+    "esrrf_sweep_destroy": (_c.c_int, [_c.c_void_p]),
+})
+
 _LIB = None
 
 
@@ -95,9 +121,9 @@ def lib():
     return _LIB
 
 
-def check(handle, rc: int) -> None:
+def check(handle, rc: int, sweep: bool = False) -> None:
     if rc == 0:
         return
-    msg = lib().esrrf_last_error(handle)
+    msg = (lib().esrrf_sweep_last_error if sweep else lib().esrrf_last_error)(handle)
     msg = msg.decode() if msg else ""
     raise EsrrfError(f"esrrf status {STATUS.get(rc, rc)}: {msg}")
