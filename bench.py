@@ -35,10 +35,17 @@ for _p in (ROOT, PKG):
         sys.path.insert(0, _p)
 
 WORKLOADS = {
-    # name: (synth workload, frames per block, cumulants)
-    "fht512": ("fht512", 100),
-    "fht64": ("fht64", 100),
+    # name: (synth workload, frames per block)
+    "fht512": ("fht512", 100),   # 2-D FHT path, the headline workload
+    "fht64": ("fht64", 100),     # 2-D FHT path, 64x64 M5
+    "sweep256": ("sweep256", 0),  # batched parameter sweep (88 combinations, uneven blocks)
+    "mfm3d": ("mfm3d", 200),     # 3-D MFM path, 9 planes
 }
+SWEEP_RADII = [0.5 + 0.25 * i for i in range(11)]
+SWEEP_SENS = [1, 2, 3, 4]
+SWEEP_MAGS = [2, 4]
+# blocks of 37, 64, 99 frames tiling the 200-frame stack, plus an overlapping [0, 100)
+SWEEP_BLOCKS = [(0, 37), (37, 64), (101, 99), (0, 100)]
 # Fixed convention for algorithmic FP32 work: 22 ops per evaluated tap
 OPS_PER_TAP = 22.0
 FP32_PEAK_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4 at the 1965 MHz max clock
@@ -351,6 +358,169 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line))
 
 
+def run_sweep(args, world, rank, local):
+    """Batched sweep (one captured graph) against a loop of single-combination plain-kernel
+    engine runs, the structure of ParametersSweep_.run; metric combos/s."""
+    import ctypes
+
+    import torch
+
+    import esrrf
+    from esrrf import synth
+
+    torch.cuda.set_device(local)
+    stack = synth.make_stack("sweep256")
+    n, h, w = stack.shape
+    L = esrrf.lib()
+    sw = esrrf.Sweep(w, h, n, SWEEP_MAGS, SWEEP_RADII, SWEEP_SENS, SWEEP_BLOCKS, device=local)
+    d_stack = torch.from_numpy(stack.view(np.int16)).to(f"cuda:{local}")
+    d_out = torch.empty(sw.total, dtype=torch.float32, device=f"cuda:{local}")
+    combos = len(SWEEP_MAGS) * len(SWEEP_RADII) * len(SWEEP_SENS)
+
+    def step():
+        esrrf._lib.check(sw.handle, L.esrrf_sweep_run_device(sw.handle, ctypes.c_void_p(d_stack.data_ptr()),
+                                                            1, ctypes.c_void_p(d_out.data_ptr())), sweep=True)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        torch.cuda.synchronize()
+        t_step = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
+    launches = sw.launch_count()
+    # e2e: host stack in, host results out
+    h_stack = torch.from_numpy(stack.view(np.int16)).pin_memory()
+    h_out = torch.empty(sw.total, dtype=torch.float32).pin_memory()
+    esrrf._lib.check(sw.handle, L.esrrf_sweep_run(sw.handle, ctypes.c_void_p(h_stack.data_ptr()), 1,
+                                                  ctypes.c_void_p(h_out.data_ptr())), sweep=True)
+    t0 = time.perf_counter()
+    esrrf._lib.check(sw.handle, L.esrrf_sweep_run(sw.handle, ctypes.c_void_p(h_stack.data_ptr()), 1,
+                                                  ctypes.c_void_p(h_out.data_ptr())), sweep=True)
+    e2e = time.perf_counter() - t0
+    sw.release()
+
+    def single_combo_loop(kernel, subset=None):
+        """One engine per combination, every block pushed and read back (device frames)."""
+        fb = h * w * 2
+        t_total = 0.0
+        todo = [(M, r, S) for M in SWEEP_MAGS for r in SWEEP_RADII for S in SWEEP_SENS]
+        if subset:
+            todo = todo[::subset]
+        for (M, r, S) in todo:
+            eng = esrrf.LiveSRRF_CL()
+            out = torch.empty((4, h * M, w * M), dtype=torch.float32, device=f"cuda:{local}")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for (st, ln) in SWEEP_BLOCKS:
+                eng.initialise(w, h, M, r, S, ln, ln, chosenDevice=local, kernel=kernel)
+                H = eng.handle
+                esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
+                esrrf._lib.check(H, L.esrrf_calculate_srrf_u16_device(
+                    H, ctypes.c_void_p(d_stack.data_ptr() + st * fb), ln))
+                esrrf._lib.check(H, L.esrrf_read_srrf_device(H, ctypes.c_void_p(out.data_ptr())))
+            torch.cuda.synchronize()
+            t_total += time.perf_counter() - t0
+            eng.release()
+        return t_total * (subset or 1)
+
+    plain_s = single_combo_loop("plain", subset=8) if rank == 0 else 0.0
+    fused_s = single_combo_loop("fused", subset=4) if rank == 0 else 0.0
+    if rank != 0:
+        return
+    line = {
+        "metric": "sweep combos/s (batched, one CUDA graph)", "value": world * combos / t_step,
+        "unit": "combos/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "sweep256: 256x256x200 uint16, radius 0.5..3.0 (11) x S 1..4 x M {2,4} "
+                               "= 88 combinations, blocks [0,37) [37,101) [101,200) [0,100)"},
+        "plain_loop_combos_s": combos / plain_s, "fused_loop_combos_s": combos / fused_s,
+        "speedup_vs_plain_loop": (combos / t_step) / (combos / plain_s),
+        "baseline_note": "single-combination loops re-create the engine per block (as "
+                         "ParametersSweep_ re-initialises per combination); plain loop timed on "
+                         "every 8th combination, fused loop on every 4th, scaled to 88",
+        "e2e": {"value": combos / e2e, "unit": "combos/s", "h2d_bytes_per_step": int(stack.nbytes),
+                "d2h_bytes_per_step": int(h_out.numel() * 4)},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+def run_3d(args, world, rank, local):
+    """3-D MFM workload: 9 planes of 128x128 (a 384x384 camera frame) x 200 timepoints, M3,
+    radius 1.5, S1, AVG+VAR; one block of all timepoints through the engine."""
+    import ctypes
+
+    import torch
+
+    import esrrf
+    from esrrf import synth
+
+    torch.cuda.set_device(local)
+    planes = synth.make_stack("mfm3d", frames=args.frames)
+    n, P, h, w = planes.shape
+    roi = np.array([4, 0, 1, 2, 3, 5, 6, 7, 8], np.float32)[:P]
+    cam = np.zeros((n, 3 * h, 3 * w), np.uint16)
+    for z in range(P):
+        i, j = int(roi[z]) % 3, int(roi[z]) // 3
+        cam[:, j * h:(j + 1) * h, i * w:(i + 1) * w] = planes[:, z]
+    calib = {"X-shift (pixels)": np.linspace(-0.2, 0.2, P), "Y-shift (pixels)": np.linspace(0.1, -0.1, P),
+             "Theta (degrees)": np.linspace(-0.5, 0.5, P), "Axial positions": np.zeros(P),
+             "ROI #": roi, "Intensity scaling": np.ones(P), "Background level (ADC)": np.full(P, 0.0)}
+    M, fwhm, S = 3, 1.5, 1
+    eng = esrrf.LiveSRRF_CL()
+    eng.initialise(3 * w, 3 * h, M, fwhm, S, n, n, chosenDevice=local, doMPmapCorrection=True,
+                   calibTable3DSRRF=calib, framesPerLaunch=args.frames_per_launch or 8)
+    H = eng.handle
+    d_cam = torch.from_numpy(cam.view(np.int16)).to(f"cuda:{local}")
+    d_out = torch.empty((4 * P * M, h * M, w * M), dtype=torch.float32, device=f"cuda:{local}")
+    launches = [0]
+
+    def step():
+        esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
+        esrrf._lib.check(H, L.esrrf_calculate_srrf_u16_device(H, ctypes.c_void_p(d_cam.data_ptr()), n))
+        launches[0] += eng.lastTiming()[2] + 3
+        esrrf._lib.check(H, L.esrrf_read_srrf_device(H, ctypes.c_void_p(d_out.data_ptr())))
+
+    L = esrrf.lib()
+    for _ in range(args.warmup):
+        step()
+    launches[0] = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        torch.cuda.synchronize()
+        t_step = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
+    h_cam = torch.from_numpy(cam.view(np.int16)).pin_memory()
+    h_out = torch.empty((4 * P * M, h * M, w * M), dtype=torch.float32).pin_memory()
+    t0 = time.perf_counter()
+    esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
+    esrrf._lib.check(H, L.esrrf_calculate_srrf_u16(H, ctypes.c_void_p(h_cam.data_ptr()), n))
+    esrrf._lib.check(H, L.esrrf_read_srrf(H, ctypes.c_void_p(h_out.data_ptr())))
+    e2e = time.perf_counter() - t0
+    eng.release()
+    if rank != 0:
+        return
+    mpxf = n * P * h * w / 1e6
+    print(json.dumps({
+        "metric": "input Mpx*frames/s (eSRRF 3-D MFM path)", "value": world * mpxf / t_step,
+        "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"mfm3d: {P} planes of {w}x{h} x {n} timepoints, M3, radius 1.5, S1, "
+                               "AVG+VAR (+TAC2, INT), MP correction, one block", "kernel": "plain per-voxel"},
+        "e2e": {"value": mpxf / e2e, "unit": "Mpx*frames/s", "h2d_bytes_per_step": int(cam.nbytes),
+                "d2h_bytes_per_step": int(h_out.numel() * 4)},
+        "gpu_launches": launches[0] // max(1, args.steps), "clocks": clk.summary()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -369,6 +539,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "sweep256":
+            run_sweep(args, world, rank, local)
+        elif args.workload == "mfm3d":
+            run_3d(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
