@@ -206,6 +206,26 @@ esrrf_status esrrf_sweep_launch_count(const esrrf_sweep* s, int* launches);
 const char* esrrf_sweep_last_error(const esrrf_sweep* s);
 esrrf_status esrrf_sweep_destroy(esrrf_sweep* s);
 
+/* ---- Differentiable eSRRF ---------------------------------------------------------------------
+ * A fidelity loss of the 2-D FHT-path AVG reconstruction and its hand-written adjoint; there is
+ * no counterpart in the reference's OpenCL path (the closest is the post-hoc error map of
+ * ErrorMapLiveSRRF.java:81-233).  With R = (1/T) sum_t I_t C_t^S (S real), B = Gaussian(sigma) * R,
+ * D = M x M box average of B and F the frame average of the input,
+ *   loss = mean((alpha D + beta - F)^2),  alpha, beta the least-squares fit of F on D.
+ * esrrf_loss_and_grad gives the loss and d loss / d(radius, S, sigma) in grads[0..2] and, if
+ * d_grad_frames is non-NULL, d loss / d frames ([T][height][width] float, device).  Zero drift,
+ * intensity weighting on, mean-preserving interpolation; tap boxes 6..22 pixels wide. */
+typedef struct esrrf_adjoint esrrf_adjoint;
+esrrf_status esrrf_adjoint_create(int width, int height, int n_frames, int magnification, int device,
+                                  esrrf_adjoint** out);
+esrrf_status esrrf_adjoint_forward(esrrf_adjoint* a, const float* d_frames, float fwhm,
+                                   float sensitivity, float sigma_b, double* loss);
+esrrf_status esrrf_loss_and_grad(esrrf_adjoint* a, const float* d_frames, float fwhm,
+                                 float sensitivity, float sigma_b, double* loss, double* grads,
+                                 float* d_grad_frames);
+const char* esrrf_adjoint_last_error(const esrrf_adjoint* a);
+esrrf_status esrrf_adjoint_destroy(esrrf_adjoint* a);
+
 /* Allocation-free variant of one FHT-path SR block; it has no counterpart in the reference.
  * For callers that must not allocate device memory when they reconstruct -- e.g. a
  * live-acquisition callback, where cudaMalloc/cudaFree can synchronise the device and stall

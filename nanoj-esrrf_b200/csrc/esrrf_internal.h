@@ -53,6 +53,12 @@ struct InterpScratch {
 cudaError_t interp_plan_create(InterpPlan& plan, int w, int h, int M, int scale_mode);
 void interp_plan_destroy(InterpPlan& plan);
 
+// Adjoint of the interpolation: graw[F][h][w] += L^T gI[F][HM][WM].  dx: Dx row-major [WM][N]
+// (scaled like dxT); scratch T1 [F][N][WM], gX [F][N][N], proj [F][2HM+2WM], dvec [F][2N+1].
+cudaError_t interp_adjoint_run(const InterpPlan& p, const float* dx, const float* gI, int F,
+                               float* T1, float* gX, float* proj, float* dvec, float* graw,
+                               cudaStream_t stream);
+
 // raw: [F][h][w] uint16 (is_u16) or float; out: [F][HM][WM]
 cudaError_t interp_run(const InterpPlan& plan, InterpScratch& scratch, const void* raw,
                        bool is_u16, int F, float* out, cudaStream_t stream, int* launches);
@@ -110,6 +116,9 @@ void fht_fused_tables_free(FhtFusedTables& t);
 cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                           cudaStream_t stream);
 bool fht_fused_supported(const FhtGeometry& g);
+// Per-pixel sum of a [S][S] tap table over the in-image taps, (j, i) order.
+cudaError_t tap_table_sum(const float* tab, int r0, int S, int W, int H, float* out,
+                          cudaStream_t stream);
 
 // AVG/VAR/TAC2/INT from the block accumulators (kernelCalculateVar and the readback's NaN->0).
 // tac_div2: the 2-D bicubic path's double division of TAC2 by (n-1).

@@ -153,6 +153,8 @@ __global__ void __launch_bounds__(256) rank1_vectors_kernel(
 // 64 apart in each direction so that shared-memory reads are conflict free).
 //   PASS 1: C[f] (N x WM)  = X_f (N x N, gathered through the padding tables) . dxT (N x WM)
 //   PASS 2: C[f] (HM x WM) = dy (HM x N) . rowT[f] (N x WM) + rank-one epilogue
+//   PASS 3: C[f] = A (shared, row-major Mr x K) . B[f] (K x Nc)           (adjoint, columns)
+//   PASS 4: C[f] = A[f] (row-major Mr x K) . B (shared, K x Nc)           (adjoint, rows)
 // --------------------------------------------------------------------------------------------
 struct GemmArgs {
     int Mr, Nc, K;
@@ -179,7 +181,8 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
     const int tx = tid & 15, ty = tid >> 4;
     const int f = blockIdx.z;
     const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
-    const float* Bf = (PASS == 1) ? g.B : g.B + (long)f * g.K * g.Nc;
+    const float* Bf = (PASS == 1 || PASS == 4) ? g.B : g.B + (long)f * g.K * g.Nc;
+    const float* Af = (PASS == 4) ? g.A + (long)f * g.Mr * g.K : g.A;
     const void* rawf = nullptr;
     if (PASS == 1)
         rawf = g.is_u16 ? (const void*)((const unsigned short*)g.raw + (long)f * g.w * g.h)
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
                 if (PASS == 1)
                     v = load_raw(rawf, g.is_u16, (long)__ldg(g.srcy + m) * g.w + __ldg(g.srcx + k));
                 else
-                    v = __ldg(g.A + (long)m * g.K + k);
+                    v = __ldg(Af + (long)m * g.K + k);
             }
             ra[i] = v;
         }
@@ -280,7 +283,153 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
     }
 }
 
+// Adjoint of the rank-one terms, step 1: per frame, G c_x and G u_x (rows of G = dL/dI'),
+// G^T c_y and G^T u_y (columns).  Grid (ceil((HM+WM)/8), F), one warp per row or column.
+__global__ void __launch_bounds__(256) adj_proj_kernel(const float* __restrict__ G, int HM, int WM,
+                                                       const float* __restrict__ cx,
+                                                       const float* __restrict__ ux,
+                                                       const float* __restrict__ cy,
+                                                       const float* __restrict__ uy,
+                                                       float* __restrict__ proj) {
+    const int f = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const float* Gf = G + (long)f * HM * WM;
+    float* pr = proj + (long)f * (2 * HM + 2 * WM);
+    if (e < HM) {
+        float a = 0.f, b = 0.f;
+        for (int x = lane; x < WM; x += 32) {
+            const float g = Gf[(long)e * WM + x];
+            a = fmaf(g, cx[x], a);
+            b = fmaf(g, ux[x], b);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) {
+            pr[e] = a;
+            pr[HM + e] = b;
+        }
+    } else if (e < HM + WM) {
+        const int x = e - HM;
+        float a = 0.f, b = 0.f;
+        for (int y = lane; y < HM; y += 32) {
+            const float g = Gf[(long)y * WM + x];
+            a = fmaf(g, cy[y], a);
+            b = fmaf(g, uy[y], b);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) {
+            pr[2 * HM + x] = a;
+            pr[2 * HM + WM + x] = b;
+        }
+    }
+}
+
+// Adjoint of the rank-one terms, step 2 (forward: P = s_a Dy wy, T = s_a Dy flip(wy) + s q cy,
+// Q = s_a Dx wx + s q cx, R = s_a Dx flip(wx) + s q (cx + ux); I' += P cx' + cy Q' - uy R' - T ux'):
+//   dwy[m] = s_a (Dy' Gc)[m] - s_a (Dy' Gu)[(N-m)%N]
+//   dwx[m] = s_a (Dx' Gtc)[m] - s_a (Dx' Gtu)[(N-m)%N]
+//   dq     = s (cy.Gc - uy.(Gc + Gu) - cy.Gu)
+// Grid (ceil(2N/256), F); thread m < N computes dwy[m], N <= m < 2N computes dwx[m - N];
+// block 0 also reduces dq.  dx is Dx row-major [WM][N] (scaled like dxT).
+__global__ void __launch_bounds__(256) adj_rank1_kernel(const float* __restrict__ proj,
+                                                        const float* __restrict__ dy,
+                                                        const float* __restrict__ dx, int N, int HM,
+                                                        int WM, const float* __restrict__ cy,
+                                                        const float* __restrict__ uy, float s_axis,
+                                                        float s, float* __restrict__ dvec) {
+    const int f = blockIdx.y;
+    const float* pr = proj + (long)f * (2 * HM + 2 * WM);
+    float* dv = dvec + (long)f * (2 * N + 1);
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < N) {
+        const int mf = (N - m) & (N - 1);
+        float a = 0.f, b = 0.f;
+        for (int y = 0; y < HM; ++y) {
+            a = fmaf(dy[(long)y * N + m], pr[y], a);
+            b = fmaf(dy[(long)y * N + mf], pr[HM + y], b);
+        }
+        dv[m] = s_axis * (a - b);
+    } else if (m < 2 * N) {
+        const int mm = m - N, mf = (N - mm) & (N - 1);
+        float a = 0.f, b = 0.f;
+        for (int x = 0; x < WM; ++x) {
+            a = fmaf(dx[(long)x * N + mm], pr[2 * HM + x], a);
+            b = fmaf(dx[(long)x * N + mf], pr[2 * HM + WM + x], b);
+        }
+        dv[N + mm] = s_axis * (a - b);
+    }
+    if (blockIdx.x == 0) {
+        __shared__ float red[8];
+        float q = 0.f;
+        for (int y = threadIdx.x; y < HM; y += blockDim.x)
+            q += cy[y] * pr[y] - uy[y] * (pr[y] + pr[HM + y]) - cy[y] * pr[HM + y];
+        for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = q;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float t = 0.f;
+            for (int i = 0; i < 8; ++i) t += red[i];
+            dv[2 * N] = s * t;
+        }
+    }
+}
+
+// dL/draw: padded-frame gradient (dense part + rank-one part) scattered through the mirror
+// padding tables, plus the frame-average term dF / T.  Grid (ceil(N/256), N, F).
+__global__ void adj_scatter_kernel(const float* __restrict__ gX, const float* __restrict__ dvec,
+                                   int N, int w, int h, const int* __restrict__ srcx,
+                                   const int* __restrict__ srcy, int identity,
+                                   float* __restrict__ graw) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const long f = blockIdx.z;
+    if (x >= N) return;
+    const float* dv = dvec + f * (2 * N + 1);
+    const float vx = (x & 1) ? -1.f : 1.f, vy = (y & 1) ? -1.f : 1.f;
+    const float val = gX[(f * N + y) * (long)N + x] + dv[y] * vx + vy * dv[N + x] + dv[2 * N] * vx * vy;
+    float* dst = graw + f * (long)w * h + (long)srcy[y] * w + srcx[x];
+    if (identity)
+        *dst += val;
+    else
+        atomicAdd(dst, val);
+}
+
 }  // namespace
+
+cudaError_t interp_adjoint_run(const InterpPlan& p, const float* dx, const float* gI, int F,
+                               float* T1, float* gX, float* proj, float* dvec, float* graw,
+                               cudaStream_t stream) {
+    // graw must hold the frame-average term (or zeros) on entry; this adds L^T gI.
+    const int N = p.N;
+    GemmArgs g{};
+    g.Mr = N;
+    g.K = p.HM;
+    g.Nc = p.WM;
+    g.A = p.dyT;   // [N][HM]
+    g.B = gI;      // [F][HM][WM]
+    g.C = T1;      // [F][N][WM]
+    gemm_kernel<3><<<dim3((g.Nc + 127) / 128, (g.Mr + 127) / 128, F), 256, 0, stream>>>(g);
+    g.Mr = N;
+    g.K = p.WM;
+    g.Nc = N;
+    g.A = T1;      // [F][N][WM]
+    g.B = dx;      // [WM][N]
+    g.C = gX;      // [F][N][N]
+    gemm_kernel<4><<<dim3((g.Nc + 127) / 128, (g.Mr + 127) / 128, F), 256, 0, stream>>>(g);
+    adj_proj_kernel<<<dim3((p.HM + p.WM + 7) / 8, F), 256, 0, stream>>>(gI, p.HM, p.WM, p.cx, p.ux,
+                                                                         p.cy, p.uy, proj);
+    adj_rank1_kernel<<<dim3((2 * N + 255) / 256, F), 256, 0, stream>>>(
+        proj, p.dy, dx, N, p.HM, p.WM, p.cy, p.uy, (float)p.s_axis, (float)p.s, dvec);
+    adj_scatter_kernel<<<dim3((N + 255) / 256, N, F), 256, 0, stream>>>(
+        gX, dvec, N, p.w, p.h, p.srcx, p.srcy, p.identity_pad ? 1 : 0, graw);
+    return cudaGetLastError();
+}
 
 cudaError_t interp_plan_create(InterpPlan& p, int w, int h, int M, int scale_mode) {
     p.w = w;

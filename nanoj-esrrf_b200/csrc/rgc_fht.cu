@@ -490,6 +490,14 @@ cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const F
     }
 }
 
+// Sum of a tap table over the in-image taps of every pixel (the wsum_kernel above, exported).
+cudaError_t tap_table_sum(const float* tab, int r0, int S, int W, int H, float* out,
+                          cudaStream_t stream) {
+    const long wh = (long)W * H;
+    wsum_kernel<<<(unsigned)((wh + 255) / 256), 256, 0, stream>>>(tab, r0, S, W, H, out);
+    return cudaGetLastError();
+}
+
 bool fht_fused_supported(const FhtGeometry& g) { return g.S >= 4 && g.S <= 32 && g.S % 2 == 0; }
 
 cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out,

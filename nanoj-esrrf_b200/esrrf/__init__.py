@@ -320,3 +320,91 @@ def rolling(stack, magnification, fwhm, sensitivity, blocks, int_weighting=True)
         return {k[3]: v.copy() for k, v in res.items()}
     finally:
         sw.release()
+
+
+class Adjoint:
+    """Differentiable eSRRF (esrrf_adjoint_*, esrrf_loss_and_grad): a re-blur fidelity loss of the
+    2-D FHT-path AVG reconstruction and its gradients w.r.t. radius, a real sensitivity, the
+    re-blur sigma and every input pixel.  Frames are passed as a torch CUDA tensor (float32,
+    [T][h][w]) or a numpy array (copied to the device)."""
+
+    def __init__(self, width, height, n_frames, magnification, device=0):
+        h = ctypes.c_void_p()
+        _lib.check(None, lib().esrrf_adjoint_create(int(width), int(height), int(n_frames),
+                                                    int(magnification), int(device), ctypes.byref(h)),
+                   adjoint=True)
+        self._h = h
+        self.shape = (int(n_frames), int(height), int(width))
+        self.device = int(device)
+
+    def _dev(self, frames):
+        import torch
+
+        if isinstance(frames, torch.Tensor):
+            t = frames.to(device=f"cuda:{self.device}", dtype=torch.float32).contiguous()
+        else:
+            t = torch.from_numpy(np.ascontiguousarray(frames, np.float32)).to(f"cuda:{self.device}")
+        assert tuple(t.shape) == self.shape, (tuple(t.shape), self.shape)
+        return t
+
+    def loss(self, frames, fwhm, sensitivity, sigma):
+        t = self._dev(frames)
+        L = ctypes.c_double()
+        _lib.check(self._h, lib().esrrf_adjoint_forward(self._h, ctypes.c_void_p(t.data_ptr()),
+                                                        float(fwhm), float(sensitivity), float(sigma),
+                                                        ctypes.byref(L)), adjoint=True)
+        return L.value
+
+    def loss_and_grad(self, frames, fwhm, sensitivity, sigma, pixel_grad=True):
+        """(loss, {"fwhm", "S", "sigma"}, d loss / d frames as a torch tensor or None)."""
+        import torch
+
+        t = self._dev(frames)
+        L = ctypes.c_double()
+        g = (ctypes.c_double * 3)()
+        gf = torch.empty_like(t) if pixel_grad else None
+        _lib.check(self._h, lib().esrrf_loss_and_grad(
+            self._h, ctypes.c_void_p(t.data_ptr()), float(fwhm), float(sensitivity), float(sigma),
+            ctypes.byref(L), g, ctypes.c_void_p(gf.data_ptr() if gf is not None else None)), adjoint=True)
+        return L.value, {"fwhm": g[0], "S": g[1], "sigma": g[2]}, gf
+
+    def release(self):
+        if self._h:
+            lib().esrrf_adjoint_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def gradient_search(adj, frames, fwhm0, sens0, sigma0, steps=40, lr=(0.05, 0.1, 0.05),
+                    bounds=((0.5, 3.0), (0.5, 6.0), (0.5, 8.0))):
+    """Projected gradient descent with a backtracking step on (radius, sensitivity, re-blur
+    sigma), the search that stands beside the grid sweep.  Returns the trajectory."""
+    x = np.array([fwhm0, sens0, sigma0], np.float64)
+    lo = np.array([b[0] for b in bounds])
+    hi = np.array([b[1] for b in bounds])
+    step = np.array(lr, np.float64)
+    L, g, _ = adj.loss_and_grad(frames, *x, pixel_grad=False)
+    traj = [(x.copy(), L)]
+    for _ in range(steps):
+        gv = np.array([g["fwhm"], g["S"], g["sigma"]])
+        scale = np.abs(gv).max() or 1.0
+        accepted = False
+        for _ in range(8):
+            xn = np.clip(x - step * gv / scale, lo, hi)
+            Ln = adj.loss(frames, *xn)
+            if Ln < L:
+                accepted = True
+                break
+            step = step * 0.5
+        if not accepted:
+            break
+        x = xn
+        L, g, _ = adj.loss_and_grad(frames, *x, pixel_grad=False)
+        step = step * 1.5
+        traj.append((x.copy(), L))
+    return traj

@@ -101,6 +101,14 @@ SIGNATURES.update({
     "esrrf_sweep_launch_count": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
     "esrrf_sweep_last_error": (_c.c_char_p, [_c.c_void_p]),
     "esrrf_sweep_destroy": (_c.c_int, [_c.c_void_p]),
+    "esrrf_adjoint_create": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_int,
+                                        _c.POINTER(_c.c_void_p)]),
+    "esrrf_adjoint_forward": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_float, _c.c_float,
+                                         _c.c_float, _c.POINTER(_c.c_double)]),
+    "esrrf_loss_and_grad": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_float, _c.c_float, _c.c_float,
+                                       _c.POINTER(_c.c_double), _c.POINTER(_c.c_double), _c.c_void_p]),
+    "esrrf_adjoint_last_error": (_c.c_char_p, [_c.c_void_p]),
+    "esrrf_adjoint_destroy": (_c.c_int, [_c.c_void_p]),
 })
 
 _LIB = None
@@ -121,9 +129,11 @@ def lib():
     return _LIB
 
 
-def check(handle, rc: int, sweep: bool = False) -> None:
+def check(handle, rc: int, sweep: bool = False, adjoint: bool = False) -> None:
     if rc == 0:
         return
-    msg = (lib().esrrf_sweep_last_error if sweep else lib().esrrf_last_error)(handle)
+    fn = lib().esrrf_adjoint_last_error if adjoint else (
+        lib().esrrf_sweep_last_error if sweep else lib().esrrf_last_error)
+    msg = fn(handle)
     msg = msg.decode() if msg else ""
     raise EsrrfError(f"esrrf status {STATUS.get(rc, rc)}: {msg}")
