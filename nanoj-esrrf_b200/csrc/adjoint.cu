@@ -284,7 +284,9 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
                         const float dot = fmaf(-gy[k], (float)rr, Ak[k]);
                         const float c = fmaf(gx[k], (float)rr, Bk[k]);
                         if (dot < 0.f) {
-                            const float sv = copysignf(wd[jj] * bv, c);
+                            // (w/d) b sgn(c): flip the sign bit of (w/d) b by that of c
+                            const float sv = __int_as_float(__float_as_int(wd[jj] * bv) ^
+                                                            (__float_as_int(c) & 0x80000000));
                             Sx[k] += sv;
                             Tx[k] = fmaf(sv, (float)rr, Tx[k]);
                             Sy[k] = fmaf(sv, tx_f, Sy[k]);
