@@ -40,6 +40,7 @@ WORKLOADS = {
     "fht64": ("fht64", 100),     # 2-D FHT path, 64x64 M5
     "sweep256": ("sweep256", 0),  # batched parameter sweep (88 combinations, uneven blocks)
     "mfm3d": ("mfm3d", 200),     # 3-D MFM path, 9 planes
+    "adjoint256": ("adjoint256", 100),  # differentiable eSRRF: loss + gradients
 }
 SWEEP_RADII = [0.5 + 0.25 * i for i in range(11)]
 SWEEP_SENS = [1, 2, 3, 4]
@@ -521,6 +522,71 @@ def run_3d(args, world, rank, local):
         "gpu_launches": launches[0] // max(1, args.steps), "clocks": clk.summary()}))
 
 
+def run_adjoint(args, world, rank, local):
+    """Differentiable eSRRF on 256x256x100, M4: forward (loss) time, loss-and-gradient time, their
+    ratio, and a gradient search on (radius, sensitivity, re-blur sigma) beside a grid search."""
+    import torch
+
+    import esrrf
+    from esrrf import synth
+
+    torch.cuda.set_device(local)
+    stack = synth.make_stack("adjoint256").astype(np.float32)
+    n, h, w = stack.shape
+    M = 4
+    adj = esrrf.Adjoint(w, h, n, M, device=local)
+    d = torch.from_numpy(stack).to(f"cuda:{local}")
+    x0 = (1.5, 2.0, 1.5)
+    for _ in range(args.warmup):
+        adj.loss(d, *x0)
+        adj.loss_and_grad(d, *x0)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            adj.loss(d, *x0)
+        torch.cuda.synchronize()
+        t_f = (time.perf_counter() - t0) / args.steps
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            L, g, gf = adj.loss_and_grad(d, *x0)
+        torch.cuda.synchronize()
+        t_fb = (time.perf_counter() - t0) / args.steps
+    t_f = max_over_ranks(world, t_f)
+    t_fb = max_over_ranks(world, t_fb)
+    # grid search (forward only) and gradient search
+    grid = []
+    t0 = time.perf_counter()
+    for r in SWEEP_RADII:
+        for S in SWEEP_SENS:
+            for sg in (1.0, 1.5, 2.0, 3.0):
+                grid.append((adj.loss(d, r, S, sg), r, S, sg))
+    t_grid = time.perf_counter() - t0
+    best = min(grid)
+    t0 = time.perf_counter()
+    traj = esrrf.gradient_search(adj, d, 1.0, 1.0, 1.5, steps=25)
+    t_gs = time.perf_counter() - t0
+    adj.release()
+    if rank != 0:
+        return
+    xg, Lg = traj[-1]
+    print(json.dumps({
+        "metric": "adjoint time / forward time (loss + all gradients vs loss)", "value": (t_fb - t_f) / t_f,
+        "unit": "ratio", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_fb * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "adjoint256: 256x256x100, M4, AVG, loss = re-blur MSE vs frame mean "
+                               "(alpha, beta refit), gradients w.r.t. radius, S, sigma and all 6.6 M input pixels"},
+        "forward_ms": t_f * 1e3, "loss_and_grad_ms": t_fb * 1e3,
+        "forward_input_mpx_frames_s": n * h * w / 1e6 / t_f,
+        "grid_search": {"evaluations": len(grid), "seconds": t_grid, "best_loss": best[0],
+                        "best": {"radius": best[1], "S": best[2], "sigma": best[3]}},
+        "gradient_search": {"iterations": len(traj) - 1, "seconds": t_gs, "loss": Lg,
+                            "x": {"radius": float(xg[0]), "S": float(xg[1]), "sigma": float(xg[2])}},
+        "e2e": {"value": (t_fb - t_f) / t_f, "unit": "ratio", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -543,6 +609,8 @@ def main():
             run_sweep(args, world, rank, local)
         elif args.workload == "mfm3d":
             run_3d(args, world, rank, local)
+        elif args.workload == "adjoint256":
+            run_adjoint(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -214,7 +214,7 @@ esrrf_status esrrf_sweep_destroy(esrrf_sweep* s);
  *   loss = mean((alpha D + beta - F)^2),  alpha, beta the least-squares fit of F on D.
  * esrrf_loss_and_grad gives the loss and d loss / d(radius, S, sigma) in grads[0..2] and, if
  * d_grad_frames is non-NULL, d loss / d frames ([T][height][width] float, device).  Zero drift,
- * intensity weighting on, mean-preserving interpolation; tap boxes 6..22 pixels wide. */
+ * intensity weighting on, mean-preserving interpolation; tap boxes 6..26 pixels wide. */
 typedef struct esrrf_adjoint esrrf_adjoint;
 esrrf_status esrrf_adjoint_create(int width, int height, int n_frames, int magnification, int device,
                                   esrrf_adjoint** out);

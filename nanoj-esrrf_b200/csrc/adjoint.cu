@@ -459,6 +459,8 @@ cudaError_t launch_adj_any(int S, const AdjAArgs& a, const AdjBArgs& b, bool bac
         case 18: return launch_adj<18>(a, b, backward_b, st);
         case 20: return launch_adj<20>(a, b, backward_b, st);
         case 22: return launch_adj<22>(a, b, backward_b, st);
+        case 24: return launch_adj<24>(a, b, backward_b, st);
+        case 26: return launch_adj<26>(a, b, backward_b, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -535,8 +537,8 @@ esrrf_status esrrf_adjoint::set_radius(float fwhm) {
     tabA = nullptr;
     wdB = kwtab = nullptr;
     geo = fht_geometry(M, fwhm, 1);
-    if (!fht_fused_supported(geo) || geo.S < 6 || geo.S > 22)
-        return fail(ESRRF_ERR_INVALID, "radius gives a tap box outside 6..22 pixels for the adjoint");
+    if (!fht_fused_supported(geo) || geo.S < 6 || geo.S > 26)
+        return fail(ESRRF_ERR_INVALID, "radius gives a tap box outside 6..26 pixels for the adjoint");
     AK(fht_fused_tables(geo, WM, HM, tables, stream), "RGC tables");
     const int S = geo.S;
     std::vector<float4> ta(S * S);
