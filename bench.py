@@ -564,7 +564,9 @@ def run_adjoint(args, world, rank, local):
     t_grid = time.perf_counter() - t0
     best = min(grid)
     t0 = time.perf_counter()
-    traj = esrrf.gradient_search(adj, d, 1.0, 1.0, 1.5, steps=25)
+    # same domain as the grid: radius 0.5..3.0, S 1..4, sigma 0.5..8
+    traj = esrrf.gradient_search(adj, d, 1.0, 2.0, 1.5, steps=25,
+                                 bounds=((0.5, 3.0), (1.0, 4.0), (0.5, 8.0)))
     t_gs = time.perf_counter() - t0
     adj.release()
     if rank != 0:
