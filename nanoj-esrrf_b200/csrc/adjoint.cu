@@ -727,8 +727,8 @@ esrrf_status esrrf_adjoint_create(int width, int height, int n_frames, int magni
     const long P = (long)a->WM * a->HM, p = (long)width * height;
     auto al = [&](auto** ptr, size_t bytes) { return cudaMalloc((void**)ptr, bytes); };
     if ((e = al(&a->scratch.rowT, sizeof(float) * Fc * (size_t)N * a->WM)) != cudaSuccess ||
-        (e = al(&a->scratch.alt, sizeof(float) * Fc * (size_t)(2 * N + 1))) != cudaSuccess ||
-        (e = al(&a->scratch.vec, sizeof(float) * Fc * (size_t)(2 * a->HM + 2 * a->WM))) != cudaSuccess ||
+        (e = al(&a->scratch.alt, sizeof(float) * Fc * interp_alt_floats(N))) != cudaSuccess ||
+        (e = al(&a->scratch.vec, sizeof(float) * Fc * interp_vec_floats(a->HM, a->WM))) != cudaSuccess ||
         (e = al(&a->dx, sizeof(float) * (size_t)a->WM * N)) != cudaSuccess ||
         (e = al(&a->dwsum, sizeof(float) * P)) != cudaSuccess ||
         (e = al(&a->I, sizeof(float) * P * n_frames)) != cudaSuccess ||

@@ -217,8 +217,8 @@ esrrf_status esrrf_handle::init_fht() {
     const long whM = (long)WM * HM;
     scratch.capacity = F;
     CK(cudaMalloc(&scratch.rowT, sizeof(float) * (size_t)F * plan.N * WM));
-    CK(cudaMalloc(&scratch.alt, sizeof(float) * (size_t)F * (2 * plan.N + 1)));
-    CK(cudaMalloc(&scratch.vec, sizeof(float) * (size_t)F * (2 * HM + 2 * WM)));
+    CK(cudaMalloc(&scratch.alt, sizeof(float) * (size_t)F * interp_alt_floats(plan.N)));
+    CK(cudaMalloc(&scratch.vec, sizeof(float) * (size_t)F * interp_vec_floats(HM, WM)));
     CK(cudaMalloc(&d_interp, sizeof(float) * (size_t)F * whM));
     CK(cudaMalloc(&d_gx, sizeof(float) * (size_t)F * whM));
     CK(cudaMalloc(&d_gy, sizeof(float) * (size_t)F * whM));

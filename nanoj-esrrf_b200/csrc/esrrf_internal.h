@@ -46,9 +46,11 @@ struct InterpPlan {
 struct InterpScratch {
     int capacity = 0;
     float* rowT = nullptr;    // [F][N][WM]  first-pass output
-    float* alt = nullptr;     // [F][2N+1]   alternating row sums, column sums, q
-    float* vec = nullptr;     // [F][2HM+2WM] P, T (rows) and Q, R (columns)
+    float* alt = nullptr;     // [F][interp_alt_floats(N)]  alternating row/column sums, row sums
+    float* vec = nullptr;     // [F][interp_vec_floats(HM, WM)]  P, T, Q, R and the frame mean
 };
+inline size_t interp_alt_floats(int N) { return 3 * (size_t)N + 1; }
+inline size_t interp_vec_floats(int HM, int WM) { return 2 * (size_t)HM + 2 * (size_t)WM + 1; }
 
 cudaError_t interp_plan_create(InterpPlan& plan, int w, int h, int M, int scale_mode);
 void interp_plan_destroy(InterpPlan& plan);

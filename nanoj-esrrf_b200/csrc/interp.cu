@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u
     const int f = blockIdx.y;
     const void* frame = is_u16 ? (const void*)((const unsigned short*)raw + (long)f * w * h)
                                : (const void*)((const float*)raw + (long)f * w * h);
-    float* out = alt + (long)f * (2 * N + 1);
+    float* out = alt + (long)f * (3 * N + 1);
     __shared__ double red[8][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int base = blockIdx.x * 32;
@@ -79,8 +79,16 @@ __global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u
             const float v = load_raw(frame, is_u16, rowoff + srcx[x]);
             acc += (x & 1) ? -(double)v : (double)v;
         }
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) out[y] = (float)acc;
+        double tot = 0.0;
+        for (int x = lane; x < N; x += 32) tot += (double)load_raw(frame, is_u16, rowoff + srcx[x]);
+        for (int o = 16; o > 0; o >>= 1) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if (lane == 0) {
+            out[y] = (float)acc;
+            out[2 * N + 1 + y] = (float)tot;  // plain row sum, for the frame mean
+        }
     }
     // columns base .. base+31: lane = column, warps stride the rows
     const int x = base + lane;
@@ -110,22 +118,38 @@ __global__ void __launch_bounds__(256) rank1_vectors_kernel(
     const float* __restrict__ cx, const float* __restrict__ ux, const float* __restrict__ cy,
     int N, int HM, int WM, float s_axis, float s, float* __restrict__ vec) {
     extern __shared__ float wsh[];  // [2N]: wy then wx
-    __shared__ float qred[8];
+    __shared__ float qred[8], mred[8];
     const int f = blockIdx.y;
-    const float* a = alt + (long)f * (2 * N + 1);
-    float qp = 0.f;  // q = sum_y (-1)^y wy[y]
+    const float* a = alt + (long)f * (3 * N + 1);
+    float qp = 0.f, mp = 0.f;  // q = sum_y (-1)^y wy[y]; frame sum from the row sums
     for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) {
         const float v = a[i];
         wsh[i] = v;
-        if (i < N) qp += (i & 1) ? -v : v;
+        if (i < N) {
+            qp += (i & 1) ? -v : v;
+            mp += a[2 * N + 1 + i];
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) qp += __shfl_xor_sync(0xffffffffu, qp, o);
-    if ((threadIdx.x & 31) == 0) qred[threadIdx.x >> 5] = qp;
+    for (int o = 16; o > 0; o >>= 1) {
+        qp += __shfl_xor_sync(0xffffffffu, qp, o);
+        mp += __shfl_xor_sync(0xffffffffu, mp, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        qred[threadIdx.x >> 5] = qp;
+        mred[threadIdx.x >> 5] = mp;
+    }
     __syncthreads();
-    float q = 0.f;
-    for (int i = 0; i < 8; ++i) q += qred[i];
+    float q = 0.f, msum = 0.f;
+    for (int i = 0; i < 8; ++i) {
+        q += qred[i];
+        msum += mred[i];
+    }
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    float* v = vec + (long)f * (2 * HM + 2 * WM);
+    float* v = vec + (long)f * (2 * HM + 2 * WM + 1);
+    // The dense passes interpolate X - c (c = frame mean) and add c s N^2 back: the map sends a
+    // constant to (s N^2) times it, and the alternating sums of a constant vanish (N even), so
+    // this only shrinks the GEMM summands.
+    if (e == 0) v[2 * HM + 2 * WM] = msum / ((float)N * (float)N);
     if (e < HM) {
         float d0 = 0.f, d1 = 0.f;
         for (int y = 0; y < N; ++y) {
@@ -171,6 +195,7 @@ struct GemmArgs {
     const float* cy;
     const float* uy;
     int HM, WM;
+    float cscale;      // pass 2: s N^2 (1 for the mean-preserving scale)
 };
 
 template <int PASS>
@@ -184,9 +209,12 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
     const float* Bf = (PASS == 1 || PASS == 4) ? g.B : g.B + (long)f * g.K * g.Nc;
     const float* Af = (PASS == 4) ? g.A + (long)f * g.Mr * g.K : g.A;
     const void* rawf = nullptr;
-    if (PASS == 1)
+    float cmean = 0.f;
+    if (PASS == 1) {
         rawf = g.is_u16 ? (const void*)((const unsigned short*)g.raw + (long)f * g.w * g.h)
                         : (const void*)((const float*)g.raw + (long)f * g.w * g.h);
+        cmean = g.vec[(long)f * (2 * g.HM + 2 * g.WM + 1) + 2 * g.HM + 2 * g.WM];
+    }
 
     // global-load mapping
     const int a_row = tid >> 1, a_k = (tid & 1) * 4;   // A: 128 rows x 8 k
@@ -201,7 +229,7 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
             float v = 0.f;
             if (m < g.Mr && k < g.K) {
                 if (PASS == 1)
-                    v = load_raw(rawf, g.is_u16, (long)__ldg(g.srcy + m) * g.w + __ldg(g.srcx + k));
+                    v = load_raw(rawf, g.is_u16, (long)__ldg(g.srcy + m) * g.w + __ldg(g.srcx + k)) - cmean;
                 else
                     v = __ldg(Af + (long)m * g.K + k);
             }
@@ -257,7 +285,8 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
     }
 
     float* Cf = g.C + (long)f * g.Mr * g.Nc;
-    const float* vec = (PASS == 2) ? g.vec + (long)f * (2 * g.HM + 2 * g.WM) : nullptr;
+    const float* vec = (PASS == 2) ? g.vec + (long)f * (2 * g.HM + 2 * g.WM + 1) : nullptr;
+    const float cback = (PASS == 2) ? vec[2 * g.HM + 2 * g.WM] * g.cscale : 0.f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
@@ -276,7 +305,7 @@ __global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
             float v = acc[i][j];
             if (PASS == 2) {
                 const float qn = vec[2 * g.HM + n], rn = vec[2 * g.HM + g.WM + n];
-                v += pm * g.cx[n] + cym * qn - uym * rn - tm * g.ux[n];
+                v += pm * g.cx[n] + cym * qn - uym * rn - tm * g.ux[n] + cback;
             }
             Cf[(long)m * g.Nc + n] = v;
         }
@@ -526,6 +555,8 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
     g.srcy = p.srcy;
     g.HM = p.HM;
     g.WM = p.WM;
+    g.vec = sc.vec;
+    g.cscale = (float)(p.s * (double)N * (double)N);
     // pass 1: rows of the padded frame times dxT
     g.Mr = N;
     g.Nc = p.WM;

@@ -56,8 +56,8 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 size_t chunk_bytes(const esrrf::InterpPlan& p, int F) {
     const size_t whM = (size_t)p.WM * p.HM;
     return align256(sizeof(float) * (size_t)F * p.N * p.WM)        // first-pass rows
-           + align256(sizeof(float) * (size_t)F * (2 * p.N + 1))   // alternating sums
-           + align256(sizeof(float) * (size_t)F * (2 * p.HM + 2 * p.WM))  // rank-one vectors
+           + align256(sizeof(float) * (size_t)F * esrrf::interp_alt_floats(p.N))   // alternating sums
+           + align256(sizeof(float) * (size_t)F * esrrf::interp_vec_floats(p.HM, p.WM))  // rank-one vectors
            + align256(sizeof(float) * (size_t)F * whM)             // interpolated frames
            + align256(sizeof(double) * 4 * whM)                    // block accumulators
            + align256(sizeof(float) * whM);                        // previous X
@@ -129,9 +129,9 @@ esrrf_status esrrf_fht_block_noalloc(const void* d_frames, int is_u16, int n_fra
     sc.rowT = (float*)(base + off);
     off += align256(sizeof(float) * (size_t)F * plan.N * plan.WM);
     sc.alt = (float*)(base + off);
-    off += align256(sizeof(float) * (size_t)F * (2 * plan.N + 1));
+    off += align256(sizeof(float) * (size_t)F * interp_alt_floats(plan.N));
     sc.vec = (float*)(base + off);
-    off += align256(sizeof(float) * (size_t)F * (2 * plan.HM + 2 * plan.WM));
+    off += align256(sizeof(float) * (size_t)F * interp_vec_floats(plan.HM, plan.WM));
     float* interp = (float*)(base + off);
     off += align256(sizeof(float) * (size_t)F * whM);
     BlockState st;

@@ -321,8 +321,8 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
     size_t maxHM = 0;
     for (auto& m : s->mp) maxHM = std::max(maxHM, (size_t)m.plan.HM);
     if ((e = cudaMalloc(&s->scratch.rowT, sizeof(float) * Fi * (size_t)maxN * maxWM)) != cudaSuccess ||
-        (e = cudaMalloc(&s->scratch.alt, sizeof(float) * Fi * (size_t)(2 * maxN + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&s->scratch.vec, sizeof(float) * Fi * (2 * maxHM + 2 * (size_t)maxWM))) != cudaSuccess ||
+        (e = cudaMalloc(&s->scratch.alt, sizeof(float) * Fi * interp_alt_floats(maxN))) != cudaSuccess ||
+        (e = cudaMalloc(&s->scratch.vec, sizeof(float) * Fi * interp_vec_floats((int)maxHM, maxWM))) != cudaSuccess ||
         (e = cudaMalloc(&s->d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||
         (e = cudaMalloc(&s->d_cg, sizeof(float) * (size_t)T * maxP)) != cudaSuccess)
         return bail(s->fail_cuda(e, "sweep buffers"));
