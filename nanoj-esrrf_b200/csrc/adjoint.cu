@@ -596,6 +596,9 @@ esrrf_status esrrf_adjoint::forward(const float* frames, float fwhm, float sens,
     double st[5];
     AK(cudaMemcpyAsync(st, dstat, sizeof(double) * 5, cudaMemcpyDeviceToHost, stream), "stats");
     AK(cudaStreamSynchronize(stream), "forward");
+    bool tc_failed = false;
+    AK(interp_tc_check(plan, stream, &tc_failed), "interpolation status");
+    if (tc_failed) return fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
     const double n = (double)p;
     const double md = st[0] / n, mf = st[1] / n;
     const double vdd = st[2] / n - md * md, vdf = st[3] / n - md * mf;

@@ -481,7 +481,10 @@ esrrf_status esrrf_handle::read(float* out, bool on_device) {
     const size_t bytes = sizeof(float) * 4 * (size_t)st.pixels;
     CK(cudaMemcpyAsync(out, d_out, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                        stream));
-    CK(cudaStreamSynchronize(stream));
+    bool tc_failed = false;
+    CK(interp_tc_check(plan, stream, &tc_failed));  // synchronises the stream
+    if (tc_failed)
+        return fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
     return ESRRF_OK;
 }
 

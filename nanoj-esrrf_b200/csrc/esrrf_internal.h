@@ -40,6 +40,10 @@ struct InterpPlan {
     float* uy = nullptr;      // [HM]
     int* srcx = nullptr;      // [N] source column of padded column
     int* srcy = nullptr;      // [N] source row of padded row
+    // tensor-core passes (tc): Dx row-major and a device flag set when a bounded wait gave up
+    bool tc = false;
+    float* dx = nullptr;      // [WM][N]   (scaled like dxT)
+    int* tc_err = nullptr;
 };
 
 // Per-frame interpolation scratch for a chunk of F frames.
@@ -60,6 +64,14 @@ void interp_plan_destroy(InterpPlan& plan);
 cudaError_t interp_adjoint_run(const InterpPlan& p, const float* dx, const float* gI, int F,
                                float* T1, float* gX, float* proj, float* dvec, float* graw,
                                cudaStream_t stream);
+
+// Tensor-core (tcgen05, three-term TF32) form of the two dense passes; needs N % 32 == 0.
+// Writes the first-pass rows transposed into scratch.rowT ([F][WM][N]).
+bool tc_interp_supported(const InterpPlan& plan);
+cudaError_t tc_interp_passes(const InterpPlan& plan, InterpScratch& scratch, const void* raw,
+                             bool is_u16, int F, float* out, cudaStream_t stream);
+// Reads (and clears) the plan's tensor-core failure flag; synchronises `stream`.
+cudaError_t interp_tc_check(const InterpPlan& plan, cudaStream_t stream, bool* failed);
 
 // raw: [F][h][w] uint16 (is_u16) or float; out: [F][HM][WM]
 cudaError_t interp_run(const InterpPlan& plan, InterpScratch& scratch, const void* raw,

@@ -12,6 +12,8 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 
 #include "esrrf_internal.h"
 
@@ -517,6 +519,22 @@ cudaError_t interp_plan_create(InterpPlan& p, int w, int h, int M, int scale_mod
     if ((e = upload(&p.uy, uy)) != cudaSuccess) return e;
     if ((e = upload(&p.srcx, sx)) != cudaSuccess) return e;
     if ((e = upload(&p.srcy, sy)) != cudaSuccess) return e;
+    // Tensor-core passes on compute capability 10.x unless ESRRF_INTERP_GEMM=simt selects the
+    // FP32 SIMT kernels.
+    const char* sel = std::getenv("ESRRF_INTERP_GEMM");
+    int dev = 0, major = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev)) != cudaSuccess)
+        return e;
+    p.tc = major == 10 && tc_interp_supported(p) && !(sel && std::strcmp(sel, "simt") == 0);
+    if (p.tc) {
+        std::vector<float> dx((size_t)p.WM * N);
+        for (int n = 0; n < p.WM; ++n)
+            for (int m = 0; m < N; ++m) dx[(size_t)n * N + m] = dxT[(size_t)m * p.WM + n];
+        if ((e = upload(&p.dx, dx)) != cudaSuccess) return e;
+        if ((e = cudaMalloc((void**)&p.tc_err, sizeof(int))) != cudaSuccess) return e;
+        if ((e = cudaMemset(p.tc_err, 0, sizeof(int))) != cudaSuccess) return e;
+    }
     return cudaSuccess;
 }
 
@@ -530,6 +548,8 @@ void interp_plan_destroy(InterpPlan& p) {
     cudaFree(p.uy);
     cudaFree(p.srcx);
     cudaFree(p.srcy);
+    cudaFree(p.dx);
+    cudaFree(p.tc_err);
     p = InterpPlan();
 }
 
@@ -545,6 +565,11 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
         rank1_vectors_kernel<<<grid, 256, sizeof(float) * 2 * N, stream>>>(
             sc.alt, p.dyT, p.dxT, p.cx, p.ux, p.cy, N, p.HM, p.WM, (float)p.s_axis, (float)p.s,
             sc.vec);
+    }
+    if (p.tc) {
+        if (launches) *launches += 4;
+        cudaError_t e = cudaGetLastError();
+        return e != cudaSuccess ? e : tc_interp_passes(p, sc, raw, is_u16, F, out, stream);
     }
     GemmArgs g{};
     g.raw = raw;

@@ -339,6 +339,16 @@ esrrf_status esrrf_sweep_output_layout(const esrrf_sweep* s, size_t* total_float
     return ESRRF_OK;
 }
 
+// Reads every plan's tensor-core failure flag after the stream has drained.
+static esrrf_status sweep_tc_check(esrrf_sweep* s) {
+    for (auto& m : s->mp) {
+        bool failed = false;
+        SK(interp_tc_check(m.plan, s->stream, &failed), "interpolation status");
+        if (failed) return s->fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
+    }
+    return ESRRF_OK;
+}
+
 static esrrf_status sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out) {
     if (cudaSetDevice(s->device) != cudaSuccess) return s->fail(ESRRF_ERR_CUDA, "cudaSetDevice failed");
     // The graph bakes in the input and output pointers: (re)capture when they change.
@@ -366,11 +376,11 @@ static esrrf_status sweep_run_device(esrrf_sweep* s, const void* d_frames, int i
         s->g_out = d_out;
         s->g_u16 = is_u16;
         SK(cudaStreamSynchronize(s->stream), "sweep");
-        return ESRRF_OK;
+        return sweep_tc_check(s);
     }
     SK(cudaGraphLaunch(s->exec, s->stream), "graph launch");
     SK(cudaStreamSynchronize(s->stream), "sweep");
-    return ESRRF_OK;
+    return sweep_tc_check(s);
 }
 
 esrrf_status esrrf_sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out) {

@@ -1,0 +1,74 @@
+"""GPU tests of the tensor-core (tcgen05, three-term TF32) form of the Fourier interpolation's two
+dense passes against the FP32 SIMT kernels (ESRRF_INTERP_GEMM=simt) and the float64
+interpolation (FourierInterpolation.java's map by numpy FFT).
+
+The INT slice of a block is the frame average of the interpolated frames, so it exposes the
+interpolation directly.  Sizes cover partial tiles in both directions (output rows not a multiple
+of 128, columns not a multiple of 256), mirror padding, the smallest padded size N = 32 (one K
+block) and a 512 x 512 frame.  Tolerance: within 2e-6 of the slice's dynamic range of the float64
+interpolation, and no worse than twice the SIMT kernels' error plus 1e-6 of range.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def run_block(esrrf, frames, M, fwhm=1.5, S=2):
+    eng = esrrf.LiveSRRF_CL()
+    n = frames.shape[0]
+    eng.initialise(frames.shape[-1], frames.shape[-2], M, fwhm, S, n, n)
+    try:
+        eng.resetFramePosition()
+        assert not eng.calculateSRRF(frames)
+        return eng.readSRRFbuffer().copy()
+    finally:
+        eng.release()
+
+
+CASES = [
+    (40, 24, 3, 3),    # N 64: every tile partial
+    (20, 32, 2, 2),    # N 32: one K block
+    (96, 160, 5, 2),   # N 256, 480 x 800 output
+    (512, 512, 4, 2),  # N 512
+]
+
+
+@pytest.mark.parametrize("w,h,M,T", CASES)
+def test_tc_interpolation_matches_fp64(esrrf_mod, monkeypatch, w, h, M, T):
+    from esrrf import synth
+    from oracle import adjoint_oracle as A
+    raw = synth.small_stack(100 + w + h + M, T, h, w).astype(np.float32)
+    ref = A.interpolate_f64(raw, M).mean(axis=0)
+    monkeypatch.delenv("ESRRF_INTERP_GEMM", raising=False)
+    tc = run_block(esrrf_mod, raw, M)
+    monkeypatch.setenv("ESRRF_INTERP_GEMM", "simt")
+    simt = run_block(esrrf_mod, raw, M)
+    e_tc, e_simt = rel_err(tc[3], ref), rel_err(simt[3], ref)
+    # different rounding shows that the tensor-core passes ran
+    assert not np.array_equal(tc[3], simt[3])
+    assert e_tc < 2e-6 and e_tc <= 2 * e_simt + 1e-6, (e_tc, e_simt)
+    # the remaining slices agree with the SIMT path's to the engine's parity bar
+    for k in range(3):
+        assert rel_err(tc[k], simt[k]) < 1e-4, (k, rel_err(tc[k], simt[k]))
+
+
+def test_tc_interpolation_u16_and_chunks(esrrf_mod, oracle_mod, monkeypatch):
+    """uint16 input pushed in uneven GPU loads through the tensor-core passes."""
+    from esrrf import synth
+    monkeypatch.delenv("ESRRF_INTERP_GEMM", raising=False)
+    raw = synth.small_stack(5, 9, 64, 64)
+    ref = oracle_mod.fht_block(oracle_mod.fht_interpolate(raw.astype(np.float32), 4), 4, 1.5, 2)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(64, 64, 4, 1.5, 2, 9, 9, framesPerLaunch=4)
+    try:
+        eng.resetFramePosition()
+        assert not eng.calculateSRRF(raw[:2])
+        assert not eng.calculateSRRF(raw[2:])
+        got = eng.readSRRFbuffer().copy()
+    finally:
+        eng.release()
+    for k in range(4):
+        assert rel_err(got[k], ref[k]) < 1e-4, k
