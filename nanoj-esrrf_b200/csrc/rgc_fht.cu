@@ -184,9 +184,16 @@ template <int S>
 struct FusedLayout {
     static constexpr int EW = kTX + S - 1, EH = kTH + S - 1;  // unit-gradient tile
     static constexpr int IW = EW + 2, IH = EH + 2;            // intensity tile (+1 px margin)
+    static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
     static constexpr size_t off_E = 0;
-    static constexpr size_t off_I = off_E + sizeof(float2) * EW * EH;
-    static constexpr size_t off_wt = (off_I + sizeof(float) * IW * IH + 15) & ~size_t(15);
+    static constexpr size_t off_I = off_E + ((sizeof(float2) * EW * EH + 15) & ~size_t(15));
+    static constexpr size_t tail = ((sizeof(float2) * S * S + sizeof(int) * 2 * S + 15) & ~size_t(15)) +
+                                   sizeof(float) * 5 * kTX * kTH;
+    // A second intensity buffer (the next frame's tile prefetched during this frame's taps) is
+    // used where two CTAs of 256 threads still fit in an SM's 228 KB of shared memory.
+    static constexpr bool kDB = 2 * (off_I + 2 * I_bytes + tail + 1024) <= 228 * 1024;
+    static constexpr int nI = kDB ? 2 : 1;
+    static constexpr size_t off_wt = off_I + nI * I_bytes;
     static constexpr size_t off_jr = off_wt + sizeof(float2) * S * S;
     static constexpr size_t off_st = (off_jr + sizeof(int) * 2 * S + 15) & ~size_t(15);
     static constexpr size_t bytes = off_st + sizeof(float) * 5 * kTX * kTH;
@@ -202,32 +209,47 @@ struct FusedParams {
 };
 
 // One column offset i of the tap box for a thread's 8 outputs: source rows rr = 0 .. S+6 of the
-// unit-gradient tile column; row rr feeds output k with tap row jj = rr - k.  CHECK skips rows
-// outside [lo, hi] (columns whose disc chord is shorter than the box).
+// unit-gradient tile column; row rr feeds output k with tap row jj = rr - k, j = r0 + jj, where
+// r0 = -(S - 2) / 2 (the box of an integer radius R is [-R, R + 1]).  CHECK skips rows outside
+// [lo, hi] (columns whose disc chord is shorter than the box).
+//
+// The inward test g . (i, j) < 0 with j = fr - k is, for gy > 0, k > fr + i gx / gy, and the
+// reverse for gy < 0, so one threshold per source row and one compare per output replace the
+// per-output dot product.  gy = +0 gives an infinite threshold of the right sign (the tile stores
+// +0, never -0), a zero gradient a NaN threshold (never inward).  The two tests can disagree only
+// where g . (i, j) is within rounding of 0, where |g x (i, j)| = d and the contribution
+// w - (w / d) |g x (i, j)| vanishes quadratically.
 template <int S, bool CHECK>
-__device__ __forceinline__ void tap_column(const float2* __restrict__ col, float fi, float fr0,
-                                           int lo, int hi, const float (&w)[S],
-                                           const float (&wd)[S], float (&acc)[kK]) {
+__device__ __forceinline__ void tap_column(const float2* __restrict__ col, float fi, int lo, int hi,
+                                           const float (&w)[S], const float (&wd)[S],
+                                           float (&acc)[kK]) {
     constexpr int EW = FusedLayout<S>::EW;
+    constexpr float fr0 = -(float)((S - 2) / 2);
 #pragma unroll
     for (int rr = 0; rr < S + kK - 1; ++rr) {
         if (CHECK && (rr < lo || rr > hi)) continue;
         const float2 e = col[rr * EW];
         const float fr = fr0 + (float)rr;       // tap row j of output k = 0
-        const float dot0 = fmaf(e.y, fr, e.x * fi);
+        const float thr = fmaf(__fdividef(e.x, e.y), fi, fr);
+        const bool neg = e.y < 0.f;
         const float cr0 = fmaf(-e.x, fr, e.y * fi);
 #pragma unroll
         for (int k = 0; k < kK; ++k) {
             const int jj = rr - k;
             if (jj >= 0 && jj < S) {
-                // j = fr - k: dot = dot0 - k g_y, cross = cr0 + k g_x (independent of k - 1)
-                const float dk = k == 0 ? dot0 : fmaf(-(float)k, e.y, dot0);
+                // cross = cr0 + k g_x (independent of k - 1)
                 const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
                 const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
-                if (dk < 0.f) acc[k] += t;
+                if (((float)k > thr) != neg) acc[k] += t;
             }
         }
     }
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
 }
 
 template <int S>
@@ -236,7 +258,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
     constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
     extern __shared__ __align__(16) unsigned char smem[];
     float2* sE = reinterpret_cast<float2*>(smem + L::off_E);
-    float* sI = reinterpret_cast<float*>(smem + L::off_I);
+    float* sIb = reinterpret_cast<float*>(smem + L::off_I);  // nI buffers of L::I_bytes
     float2* swt = reinterpret_cast<float2*>(smem + L::off_wt);  // [ii][jj] = (w, w/d)
     int* sjr = reinterpret_cast<int*>(smem + L::off_jr);
     float* sst = reinterpret_cast<float*>(smem + L::off_st);    // [5][kTH][kTX]
@@ -274,15 +296,33 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
 
     const int gX0 = x0 + r0 - 1, gY0 = y0 + r0 - 1;  // global origin of the intensity tile
     const float fr0 = (float)r0;
-
-    for (int f = 0; f < a.F; ++f) {
+    constexpr int kIStride = (int)(L::I_bytes / sizeof(float));
+    // interpolated tile of frame f with a one-pixel margin beyond the gradient halo (clamped
+    // reads), copied asynchronously into dst
+    auto prefetch_tile = [&](int f, float* dst) {
         const float* fr = a.interp + (long)f * wh;
-        __syncthreads();
-        // 1. interpolated tile with a one-pixel margin beyond the gradient halo (clamped reads)
         for (int ly = ty; ly < IH; ly += kTYT) {
             const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
             for (int lx = tx; lx < IW; lx += kTX)
-                sI[ly * IW + lx] = __ldg(fr + grow + min(max(gX0 + lx, 0), W - 1));
+                cp_async4(dst + ly * IW + lx, fr + grow + min(max(gX0 + lx, 0), W - 1));
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (L::kDB && a.F > 0) prefetch_tile(0, sIb);
+
+    for (int f = 0; f < a.F; ++f) {
+        float* sI = sIb + (L::kDB ? (f & 1) * kIStride : 0);
+        __syncthreads();
+        // 1. this frame's intensity tile: prefetched during the previous frame, or loaded now
+        if (L::kDB) {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        } else {
+            const float* fr = a.interp + (long)f * wh;
+            for (int ly = ty; ly < IH; ly += kTYT) {
+                const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
+                for (int lx = tx; lx < IW; lx += kTX)
+                    sI[ly * IW + lx] = __ldg(fr + grow + min(max(gX0 + lx, 0), W - 1));
+            }
         }
         __syncthreads();
         // 2. unit gradient at each tap source: Gx read at min(X+1, W-1), Gy at min(Y+1, H-1),
@@ -309,13 +349,15 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
                     const float n2 = Gx * Gx + Gy * Gy;
                     if (n2 > 0.f) {
                         const float inv = rsqrtf(n2);
-                        e = make_float2(Gx * inv, Gy * inv);
+                        e = make_float2(Gx * inv, Gy * inv + 0.f);  // + 0: -0 becomes +0
                     }
                 }
                 sE[ey * EW + ex] = e;
             }
         }
         __syncthreads();
+        // the next frame's tile goes into the other buffer while this frame's taps run
+        if (L::kDB && f + 1 < a.F) prefetch_tile(f + 1, sIb + ((f + 1) & 1) * kIStride);
         // 3. tap loop, one box column at a time with its weights in registers
         float acc[kK];
 #pragma unroll
@@ -336,9 +378,9 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             const int hi = sjr[2 * ii + 1] + kK - 1;
             const float2* col = sE + (ty * kK) * EW + tx + ii;
             if (lo == 0 && hi == S + kK - 2)
-                tap_column<S, false>(col, fi, fr0, lo, hi, w, wd, acc);
+                tap_column<S, false>(col, fi, lo, hi, w, wd, acc);
             else
-                tap_column<S, true>(col, fi, fr0, lo, hi, w, wd, acc);
+                tap_column<S, true>(col, fi, lo, hi, w, wd, acc);
         }
         // 4. normalisation, sensitivity, intensity weighting and cumulants
         if (emit) {
@@ -498,7 +540,9 @@ cudaError_t tap_table_sum(const float* tab, int r0, int S, int W, int H, float* 
     return cudaGetLastError();
 }
 
-bool fht_fused_supported(const FhtGeometry& g) { return g.S >= 4 && g.S <= 32 && g.S % 2 == 0; }
+bool fht_fused_supported(const FhtGeometry& g) {
+    return g.S >= 4 && g.S <= 32 && g.S % 2 == 0 && g.r0 == -(g.S - 2) / 2;
+}
 
 cudaError_t finalize_block(const BlockState& st, int n, int tac_div2, float* out,
                            cudaStream_t stream) {
