@@ -216,7 +216,8 @@ struct FusedParams {
 // The inward test g . (i, j) < 0 with j = fr - k is, for gy > 0, k > fr + i gx / gy, and the
 // reverse for gy < 0, so one threshold per source row and one compare per output replace the
 // per-output dot product.  gy = +0 gives an infinite threshold of the right sign (the tile stores
-// +0, never -0), a zero gradient a NaN threshold (never inward).  The two tests can disagree only
+// +0, never -0), a zero gradient a NaN threshold (never inward); 1 / gy is the approximate
+// reciprocal, whose error only moves the threshold within rounding.  The two tests can disagree only
 // where g . (i, j) is within rounding of 0, where |g x (i, j)| = d and the contribution
 // w - (w / d) |g x (i, j)| vanishes quadratically.
 template <int S, bool CHECK>
@@ -230,7 +231,9 @@ __device__ __forceinline__ void tap_column(const float2* __restrict__ col, float
         if (CHECK && (rr < lo || rr > hi)) continue;
         const float2 e = col[rr * EW];
         const float fr = fr0 + (float)rr;       // tap row j of output k = 0
-        const float thr = fmaf(__fdividef(e.x, e.y), fi, fr);
+        float rgy;  // 1 / gy, +-inf for gy = +-0 (subnormals flush to a zero of their sign)
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
+        const float thr = fmaf(e.x * rgy, fi, fr);
         const bool neg = e.y < 0.f;
         const float cr0 = fmaf(-e.x, fr, e.y * fi);
 #pragma unroll
