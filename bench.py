@@ -207,14 +207,23 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
+TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md"}
+
+
 def read_traffic_summary(kernel):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (its
+    `traffic_bytes_per_launch:` line), if any."""
+    name = TRAFFIC_SUMMARIES.get(kernel)
+    if not name:
+        return None
     try:
-        with open(path) as f:
-            return json.load(f).get(kernel)
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
     except (OSError, ValueError):
         return None
+    return None
 
 
 def run_ours(args, world, rank, local):
