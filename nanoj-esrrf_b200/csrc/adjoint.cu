@@ -675,7 +675,7 @@ void esrrf_adjoint::release() {
     if (stream) cudaStreamSynchronize(stream);
     interp_plan_destroy(plan);
     fht_fused_tables_free(tables);
-    for (void* q : {(void*)scratch.rowT, (void*)scratch.alt, (void*)scratch.vec, (void*)dx, (void*)tabA,
+    for (void* q : {(void*)scratch.rowT, (void*)scratch.xs, (void*)scratch.alt, (void*)scratch.vec, (void*)dx, (void*)tabA,
                     (void*)wdB, (void*)kwtab, (void*)dwsum, (void*)I, (void*)C, (void*)R, (void*)tmp,
                     (void*)Bb, (void*)gB, (void*)gR, (void*)t1, (void*)t2, (void*)Fm, (void*)D, (void*)dF,
                     (void*)bbuf, (void*)gI, (void*)T1, (void*)gX, (void*)proj, (void*)dvec,
@@ -729,7 +729,9 @@ esrrf_status esrrf_adjoint_create(int width, int height, int n_frames, int magni
     const int N = a->plan.N, Fc = a->Fc;
     const long P = (long)a->WM * a->HM, p = (long)width * height;
     auto al = [&](auto** ptr, size_t bytes) { return cudaMalloc((void**)ptr, bytes); };
-    if ((e = al(&a->scratch.rowT, sizeof(float) * Fc * (size_t)N * a->WM)) != cudaSuccess ||
+    if (a->plan.tc && (e = al(&a->scratch.xs, sizeof(float) * Fc * interp_xs_floats(a->plan))) != cudaSuccess)
+        return bail(a->fail_cuda(e, "buffers"));
+    if ((e = al(&a->scratch.rowT, sizeof(float) * Fc * interp_rowT_floats(a->plan))) != cudaSuccess ||
         (e = al(&a->scratch.alt, sizeof(float) * Fc * interp_alt_floats(N))) != cudaSuccess ||
         (e = al(&a->scratch.vec, sizeof(float) * Fc * interp_vec_floats(a->HM, a->WM))) != cudaSuccess ||
         (e = al(&a->dx, sizeof(float) * (size_t)a->WM * N)) != cudaSuccess ||

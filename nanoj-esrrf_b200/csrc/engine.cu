@@ -216,7 +216,8 @@ esrrf_status esrrf_handle::init_fht() {
     if (use_fused) CK(fht_fused_tables(geo, WM, HM, tables, stream));
     const long whM = (long)WM * HM;
     scratch.capacity = F;
-    CK(cudaMalloc(&scratch.rowT, sizeof(float) * (size_t)F * plan.N * WM));
+    CK(cudaMalloc(&scratch.rowT, sizeof(float) * (size_t)F * interp_rowT_floats(plan)));
+    if (plan.tc) CK(cudaMalloc(&scratch.xs, sizeof(float) * (size_t)F * interp_xs_floats(plan)));
     CK(cudaMalloc(&scratch.alt, sizeof(float) * (size_t)F * interp_alt_floats(plan.N)));
     CK(cudaMalloc(&scratch.vec, sizeof(float) * (size_t)F * interp_vec_floats(HM, WM)));
     CK(cudaMalloc(&d_interp, sizeof(float) * (size_t)F * whM));
@@ -232,6 +233,7 @@ void esrrf_handle::release() {
     interp_plan_destroy(plan);
     fht_fused_tables_free(tables);
     cudaFree(scratch.rowT);
+    cudaFree(scratch.xs);
     cudaFree(scratch.alt);
     cudaFree(scratch.vec);
     cudaFree(d_interp);

@@ -40,16 +40,19 @@ struct InterpPlan {
     float* uy = nullptr;      // [HM]
     int* srcx = nullptr;      // [N] source column of padded column
     int* srcy = nullptr;      // [N] source row of padded row
-    // tensor-core passes (tc): Dx row-major and a device flag set when a bounded wait gave up
+    // tensor-core passes (tc): Dx and Dy as split operand panels, and a device flag set when a
+    // bounded wait gave up
     bool tc = false;
-    float* dx = nullptr;      // [WM][N]   (scaled like dxT)
+    float* dxp = nullptr;     // pass 1 B panels [WM/256][N/16] (hi, lo)
+    float* dyp = nullptr;     // pass 2 A panels [HM/128][N/16] (hi, lo)
     int* tc_err = nullptr;
 };
 
 // Per-frame interpolation scratch for a chunk of F frames.
 struct InterpScratch {
     int capacity = 0;
-    float* rowT = nullptr;    // [F][N][WM]  first-pass output
+    float* rowT = nullptr;    // [F][interp_rowT_floats]  first-pass output
+    float* xs = nullptr;      // [F][interp_xs_floats]  padded frame as operand panels (tc)
     float* alt = nullptr;     // [F][interp_alt_floats(N)]  alternating row/column sums, row sums
     float* vec = nullptr;     // [F][interp_vec_floats(HM, WM)]  P, T, Q, R and the frame mean
 };
@@ -65,9 +68,13 @@ cudaError_t interp_adjoint_run(const InterpPlan& p, const float* dx, const float
                                float* T1, float* gX, float* proj, float* dvec, float* graw,
                                cudaStream_t stream);
 
-// Tensor-core (tcgen05, three-term TF32) form of the two dense passes; needs N % 32 == 0.
-// Writes the first-pass rows transposed into scratch.rowT ([F][WM][N]).
+// Tensor-core (tcgen05, three-term TF32) form of the two dense passes; needs N % 128 == 0.
+// Writes the first-pass rows into scratch.rowT as pass 2's operand panels.
 bool tc_interp_supported(const InterpPlan& plan);
+cudaError_t tc_plan_tables(InterpPlan& plan, const std::vector<float>& dxT, const std::vector<float>& dy);
+// Scratch floats per frame: first-pass rows (either form) and the frame's operand panels.
+size_t interp_rowT_floats(const InterpPlan& plan);
+size_t interp_xs_floats(const InterpPlan& plan);
 cudaError_t tc_interp_passes(const InterpPlan& plan, InterpScratch& scratch, const void* raw,
                              bool is_u16, int F, float* out, cudaStream_t stream);
 // Reads (and clears) the plan's tensor-core failure flag; synchronises `stream`.

@@ -527,14 +527,7 @@ cudaError_t interp_plan_create(InterpPlan& p, int w, int h, int M, int scale_mod
     if ((e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev)) != cudaSuccess)
         return e;
     p.tc = major == 10 && tc_interp_supported(p) && !(sel && std::strcmp(sel, "simt") == 0);
-    if (p.tc) {
-        std::vector<float> dx((size_t)p.WM * N);
-        for (int n = 0; n < p.WM; ++n)
-            for (int m = 0; m < N; ++m) dx[(size_t)n * N + m] = dxT[(size_t)m * p.WM + n];
-        if ((e = upload(&p.dx, dx)) != cudaSuccess) return e;
-        if ((e = cudaMalloc((void**)&p.tc_err, sizeof(int))) != cudaSuccess) return e;
-        if ((e = cudaMemset(p.tc_err, 0, sizeof(int))) != cudaSuccess) return e;
-    }
+    if (p.tc) return tc_plan_tables(p, dxT, dy);
     return cudaSuccess;
 }
 
@@ -548,7 +541,8 @@ void interp_plan_destroy(InterpPlan& p) {
     cudaFree(p.uy);
     cudaFree(p.srcx);
     cudaFree(p.srcy);
-    cudaFree(p.dx);
+    cudaFree(p.dxp);
+    cudaFree(p.dyp);
     cudaFree(p.tc_err);
     p = InterpPlan();
 }

@@ -215,6 +215,7 @@ void esrrf_sweep::release() {
     }
     mp.clear();
     cudaFree(scratch.rowT);
+    cudaFree(scratch.xs);
     cudaFree(scratch.alt);
     cudaFree(scratch.vec);
     cudaFree(d_interp);
@@ -318,9 +319,15 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
     const int T = sp->n_frames;
     s->scratch.capacity = std::min(16, T);
     const int Fi = s->scratch.capacity;
-    size_t maxHM = 0;
-    for (auto& m : s->mp) maxHM = std::max(maxHM, (size_t)m.plan.HM);
-    if ((e = cudaMalloc(&s->scratch.rowT, sizeof(float) * Fi * (size_t)maxN * maxWM)) != cudaSuccess ||
+    size_t maxHM = 0, maxRowT = 0, maxXs = 0;
+    for (auto& m : s->mp) {
+        maxHM = std::max(maxHM, (size_t)m.plan.HM);
+        maxRowT = std::max(maxRowT, interp_rowT_floats(m.plan));
+        maxXs = std::max(maxXs, interp_xs_floats(m.plan));
+    }
+    if (maxXs && (e = cudaMalloc(&s->scratch.xs, sizeof(float) * Fi * maxXs)) != cudaSuccess)
+        return bail(s->fail_cuda(e, "sweep buffers"));
+    if ((e = cudaMalloc(&s->scratch.rowT, sizeof(float) * Fi * maxRowT)) != cudaSuccess ||
         (e = cudaMalloc(&s->scratch.alt, sizeof(float) * Fi * interp_alt_floats(maxN))) != cudaSuccess ||
         (e = cudaMalloc(&s->scratch.vec, sizeof(float) * Fi * interp_vec_floats((int)maxHM, maxWM))) != cudaSuccess ||
         (e = cudaMalloc(&s->d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||

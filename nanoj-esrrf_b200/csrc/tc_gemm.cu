@@ -3,18 +3,28 @@
 //     A B ~= Ah Bh + Ah Bl + Al Bh,   Ah = tf32_rn(A), Al = tf32_rn(A - Ah)  (same for B),
 // accumulated in FP32 in tensor memory (TMEM).
 //
-//   pass 1:  rowsT[f] (WM x N)  = (X_f - c_f) Dx^T, stored transposed (K-major for pass 2)
+//   pass 1:  rowsT[f] (WM x N)  = (X_f - c_f) Dx^T, written split into pass 2's operand panels
 //   pass 2:  I'[f]    (HM x WM) = Dy rowsT[f]^T + rank-one terms + c_f s N^2
 //
-// The large product Ah Bh and the two small correction products accumulate in separate TMEM
-// accumulators (512 columns in all), summed in the epilogue, so the corrections add no rounding to
-// the main sum.  CTA tile 128 (M) x 256 (N), K blocks of 32, two shared-memory stages of
-// (A hi, A lo, B hi, B lo) in the canonical K-major no-swizzle core-matrix layout (8 rows x 16 bytes per core
-// matrix).  All 256 threads stage a K block (global loads, TF32 split, shared stores), then one
-// thread issues the 12 MMAs of the block and commits them to the stage's mbarrier; a stage is
-// refilled only after that barrier completes.  Every mbarrier wait is bounded: on timeout the
-// kernel records the failure in `err`, stops issuing work, releases its TMEM and returns.
+// Operands live in HBM already split and laid out as "panels": for a tile of R rows (128 for A,
+// 256 for B) and a K block of 16, the hi part then the lo part, each in the canonical K-major
+// no-swizzle core-matrix layout (core matrix = 8 rows x 16 bytes; the 16-byte chunk k4 of row r
+// at ((k4 (R/8) + r/8) 128 + (r%8) 16) bytes).  Dx and Dy panels are built once per plan, the
+// padded frame's panels by x_split_kernel, and pass 1's epilogue writes pass 2's B panels.  So a
+// pipeline stage is filled by two plain bulk copies (cp.async.bulk, no tensor map, no multicast).
+//
+// CTA: 10 warps.  Warp 8 (one lane) streams the panels into a ring of 4 shared-memory stages of
+// 48 KB; warp 9 (one lane) issues tcgen05.mma 128x256x8 (6 per K block) and commits; warps 0-7
+// drain the accumulators.  The tensor core's FP32 accumulation behaves like round-toward-zero, so
+// a run of K = 64 accumulates in one of two TMEM accumulators (columns 0-255 and 256-511) and is
+// then drained by warps 0-7 into FP32 registers with round-to-nearest adds while the next run
+// fills the other accumulator.  Every mbarrier wait is bounded: a role that gives up records the
+// failure in `err`, waits (bounded) for the copies or MMAs it has in flight and leaves; the CTA
+// then skips its stores and releases its TMEM.
 #include <stdint.h>
+
+#include <cstring>
+#include <vector>
 
 #include "esrrf_internal.h"
 
@@ -22,19 +32,27 @@ namespace esrrf {
 
 namespace {
 
-constexpr int TC_M = 128, TC_N = 256, TC_BK = 32;
-constexpr uint32_t TC_A_BYTES = TC_M * TC_BK * 4;  // 16 KB
-constexpr uint32_t TC_B_BYTES = TC_N * TC_BK * 4;  // 32 KB
-constexpr uint32_t TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
-constexpr uint32_t TC_SMEM_BYTES = 2 * TC_STAGE_BYTES + 128;
-constexpr uint32_t TC_TMEM_COLS = 512;  // main accumulator in columns 0-255, corrections 256-511
-constexpr int TC_DRAIN = 4;             // K blocks per main-accumulator run (K = 128)
+constexpr int TC_M = 128, TC_N = 256, TC_BK = 16;
+constexpr uint32_t TC_A_PANEL = TC_M * TC_BK * 4;   // 8 KB per part
+constexpr uint32_t TC_B_PANEL = TC_N * TC_BK * 4;   // 16 KB per part
+constexpr uint32_t TC_A_BYTES = 2 * TC_A_PANEL;     // hi + lo
+constexpr uint32_t TC_B_BYTES = 2 * TC_B_PANEL;
+constexpr uint32_t TC_STAGE = TC_A_BYTES + TC_B_BYTES;  // 48 KB
+constexpr int TC_STAGES = 4;
+constexpr uint32_t TC_SMEM_BYTES = TC_STAGES * TC_STAGE;
+constexpr int TC_RUN = 4;                 // K blocks per accumulator run (K = 64)
+constexpr uint32_t TC_TMEM_COLS = 512;    // two 128 x 256 FP32 accumulators
+constexpr int TC_THREADS = 320;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s of SM clock before a wait gives up
 
 // Instruction descriptor: D f32 (bits 4-5 = 1), A tf32 (7-9 = 2), B tf32 (10-12 = 2), both
 // K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
                               ((uint32_t)(TC_M >> 4) << 24);
+
+__host__ __device__ constexpr uint32_t panel_off(int R, int r, int k4) {
+    return ((uint32_t)(k4 * (R / 8) + (r >> 3)) << 7) + ((uint32_t)(r & 7) << 4);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -47,30 +65,10 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
 
-// Byte offset of the 16-byte chunk (row r, k-chunk k4) in a K-major tile of R rows x 32 k.
-template <int R>
-__device__ __forceinline__ uint32_t kmaj(int r, int k4) {
-    return ((uint32_t)(k4 * (R / 8) + (r >> 3)) << 7) + ((uint32_t)(r & 7) << 4);
-}
-
-// hi = x rounded to TF32; lo = the remainder (exact in FP32) rounded to TF32 as well, so the
-// tensor core does not truncate it
-__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
-    uint32_t h, l;
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t h;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-    hi = __uint_as_float(h);
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
-    lo = __uint_as_float(l);
-}
-
-__device__ __forceinline__ void st_split(unsigned char* hi, unsigned char* lo, uint32_t off, float4 v) {
-    float4 h, l;
-    split_tf32(v.x, h.x, l.x);
-    split_tf32(v.y, h.y, l.y);
-    split_tf32(v.z, h.z, l.z);
-    split_tf32(v.w, h.w, l.w);
-    *reinterpret_cast<float4*>(hi + off) = h;
-    *reinterpret_cast<float4*>(lo + off) = l;
+    return __uint_as_float(h);
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
@@ -94,6 +92,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(addr), "r"(bytes)
+                 : "memory");
+}
+
+// Plain (non-tensor, non-multicast) bulk copy global -> this CTA's shared memory, completing
+// `bytes` of the mbarrier's transaction count.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(mbar)
+        : "memory");
+}
+
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -105,48 +125,36 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-        "%30, %31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// Adds a warp's 32 x 128 quarter of the main accumulator into the register accumulator.
-__device__ __forceinline__ void drain_main(uint32_t taddr, float (&racc)[128]) {
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        float v[32];
-        tmem_ld32(taddr + 32 * c, v);
-#pragma unroll
-        for (int j = 0; j < 32; ++j) racc[32 * c + j] += v[j];
-    }
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 struct TcArgs {
-    int Mr, Nc, K;             // C[f] (Mr x Nc) = A (Mr x K) . B^T, B stored K-major (Nc x K)
-    // pass 1 A: padded frame gathered from raw, minus the frame mean
-    const void* raw;
-    int is_u16, w, h;
-    const int* srcx;
-    const int* srcy;
-    // pass 2 A: shared row-major matrix
-    const float* A;
-    // B: K-major (rows of length K); per frame (stride Nc*K) when b_per_frame
-    const float* B;
-    int b_per_frame;
+    int Mr, Nc, nkb;                 // C (Mr x Nc) over nkb K blocks of 16
+    const unsigned char* Ap;         // A panels [mt][kb], TC_A_BYTES each
+    long a_frame;                    // bytes between frames' A panels (0: shared)
+    const unsigned char* Bp;         // B panels [nt][kb], TC_B_BYTES each
+    long b_frame;
+    // pass 1: C written as pass 2's B panels [f][nt][kb2] (K of pass 2 = the rows here)
+    unsigned char* Cp;
+    long c_frame;
+    // pass 2: C row-major [f][Mr][Nc] plus the rank-one terms
     float* C;
-    // rank-one epilogue (pass 2) and frame means
     const float* vec;
     const float* cx;
     const float* ux;
@@ -154,215 +162,254 @@ struct TcArgs {
     const float* uy;
     int HM, WM;
     float cscale;
+    int v8;                          // pass 2: rows 32-byte aligned (256-bit stores)
     int* err;
 };
 
-// Staging map of the 16-byte chunk q of a K block: eight consecutive lanes take the eight rows of
-// one core matrix, four lanes along K, so a warp stores four whole core matrices (512 contiguous
-// bytes, no bank conflict) and loads eight rows x 64 contiguous bytes from global memory.
-__device__ __forceinline__ void chunk_of(int q, int& r, int& k4) {
-    r = ((q >> 6) << 3) | (q & 7);
-    k4 = (((q >> 5) & 1) << 2) | ((q >> 3) & 3);
-}
-
-// PASS 1: A gathered from the raw frame (minus its mean), C stored transposed.
-// PASS 2: A shared, rank-one epilogue, C row-major (written through a shared-memory transpose).
 template <int PASS>
-__global__ void __launch_bounds__(256, 1) tc_gemm_kernel(TcArgs g) {
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs g) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_empty[TC_STAGES], bar_accf[2], bar_acce[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ __align__(16) float4 colterm[TC_N];  // pass 2: (cx, ux, q, r) of the tile's columns
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int f = blockIdx.z;
-    const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * TC_N;
-    const int nkb = g.K / TC_BK;
+    const int f = blockIdx.z, mt = blockIdx.y, nt = blockIdx.x;
+    const int m0 = mt * TC_M, n0 = nt * TC_N;
+    const int nkb = g.nkb, nruns = (nkb + TC_RUN - 1) / TC_RUN;
 
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(smem_u32(&bar_full[s]), 1);
+            mbar_init(smem_u32(&bar_empty[s]), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(smem_u32(&bar_accf[a]), 1);
+            mbar_init(smem_u32(&bar_acce[a]), 8);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == 9) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_slot)),
                      "r"(TC_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    if (PASS == 2 && tid < TC_N) {
+        const float* vec = g.vec + (long)f * (2L * g.HM + 2L * g.WM + 1);
+        const int n = n0 + tid;
+        colterm[tid] = n < g.Nc ? make_float4(g.cx[n], g.ux[n], vec[2 * g.HM + n], vec[2 * g.HM + g.WM + n])
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
+    bool ok = true;
+    float racc[128];  // warps 0-7: rows 32 (w % 4) + lane, columns (w / 4) * 128 .. +127
 
-    const void* rawf = nullptr;
-    float cmean = 0.f;
-    if (PASS == 1) {
-        rawf = g.is_u16 ? (const void*)((const unsigned short*)g.raw + (long)f * g.w * g.h)
-                        : (const void*)((const float*)g.raw + (long)f * g.w * g.h);
-        cmean = g.vec[(long)f * (2L * g.HM + 2L * g.WM + 1) + 2 * g.HM + 2 * g.WM];
-    }
-    const float* Bf = g.b_per_frame ? g.B + (long)f * g.Nc * g.K : g.B;
-    int issued = 0;  // K blocks whose MMAs have been issued and committed
-    // This warp's TMEM quarter: lanes 32 (warp % 4) .. +31 (tile rows), columns (warp / 4) * 128.
-    const uint32_t tq = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 128);
-    // The tensor core's FP32 accumulation of the main product is drained into registers every
-    // TC_DRAIN K blocks (round-to-nearest adds), which bounds the rounding bias a long TMEM
-    // accumulation builds up.
-    float racc[128];
-#pragma unroll
-    for (int i = 0; i < 128; ++i) racc[i] = 0.f;
-
-    for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb & 1;
-        unsigned char* st = smem + s * TC_STAGE_BYTES;
-        unsigned char* Ahi = st;
-        unsigned char* Alo = st + TC_A_BYTES;
-        unsigned char* Bhi = st + 2 * TC_A_BYTES;
-        unsigned char* Blo = st + 2 * TC_A_BYTES + TC_B_BYTES;
-        // the stage is free once the MMAs of block kb - 2 (its previous use) have completed
-        bool freed = true;
-        if (kb >= 2) freed = mbar_wait(smem_u32(&mbar[s]), (uint32_t)(((kb >> 1) - 1) & 1));
-        const int k0 = kb * TC_BK;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {  // A: 128 rows x 8 chunks
-            int r, k4;
-            chunk_of(tid + i * 256, r, k4);
-            const int m = m0 + r, k = k0 + 4 * k4;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (m < g.Mr) {
-                if (PASS == 1) {
-                    const long row = (long)__ldg(g.srcy + m) * g.w;
-                    const int4 sx = __ldg(reinterpret_cast<const int4*>(g.srcx + k));
-                    if (g.is_u16) {
-                        const unsigned short* src = (const unsigned short*)rawf + row;
-                        v = make_float4((float)__ldg(src + sx.x) - cmean, (float)__ldg(src + sx.y) - cmean,
-                                        (float)__ldg(src + sx.z) - cmean, (float)__ldg(src + sx.w) - cmean);
-                    } else {
-                        const float* src = (const float*)rawf + row;
-                        v = make_float4(__ldg(src + sx.x) - cmean, __ldg(src + sx.y) - cmean,
-                                        __ldg(src + sx.z) - cmean, __ldg(src + sx.w) - cmean);
-                    }
-                } else {
-                    v = __ldg(reinterpret_cast<const float4*>(g.A + (long)m * g.K + k));
+    if (warp == 8) {
+        // ---------------- producer: panels -> shared-memory ring ----------------
+        if (lane == 0) {
+            const unsigned char* Ab = g.Ap + (long)f * g.a_frame + (long)mt * nkb * TC_A_BYTES;
+            const unsigned char* Bb = g.Bp + (long)f * g.b_frame + (long)nt * nkb * TC_B_BYTES;
+            int issued = 0;
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb & (TC_STAGES - 1), u = kb / TC_STAGES;
+                if (u > 0 && !mbar_wait(smem_u32(&bar_empty[s]), (uint32_t)((u - 1) & 1))) {
+                    ok = false;
+                    break;
                 }
+                const uint32_t full = smem_u32(&bar_full[s]);
+                const uint32_t dst = smem_u32(smem + s * TC_STAGE);
+                mbar_expect_tx(full, TC_STAGE);
+                bulk_g2s(dst, Ab + (long)kb * TC_A_BYTES, TC_A_BYTES, full);
+                bulk_g2s(dst + TC_A_BYTES, Bb + (long)kb * TC_B_BYTES, TC_B_BYTES, full);
+                issued = kb + 1;
             }
-            st_split(Ahi, Alo, kmaj<TC_M>(r, k4), v);
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {  // B: 256 rows x 8 chunks
-            int r, k4;
-            chunk_of(tid + i * 256, r, k4);
-            const int n = n0 + r, k = k0 + 4 * k4;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (n < g.Nc) v = __ldg(reinterpret_cast<const float4*>(Bf + (long)n * g.K + k));
-            st_split(Bhi, Blo, kmaj<TC_N>(r, k4), v);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        // one barrier both publishes the stage and makes the give-up decision block-uniform
-        if (!__syncthreads_and(freed ? 1 : 0)) break;
-        if (kb > 0 && kb % TC_DRAIN == 0) {
-            // block kb-1 closed a run: drain it before the MMAs of block kb restart the accumulator
-            const bool ok = __all_sync(0xffffffffu,
-                                       mbar_wait(smem_u32(&mbar[(kb - 1) & 1]), (uint32_t)(((kb - 1) >> 1) & 1)));
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            if (ok) drain_main(tq, racc);
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            if (!__syncthreads_and(ok ? 1 : 0)) break;
-        }
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ahi = smem_u32(Ahi), alo = smem_u32(Alo);
-            const uint32_t bhi = smem_u32(Bhi), blo = smem_u32(Blo);
-#pragma unroll
-            for (int ks = 0; ks < TC_BK / 8; ++ks) {
-                // one MMA consumes k chunks 2ks and 2ks+1 of every row: LBO steps between the two
-                // chunks (R/8 core matrices apart), SBO between 8-row groups (one core matrix)
-                const uint32_t ao = (uint32_t)(2 * ks * (TC_M / 8)) << 7;
-                const uint32_t bo = (uint32_t)(2 * ks * (TC_N / 8)) << 7;
-                const uint64_t dah = umma_desc(ahi + ao, (TC_M / 8) << 7, 128);
-                const uint64_t dal = umma_desc(alo + ao, (TC_M / 8) << 7, 128);
-                const uint64_t dbh = umma_desc(bhi + bo, (TC_N / 8) << 7, 128);
-                const uint64_t dbl = umma_desc(blo + bo, (TC_N / 8) << 7, 128);
-                tc_mma(tmem, dah, dbh, (kb % TC_DRAIN != 0 || ks > 0) ? 1u : 0u);
-                tc_mma(tmem + TC_N, dah, dbl, (kb > 0 || ks > 0) ? 1u : 0u);
-                tc_mma(tmem + TC_N, dal, dbh, 1u);
+            if (!ok) {
+                // let the copies in flight land before the CTA can leave
+                for (int kb = issued - TC_STAGES > 0 ? issued - TC_STAGES : 0; kb < issued; ++kb)
+                    mbar_wait(smem_u32(&bar_full[kb & (TC_STAGES - 1)]), (uint32_t)((kb / TC_STAGES) & 1));
             }
-            asm volatile(
-                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    smem_u32(&mbar[s]))
-                : "memory");
         }
-        issued = kb + 1;
-    }
-    // the accumulator is final once the commit of the last issued block has arrived (a commit
-    // tracks every earlier MMA of the issuing thread); after a failed wait this still waits,
-    // bounded, for the MMAs in flight before the tensor memory is released
-    bool done = issued == nkb;
-    if (issued > 0 &&
-        !mbar_wait(smem_u32(&mbar[(issued - 1) & 1]), (uint32_t)(((issued - 1) >> 1) & 1)))
-        done = false;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!__syncthreads_and(done ? 1 : 0)) {
-        if (tid == 0 && g.err) atomicExch(g.err, 1);
+    } else if (warp == 9) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb & (TC_STAGES - 1), u = kb / TC_STAGES;
+                const int r = kb / TC_RUN, a = r & 1;
+                const bool first = kb % TC_RUN == 0;
+                // the accumulator of run r was last used by run r - 2: wait for its drain
+                if (first && r >= 2 && !mbar_wait(smem_u32(&bar_acce[a]), (uint32_t)(((r >> 1) - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                if (!mbar_wait(smem_u32(&bar_full[s]), (uint32_t)(u & 1))) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = smem_u32(smem + s * TC_STAGE);
+                const uint32_t ahi = base, alo = base + TC_A_PANEL;
+                const uint32_t bhi = base + TC_A_BYTES, blo = base + TC_A_BYTES + TC_B_PANEL;
+                const uint32_t d = tmem + (uint32_t)(a * TC_N);
+#pragma unroll
+                for (int ks = 0; ks < TC_BK / 8; ++ks) {
+                    // one MMA consumes k chunks 2ks and 2ks+1 of every row: LBO steps between the
+                    // two chunks (R/8 core matrices apart), SBO between 8-row groups
+                    const uint32_t ao = (uint32_t)(2 * ks * (TC_M / 8)) << 7;
+                    const uint32_t bo = (uint32_t)(2 * ks * (TC_N / 8)) << 7;
+                    const uint64_t dah = umma_desc(ahi + ao, (TC_M / 8) << 7, 128);
+                    const uint64_t dal = umma_desc(alo + ao, (TC_M / 8) << 7, 128);
+                    const uint64_t dbh = umma_desc(bhi + bo, (TC_N / 8) << 7, 128);
+                    const uint64_t dbl = umma_desc(blo + bo, (TC_N / 8) << 7, 128);
+                    tc_mma(d, dah, dbh, (first && ks == 0) ? 0u : 1u);
+                    tc_mma(d, dah, dbl, 1u);
+                    tc_mma(d, dal, dbh, 1u);
+                }
+                tc_commit(smem_u32(&bar_empty[s]));  // the stage can be refilled
+                if (kb % TC_RUN == TC_RUN - 1 || kb == nkb - 1) tc_commit(smem_u32(&bar_accf[a]));
+                issued = kb + 1;
+            }
+            if (!ok && issued > 0) {
+                // the MMAs in flight must finish before the TMEM is released
+                const int kb = issued - 1;
+                mbar_wait(smem_u32(&bar_empty[kb & (TC_STAGES - 1)]), (uint32_t)((kb / TC_STAGES) & 1));
+            }
+        }
     } else {
-        // epilogue: the last run and the corrections join the register accumulator
-        drain_main(tq, racc);
-        drain_main(tq + TC_N, racc);
-        const int rbase = m0 + 32 * (warp & 3);
-        const int row = rbase + lane;
-        const int cbase = n0 + (warp >> 2) * 128;
-        float* Cf = g.C + (long)f * g.Mr * g.Nc;
+        // ---------------- drain warps ----------------
+#pragma unroll
+        for (int i = 0; i < 128; ++i) racc[i] = 0.f;
+        const uint32_t tq = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 128);
+        for (int r = 0; r < nruns; ++r) {
+            const int a = r & 1;
+            const bool got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&bar_accf[a]), (uint32_t)((r >> 1) & 1)));
+            if (!got) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // 16 columns at a time: with 10 warps a scheduler holds 3, which caps a thread at 168
+            // registers, 128 of them the accumulator
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                float v[16];
+                tmem_ld16(tq + (uint32_t)(a * TC_N + 16 * c), v);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) racc[16 * c + j] += v[j];
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar_acce[a]));
+        }
+    }
+
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!all_ok) {
+        if (tid == 0 && g.err) atomicExch(g.err, 1);
+    } else if (warp < 8) {
+        const int row = m0 + 32 * (warp & 3) + lane;
+        const int cb = (warp >> 2) * 128;  // column offset within the tile
         if (PASS == 1) {
+            // C^T (columns n = output columns of pass 2, rows = K of pass 2) into pass 2's B
+            // panels, split: panel (nt, kb2 = row / 16), panel row n - n0, k = row % 16
             if (row < g.Mr) {
+                unsigned char* P = g.Cp + (long)f * g.c_frame +
+                                   ((long)nt * (g.Mr / TC_BK) + row / TC_BK) * TC_B_BYTES;
+                const int k = row % TC_BK;
 #pragma unroll
                 for (int j = 0; j < 128; ++j) {
-                    const int n = cbase + j;
-                    if (n < g.Nc) Cf[(long)n * g.Mr + row] = racc[j];  // lanes write consecutive rows
+                    const int rr = cb + j;
+                    if (n0 + rr >= g.Nc) break;
+                    const uint32_t off = panel_off(TC_N, rr, k >> 2) + ((k & 3) << 2);
+                    const float hi = tf32_rna(racc[j]);
+                    *reinterpret_cast<float*>(P + off) = hi;
+                    *reinterpret_cast<float*>(P + TC_B_PANEL + off) = tf32_rna(racc[j] - hi);
                 }
             }
         } else {
-            // rank-one terms: row factors held by the lane of that row, column factors by the
-            // lane of that column after the transpose
-            const float* vec = g.vec + (long)f * (2L * g.HM + 2L * g.WM + 1);
-            float pm = 0.f, tm = 0.f, cym = 0.f, uym = 0.f;
             if (row < g.Mr) {
-                pm = vec[row];
-                tm = vec[g.HM + row];
-                cym = g.cy[row];
-                uym = g.uy[row];
-            }
-            const float cback = vec[2 * g.HM + 2 * g.WM] * g.cscale;
-            float* buf = reinterpret_cast<float*>(smem) + warp * (32 * 33);  // stages are idle now
+                const float* vec = g.vec + (long)f * (2L * g.HM + 2L * g.WM + 1);
+                const float pm = vec[row], tm = vec[g.HM + row];
+                const float cym = g.cy[row], uym = g.uy[row];
+                const float cback = vec[2 * g.HM + 2 * g.WM] * g.cscale;
+                float* out = g.C + (long)f * g.Mr * g.Nc + (long)row * g.Nc + n0 + cb;
+                const bool full = g.v8 && n0 + cb + 128 <= g.Nc;
+                // eight columns at a time: rank-one terms, then one 256-bit store (or scalars)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+                for (int q = 0; q < 16; ++q) {
+                    float o[8];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) buf[lane * 33 + j] = racc[32 * c + j];
-                __syncwarp();
-                const int n = cbase + 32 * c + lane;
-                float cxn = 0.f, uxn = 0.f, qn = 0.f, rn = 0.f;
-                if (n < g.Nc) {
-                    cxn = g.cx[n];
-                    uxn = g.ux[n];
-                    qn = vec[2 * g.HM + n];
-                    rn = vec[2 * g.HM + g.WM + n];
+                    for (int i = 0; i < 8; ++i) {
+                        const float4 ct = colterm[cb + 8 * q + i];  // broadcast
+                        o[i] = racc[8 * q + i] + pm * ct.x + cym * ct.z - uym * ct.w - tm * ct.y + cback;
+                    }
+                    if (full) {
+                        asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(out + 8 * q),
+                                     "f"(o[0]), "f"(o[1]), "f"(o[2]), "f"(o[3]), "f"(o[4]), "f"(o[5]), "f"(o[6]),
+                                     "f"(o[7])
+                                     : "memory");
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 8; ++i)
+                            if (n0 + cb + 8 * q + i < g.Nc) out[8 * q + i] = o[i];
+                    }
                 }
-#pragma unroll 4
-                for (int r = 0; r < 32; ++r) {
-                    const float pr = __shfl_sync(0xffffffffu, pm, r);
-                    const float tr = __shfl_sync(0xffffffffu, tm, r);
-                    const float cr = __shfl_sync(0xffffffffu, cym, r);
-                    const float ur = __shfl_sync(0xffffffffu, uym, r);
-                    if (rbase + r < g.Mr && n < g.Nc)
-                        Cf[(long)(rbase + r) * g.Nc + n] =
-                            buf[r * 33 + lane] + pr * cxn + cr * qn - ur * rn - tr * uxn + cback;
-                }
-                __syncwarp();
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 9) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+    }
+}
+
+// Padded frame minus its mean, split into pass 1's A panels [f][mt][kb].  One thread per 16-byte
+// chunk; consecutive threads take consecutive rows of one chunk column (coalesced panel writes).
+__global__ void __launch_bounds__(256) x_split_kernel(const void* __restrict__ raw, int is_u16, int w, int h,
+                                                      int N, const int* __restrict__ srcx,
+                                                      const int* __restrict__ srcy,
+                                                      const float* __restrict__ vec, long vstride,
+                                                      long cmean_off, unsigned char* __restrict__ xp) {
+    const int f = blockIdx.y;
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;  // chunk index in the frame
+    const long per_panel = TC_M * (TC_BK / 4);
+    const long nchunks = (long)N * N / 4;
+    if (q >= nchunks) return;
+    const long p = q / per_panel;
+    const int within = (int)(q - p * per_panel);
+    const int k4 = within / TC_M, r = within % TC_M;
+    const int nkb = N / TC_BK;
+    const int mt = (int)(p / nkb), kb = (int)(p % nkb);
+    const int m = mt * TC_M + r, x = kb * TC_BK + 4 * k4;
+    const float c = vec[(long)f * vstride + cmean_off];
+    const long row = (long)srcy[m] * w + (long)f * w * h;
+    const int4 sx = *reinterpret_cast<const int4*>(srcx + x);
+    float v[4];
+    if (is_u16) {
+        const unsigned short* s = (const unsigned short*)raw + row;
+        v[0] = (float)s[sx.x]; v[1] = (float)s[sx.y]; v[2] = (float)s[sx.z]; v[3] = (float)s[sx.w];
+    } else {
+        const float* s = (const float*)raw + row;
+        v[0] = s[sx.x]; v[1] = s[sx.y]; v[2] = s[sx.z]; v[3] = s[sx.w];
+    }
+    float4 hi, lo;
+    float* hp = &hi.x;
+    float* lp = &lo.x;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float d = v[i] - c;
+        hp[i] = tf32_rna(d);
+        lp[i] = tf32_rna(d - hp[i]);
+    }
+    unsigned char* P = xp + ((long)f * (N / TC_M) * nkb + p) * TC_A_BYTES;
+    const uint32_t off = panel_off(TC_M, r, k4);
+    *reinterpret_cast<float4*>(P + off) = hi;
+    *reinterpret_cast<float4*>(P + TC_A_PANEL + off) = lo;
 }
 
 template <int PASS>
@@ -379,9 +426,70 @@ cudaError_t set_tc_smem() {
     return e;
 }
 
+// Host form of cvt.rna.tf32.f32 for finite values: round to nearest, ties away from zero, at the
+// 13th mantissa bit.
+float host_tf32_rna(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    b = (b + 0x1000u) & 0xFFFFE000u;
+    float y;
+    std::memcpy(&y, &b, 4);
+    return y;
+}
+
+// Panels of a row-major matrix Z (rows x K): [tile][kb] with R rows per tile, rows >= rows zero.
+std::vector<float> make_panels(const std::vector<float>& Z, int rows, int K, int R) {
+    const int tiles = (rows + R - 1) / R, nkb = K / TC_BK;
+    const size_t part = (size_t)R * TC_BK;  // floats per part
+    std::vector<float> P((size_t)tiles * nkb * 2 * part, 0.f);
+    for (int t = 0; t < tiles; ++t)
+        for (int kb = 0; kb < nkb; ++kb) {
+            float* base = P.data() + ((size_t)t * nkb + kb) * 2 * part;
+            for (int r = 0; r < R; ++r) {
+                const int row = t * R + r;
+                if (row >= rows) continue;
+                for (int k = 0; k < TC_BK; ++k) {
+                    const float v = Z[(size_t)row * K + kb * TC_BK + k];
+                    const float hi = host_tf32_rna(v);
+                    const size_t o = panel_off(R, r, k >> 2) / 4 + (k & 3);
+                    base[o] = hi;
+                    base[part + o] = host_tf32_rna(v - hi);
+                }
+            }
+        }
+    return P;
+}
+
 }  // namespace
 
-bool tc_interp_supported(const InterpPlan& p) { return p.N >= 32 && p.N % 32 == 0; }
+bool tc_interp_supported(const InterpPlan& p) { return p.N >= 128 && p.N % TC_M == 0; }
+
+size_t interp_rowT_floats(const InterpPlan& p) {
+    const size_t simt = (size_t)p.N * p.WM;
+    if (!p.tc) return simt;
+    const size_t tc = (size_t)((p.WM + TC_N - 1) / TC_N) * TC_N * p.N * 2;
+    return tc > simt ? tc : simt;
+}
+
+size_t interp_xs_floats(const InterpPlan& p) { return p.tc ? (size_t)p.N * p.N * 2 : 0; }
+
+cudaError_t tc_plan_tables(InterpPlan& p, const std::vector<float>& dxT, const std::vector<float>& dy) {
+    const int N = p.N;
+    std::vector<float> dx((size_t)p.WM * N);
+    for (int n = 0; n < p.WM; ++n)
+        for (int m = 0; m < N; ++m) dx[(size_t)n * N + m] = dxT[(size_t)m * p.WM + n];
+    const std::vector<float> dxp = make_panels(dx, p.WM, N, TC_N);
+    const std::vector<float> dyp = make_panels(dy, p.HM, N, TC_M);
+    cudaError_t e;
+    if ((e = cudaMalloc((void**)&p.dxp, sizeof(float) * dxp.size())) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(p.dxp, dxp.data(), sizeof(float) * dxp.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    if ((e = cudaMalloc((void**)&p.dyp, sizeof(float) * dyp.size())) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(p.dyp, dyp.data(), sizeof(float) * dyp.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    if ((e = cudaMalloc((void**)&p.tc_err, sizeof(int))) != cudaSuccess) return e;
+    return cudaMemset(p.tc_err, 0, sizeof(int));
+}
 
 cudaError_t interp_tc_check(const InterpPlan& p, cudaStream_t stream, bool* failed) {
     *failed = false;
@@ -401,14 +509,16 @@ cudaError_t tc_interp_passes(const InterpPlan& p, InterpScratch& sc, const void*
     cudaError_t e;
     if ((e = set_tc_smem<1>()) != cudaSuccess) return e;
     if ((e = set_tc_smem<2>()) != cudaSuccess) return e;
-    const int N = p.N;
+    const int N = p.N, nkb = N / TC_BK;
+    const int ntiles = (p.WM + TC_N - 1) / TC_N;
+    const long vstride = 2L * p.HM + 2L * p.WM + 1;
+    {
+        const long chunks = (long)N * N / 4;
+        x_split_kernel<<<dim3((unsigned)((chunks + 255) / 256), F), 256, 0, stream>>>(
+            raw, is_u16 ? 1 : 0, p.w, p.h, N, p.srcx, p.srcy, sc.vec, vstride, 2L * p.HM + 2L * p.WM,
+            reinterpret_cast<unsigned char*>(sc.xs));
+    }
     TcArgs g{};
-    g.raw = raw;
-    g.is_u16 = is_u16 ? 1 : 0;
-    g.w = p.w;
-    g.h = p.h;
-    g.srcx = p.srcx;
-    g.srcy = p.srcy;
     g.vec = sc.vec;
     g.cx = p.cx;
     g.ux = p.ux;
@@ -418,25 +528,29 @@ cudaError_t tc_interp_passes(const InterpPlan& p, InterpScratch& sc, const void*
     g.WM = p.WM;
     g.cscale = (float)(p.s * (double)N * (double)N);
     g.err = p.tc_err;
-    // pass 1: rowsT[f] (WM x N) = (X_f - c) . Dx^T, with B = Dx (WM x N, K-major)
+    const long rowT_frame = (long)ntiles * nkb * TC_B_BYTES;
+    // pass 1: rows of (X - c) times Dx^T, written as pass 2's B panels
     g.Mr = N;
     g.Nc = p.WM;
-    g.K = N;
-    g.B = p.dx;
-    g.b_per_frame = 0;
-    g.C = sc.rowT;
-    tc_gemm_kernel<1><<<dim3((g.Nc + TC_N - 1) / TC_N, (g.Mr + TC_M - 1) / TC_M, F), 256, TC_SMEM_BYTES,
-                        stream>>>(g);
-    // pass 2: I'[f] (HM x WM) = Dy . rowsT[f]^T + epilogue, with B = rowsT[f] (WM x N, K-major)
+    g.nkb = nkb;
+    g.Ap = reinterpret_cast<const unsigned char*>(sc.xs);
+    g.a_frame = (long)(N / TC_M) * nkb * TC_A_BYTES;
+    g.Bp = reinterpret_cast<const unsigned char*>(p.dxp);
+    g.b_frame = 0;
+    g.Cp = reinterpret_cast<unsigned char*>(sc.rowT);
+    g.c_frame = rowT_frame;
+    tc_gemm_kernel<1><<<dim3(ntiles, N / TC_M, F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g);
+    // pass 2: Dy times the first-pass rows, plus the rank-one terms
     g.Mr = p.HM;
     g.Nc = p.WM;
-    g.K = N;
-    g.A = p.dy;
-    g.B = sc.rowT;
-    g.b_per_frame = 1;
+    g.nkb = nkb;
+    g.Ap = reinterpret_cast<const unsigned char*>(p.dyp);
+    g.a_frame = 0;
+    g.Bp = reinterpret_cast<const unsigned char*>(sc.rowT);
+    g.b_frame = rowT_frame;
     g.C = out;
-    tc_gemm_kernel<2><<<dim3((g.Nc + TC_N - 1) / TC_N, (g.Mr + TC_M - 1) / TC_M, F), 256, TC_SMEM_BYTES,
-                        stream>>>(g);
+    g.v8 = (p.WM % 8 == 0 && reinterpret_cast<uintptr_t>(out) % 32 == 0) ? 1 : 0;
+    tc_gemm_kernel<2><<<dim3(ntiles, (p.HM + TC_M - 1) / TC_M, F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g);
     return cudaGetLastError();
 }
 
