@@ -249,6 +249,52 @@ __device__ __forceinline__ void tap_column(const float2* __restrict__ col, float
     }
 }
 
+// A column whose disc chord is the compile-time tap-row range [LO, HI]: only the chord's taps
+// are evaluated (rows LO .. HI + 7, and per row only the outputs whose tap row is in the chord).
+template <int S, int LO, int HI>
+__device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float fi, const float (&w)[S],
+                                          const float (&wd)[S], float (&acc)[kK]) {
+    constexpr int EW = FusedLayout<S>::EW;
+    constexpr float fr0 = -(float)((S - 2) / 2);
+#pragma unroll
+    for (int rr = LO; rr <= HI + kK - 1; ++rr) {
+        const float2 e = col[rr * EW];
+        const float fr = fr0 + (float)rr;
+        float rgy;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
+        const float thr = fmaf(e.x * rgy, fi, fr);
+        const bool neg = e.y < 0.f;
+        const float cr0 = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;
+            if (jj >= LO && jj <= HI) {
+                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
+                if (((float)k > thr) != neg) acc[k] += t;
+            }
+        }
+    }
+}
+
+// The disc is symmetric in j, so a column's chord inside the box [-R, R+1] is either the whole
+// box or the rows -J .. J, i.e. tap rows [LO, S - 2 - LO]: one instantiation per LO.  Any other
+// range takes the generic row-checked loop.
+template <int S, int LO>
+__device__ __forceinline__ void tap_dispatch(const float2* __restrict__ col, float fi, int lo, int hi,
+                                             const float (&w)[S], const float (&wd)[S],
+                                             float (&acc)[kK]) {
+    if constexpr (LO <= (S - 2) / 2) {
+        if (lo == LO && hi == S - 2 - LO) {
+            tap_chord<S, LO, S - 2 - LO>(col, fi, w, wd, acc);
+            return;
+        }
+        tap_dispatch<S, LO + 1>(col, fi, lo, hi, w, wd, acc);
+    } else {
+        tap_column<S, true>(col, fi, lo, hi + kK - 1, w, wd, acc);
+    }
+}
+
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
                  "l"(src)
@@ -366,6 +412,8 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
 #pragma unroll
         for (int k = 0; k < kK; ++k) acc[k] = 0.f;
         for (int ii = 0; ii < S; ++ii) {
+            const int lo = sjr[2 * ii], hi = sjr[2 * ii + 1];
+            if (lo > hi) continue;  // no tap of the disc in this column
             const float fi = fr0 + (float)ii;
             float w[S], wd[S];
             const float4* wc = reinterpret_cast<const float4*>(swt + ii * S);
@@ -377,13 +425,11 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
                 w[2 * q + 1] = v.z;
                 wd[2 * q + 1] = v.w;
             }
-            const int lo = sjr[2 * ii];
-            const int hi = sjr[2 * ii + 1] + kK - 1;
             const float2* col = sE + (ty * kK) * EW + tx + ii;
-            if (lo == 0 && hi == S + kK - 2)
-                tap_column<S, false>(col, fi, lo, hi, w, wd, acc);
+            if (lo == 0 && hi == S - 1)
+                tap_chord<S, 0, S - 1>(col, fi, w, wd, acc);
             else
-                tap_column<S, true>(col, fi, lo, hi, w, wd, acc);
+                tap_dispatch<S, 0>(col, fi, lo, hi, w, wd, acc);
         }
         // 4. normalisation, sensitivity, intensity weighting and cumulants
         if (emit) {

@@ -16,7 +16,7 @@
 // CTA: 10 warps.  Warp 8 (one lane) streams the panels into a ring of 4 shared-memory stages of
 // 48 KB; warp 9 (one lane) issues tcgen05.mma 128x256x8 (6 per K block) and commits; warps 0-7
 // drain the accumulators.  The tensor core's FP32 accumulation behaves like round-toward-zero, so
-// a run of K = 64 accumulates in one of two TMEM accumulators (columns 0-255 and 256-511) and is
+// a run of K = 32 accumulates in one of two TMEM accumulators (columns 0-255 and 256-511) and is
 // then drained by warps 0-7 into FP32 registers with round-to-nearest adds while the next run
 // fills the other accumulator.  Every mbarrier wait is bounded: a role that gives up records the
 // failure in `err`, waits (bounded) for the copies or MMAs it has in flight and leaves; the CTA
@@ -40,7 +40,7 @@ constexpr uint32_t TC_B_BYTES = 2 * TC_B_PANEL;
 constexpr uint32_t TC_STAGE = TC_A_BYTES + TC_B_BYTES;  // 48 KB
 constexpr int TC_STAGES = 4;
 constexpr uint32_t TC_SMEM_BYTES = TC_STAGES * TC_STAGE;
-constexpr int TC_RUN = 4;                 // K blocks per accumulator run (K = 64)
+constexpr int TC_RUN = 2;                 // K blocks per accumulator run (K = 32)
 constexpr uint32_t TC_TMEM_COLS = 512;    // two 128 x 256 FP32 accumulators
 constexpr int TC_THREADS = 320;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;  // ~2 s of SM clock before a wait gives up
