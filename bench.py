@@ -483,11 +483,40 @@ def run_3d(args, world, rank, local):
              "ROI #": roi, "Intensity scaling": np.ones(P), "Background level (ADC)": np.full(P, 0.0)}
     M, fwhm, S = 3, 1.5, 1
     eng = esrrf.LiveSRRF_CL()
-    eng.initialise(3 * w, 3 * h, M, fwhm, S, n, n, chosenDevice=local, doMPmapCorrection=True,
-                   calibTable3DSRRF=calib, framesPerLaunch=args.frames_per_launch or 8)
-    H = eng.handle
     d_cam = torch.from_numpy(cam.view(np.int16)).to(f"cuda:{local}")
     d_out = torch.empty((4 * P * M, h * M, w * M), dtype=torch.float32, device=f"cuda:{local}")
+    L = esrrf.lib()
+
+    def per_launch_form(fpl):
+        """Device time (ms) of one step with `fpl` timepoints per launch (1: the plain form, one
+        timepoint at a time)."""
+        e2 = esrrf.LiveSRRF_CL()
+        e2.initialise(3 * w, 3 * h, M, fwhm, S, n, n, chosenDevice=local, doMPmapCorrection=True,
+                      calibTable3DSRRF=calib, framesPerLaunch=fpl, kernel=args.kernel)
+        try:
+            ts = []
+            for i in range(3):
+                torch.cuda.synchronize()
+                a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a0.record()
+                esrrf._lib.check(e2.handle, L.esrrf_reset_frame_position(e2.handle))
+                esrrf._lib.check(e2.handle, L.esrrf_calculate_srrf_u16_device(
+                    e2.handle, ctypes.c_void_p(d_cam.data_ptr()), n))
+                esrrf._lib.check(e2.handle, L.esrrf_read_srrf_device(
+                    e2.handle, ctypes.c_void_p(d_out.data_ptr())))
+                a1.record()
+                torch.cuda.synchronize()
+                if i > 0:
+                    ts.append(a0.elapsed_time(a1))
+            return min(ts)
+        finally:
+            e2.release()
+
+    plain_ms = per_launch_form(1) if world == 1 else None
+    eng = esrrf.LiveSRRF_CL()
+    eng.initialise(3 * w, 3 * h, M, fwhm, S, n, n, chosenDevice=local, doMPmapCorrection=True,
+                   calibTable3DSRRF=calib, framesPerLaunch=args.frames_per_launch or 8, kernel=args.kernel)
+    H = eng.handle
     launches = [0]
 
     def step():
@@ -496,7 +525,6 @@ def run_3d(args, world, rank, local):
         launches[0] += eng.lastTiming()[2] + 3
         esrrf._lib.check(H, L.esrrf_read_srrf_device(H, ctypes.c_void_p(d_out.data_ptr())))
 
-    L = esrrf.lib()
     for _ in range(args.warmup):
         step()
     launches[0] = 0
@@ -525,7 +553,12 @@ def run_3d(args, world, rank, local):
         "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"mfm3d: {P} planes of {w}x{h} x {n} timepoints, M3, radius 1.5, S1, "
-                               "AVG+VAR (+TAC2, INT), MP correction, one block", "kernel": "plain per-voxel"},
+                               "AVG+VAR (+TAC2, INT), MP correction, one block",
+                   "kernel": "tabulated taps" if args.kernel == "fused" else "plain per-voxel",
+                   "timepoints_per_launch": args.frames_per_launch or 8},
+        "forms": {"batched_timepoints_per_launch_ms": t_step * 1e3,
+                  "plain_1_timepoint_per_launch_ms": plain_ms,
+                  "plain_1_timepoint_per_launch_mpx_frames_s": mpxf / (plain_ms / 1e3) if plain_ms else None},
         "e2e": {"value": mpxf / e2e, "unit": "Mpx*frames/s", "h2d_bytes_per_step": int(cam.nbytes),
                 "d2h_bytes_per_step": int(h_out.numel() * 4)},
         "gpu_launches": launches[0] // max(1, args.steps), "clocks": clk.summary()}))

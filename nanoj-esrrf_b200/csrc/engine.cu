@@ -197,6 +197,8 @@ esrrf_status esrrf_handle::init_bic3d() {
         CK(cudaMalloc(&d_planes, sizeof(float) * F * P * plane));
         CK(cudaMalloc(&d_gz, sizeof(float) * F * P * plane));
         CK(cudaMalloc(&d_gzi, sizeof(float) * F * P * 4 * plane));
+        CK(cudaMalloc(&d_u3, sizeof(float4) * F * P * 4 * plane));
+        CK(rgc3d_tables_build(bgeo, M, ws, hs, t3d));
     }
     CK(cudaMalloc(&d_mpmap, sizeof(float) * 3 * M * M * M));
     return alloc_common(sizeof(float) * (size_t)W * H, (long)WM * HM * PM);
@@ -250,6 +252,8 @@ void esrrf_handle::release() {
     cudaFree(st.acc);
     cudaFree(st.prev);
     cudaFree(d_out);
+    rgc3d_tables_free(t3d);
+    cudaFree(d_u3);
     for (float* b : {d_fraw, d_planes, d_gz, d_gxi, d_gyi, d_gzi, d_mpmap, mfm.coeff, mfm.cos_t,
                      mfm.sin_t, mfm.shx, mfm.shy})
         cudaFree(b);
@@ -386,6 +390,27 @@ esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int
         a.st = st;
         CK(bic_rgc(a, stream));
     } else {
+        // tabulated taps unless a frame of this launch has drift or the plain kernel was asked for
+        bool no_drift = p.kernel == 0;
+        for (int i = 0; i < 2 * F_now; ++i) no_drift = no_drift && sh[i] == 0.f;
+        if (no_drift) {
+            CK(unit_grad3d(d_gxi, d_gyi, d_gzi, ws, hs, P, F_now, d_u3, stream));
+            Rgc3dTabArgs ta{};
+            ta.U = d_u3;
+            ta.apx = d_fraw;
+            ta.w = ws;
+            ta.h = hs;
+            ta.P = P;
+            ta.M = p.magnification;
+            ta.F = F_now;
+            ta.t0 = frame_in_block;
+            ta.sens = bgeo.sensitivity;
+            ta.int_weighting = p.int_weighting;
+            ta.tab = t3d;
+            ta.st = st;
+            CK(rgc_3d_tab(ta, stream));
+            launches += 1;
+        }
         Rgc3dArgs a{};
         a.apx = d_fraw;
         a.gxi = d_gxi;
@@ -404,7 +429,7 @@ esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int
         a.shift = d_shift;
         a.int_weighting = p.int_weighting;
         a.st = st;
-        CK(rgc_3d(a, stream));
+        if (!no_drift) CK(rgc_3d(a, stream));
     }
     launches += 1;
     if (timing) CK(cudaEventRecord(e2, stream));

@@ -43,6 +43,8 @@ struct esrrf_handle {
     float* d_gyi = nullptr;
     float* d_gzi = nullptr;
     float* d_mpmap = nullptr;   // [3][M^2 or M^3]
+    esrrf::Rgc3dTables t3d;     // 3-D tap tables per sub-pixel phase (launches without drift)
+    float4* d_u3 = nullptr;     // [F][P][2hs][2ws] unit gradient field
 
     // input staging (double-buffered)
     size_t raw_frame_bytes = 0;

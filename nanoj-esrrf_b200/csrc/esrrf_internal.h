@@ -196,6 +196,34 @@ struct Mfm3dTables {
     float* shx = nullptr;     // [P]
     float* shy = nullptr;
 };
+// Tabulated 3-D RGC for launches without drift.  With zero shift the tap geometry of an output
+// voxel depends only on its sub-pixel phase (xM % M, yM % M, zM % M), so each phase's taps inside
+// the disc (reference loop order j, i, k) are listed once: source offset into the unit-gradient
+// field, (dx, dy, dz), d^2, w, w/d, and the phase's interior sum of weights.
+struct Rgc3dTables {
+    float4* taba = nullptr;   // [taps] (offset as int bits, dx, dy, dz)
+    float4* tabb = nullptr;   // [taps] (d^2, w, w/d, packed (sx, sy, sz) as int bits)
+    int* start = nullptr;     // [M^3 + 1] first tap of each phase
+    int* meta = nullptr;      // [M^3][6] sx min/max, sy min/max, sz min/max
+    float* wsum = nullptr;    // [M^3] sum of w over the phase's taps
+    int max_taps = 0;
+};
+cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, Rgc3dTables& t);
+void rgc3d_tables_free(Rgc3dTables& t);
+struct Rgc3dTabArgs {
+    const float4* U;     // [F][P][2h][2w] unit gradient, columns split by parity ([even | odd])
+    const float* apx;    // [F][P][h][w] aligned planes
+    int w, h, P, M, F, t0;
+    float sens;
+    int int_weighting;
+    Rgc3dTables tab;
+    BlockState st;
+};
+// unit gradient field from the 2x-resampled components (Gx read at x+1, Gy at y+1, Gz in place)
+cudaError_t unit_grad3d(const float* gxi, const float* gyi, const float* gzi, int w, int h, int P,
+                        int F, float4* U, cudaStream_t stream);
+cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream);
+
 // camera frames [F][H][W] -> planes [F][P][hs][ws] ((p - background) / coeff), aligned planes,
 // 3-D 2-point gradient and its 2x lateral resampling.
 cudaError_t mfm_prepare(const void* raw, int is_u16, int W, int H, int P, int ws, int hs, int F,

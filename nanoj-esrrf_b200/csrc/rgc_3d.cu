@@ -9,6 +9,10 @@
 // taps on whole planes, cubic-in-z intensity of four bicubic samples (:325-498).
 #include <math.h>
 
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
 #include "device_common.cuh"
 #include "esrrf_internal.h"
 
@@ -173,7 +177,259 @@ __global__ void __launch_bounds__(256) rgc_3d_kernel(Rgc3dArgs a) {
     a.st.prev[idx] = prev;
 }
 
+// Unit gradient of each 2x-grid source point: the reference reads Gx at (x+1, y), Gy at (x, y+1)
+// and Gz at (x, y) of the 2x-resampled components (live3DSRRF.cl RGC; for an in-bounds tap the
+// clamps never bind), so the tap test and |d x G| / |G| = |d x g| only need g = G / |G|.
+// Columns are stored split by parity so that a warp's 32 consecutive voxels read 32 consecutive
+// entries.
+__global__ void unit_grad3d_kernel(const float* __restrict__ gxi, const float* __restrict__ gyi,
+                                   const float* __restrict__ gzi, int w, int h, float4* __restrict__ U) {
+    const int ax = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ay = blockIdx.y;
+    const long fz = blockIdx.z;  // frame * P + plane
+    const int w2 = 2 * w, h2 = 2 * h;
+    if (ax >= w2) return;
+    float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ax < w2 - 1 && ay < h2 - 1) {
+        const long pl = fz * (long)w2 * h2;
+        const float Gx = __ldg(gxi + pl + (long)ay * w2 + ax + 1);
+        const float Gy = __ldg(gyi + pl + (long)(ay + 1) * w2 + ax);
+        const float Gz = __ldg(gzi + pl + (long)ay * w2 + ax);
+        const float n2 = Gx * Gx + Gy * Gy + Gz * Gz;
+        if (n2 > 0.f) {
+            const float inv = rsqrtf(n2);
+            u = make_float4(Gx * inv, Gy * inv, Gz * inv, 0.f);
+        }
+    }
+    U[(fz * h2 + ay) * w2 + (ax & 1) * w + (ax >> 1)] = u;
+}
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Dk w = w - (w / d) |d x g| for an inward tap, |d x g| from the cross product itself
+// (d^2 - (d.g)^2 would cancel for taps along the gradient, which carry the largest terms).
+__device__ __forceinline__ float tap_term(const float4& A, const float4& B, const float4& u) {
+    const float cx = fmaf(A.z, u.z, -A.w * u.y);  // dy gz - dz gy
+    const float cy = fmaf(A.w, u.x, -A.y * u.z);  // dz gx - dx gz
+    const float cz = fmaf(A.y, u.y, -A.z * u.x);  // dx gy - dy gx
+    return fmaf(-B.z, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz * cz))), B.y);
+}
+
+// One thread per output voxel; a CTA is 32 x 8 input cells of one (x, y) phase and one output
+// plane, so the whole CTA walks the same tap list (broadcast from shared memory) and a warp's
+// gradient reads are contiguous.  Warps whose taps all fall inside the volume skip the bounds
+// tests and use the phase's tabulated sum of weights; the others test each tap
+// (live3DSRRF.cl: 0 < vx < w, 0 < vy < h, 0 < vz < P) and sum their weights.
+__global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
+    extern __shared__ float4 stab[];  // [2 n]: A entries, then B entries
+    const int M = a.M, M2 = M * M;
+    const int zM = blockIdx.z / M2, pxy = blockIdx.z % M2;
+    const int px = pxy % M, py = pxy / M;
+    const int qz = zM / M, pz = zM % M;
+    const int phase = (pz * M + py) * M + px;
+    const int t0 = a.tab.start[phase], n = a.tab.start[phase + 1] - t0;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < n; i += 256) {
+        stab[i] = a.tab.taba[t0 + i];
+        stab[n + i] = a.tab.tabb[t0 + i];
+    }
+    __syncthreads();
+    const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
+    const bool valid = qx_raw < a.w && qy_raw < a.h;
+    const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
+    const int* meta = a.tab.meta + 6 * phase;
+    const int qa = blockIdx.x * 32, qb = min(blockIdx.x * 32 + 31, a.w - 1);
+    const bool interior = 2 * qa + meta[0] >= 0 && 2 * qb + meta[1] <= 2 * a.w - 2 &&
+                          2 * qy + meta[2] >= 0 && 2 * qy + meta[3] <= 2 * a.h - 2 &&
+                          qz + meta[4] >= 1 && qz + meta[5] <= a.P - 1;
+    const int xM = qx * M + px, yM = qy * M + py;
+    const int WM = a.w * M, HM = a.h * M;
+    const long whM = (long)WM * HM, total = whM * a.P * M;
+    const long idx = (long)zM * whM + (long)yM * WM + xM;
+    const long pl = (long)a.w * a.h;
+    const float wsum_in = a.tab.wsum[phase];
+    // intensity: cubic in z of four bicubic samples, the fourth plane repeating z0 + 1
+    // (live3DSRRF.cl:434-456), no shift
+    const float zc = (float)(((double)zM + 0.5) / M);
+    int z0;
+    const float zcof = zc - 0.5f;
+    if (zcof < 0)
+        z0 = 0;
+    else if (zcof >= (float)(a.P - 1))
+        z0 = a.P - 2;
+    else
+        z0 = (int)floorf(zcof);
+    const float pxf = (float)xM / (float)M - 0.5f;
+    const float pyf = (float)yM / (float)M - 0.5f;
+    const float z01 = zc - (float)(z0 + 0.5f);
+
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    float prev = valid ? a.st.prev[idx] : 0.f;
+    for (int f = 0; f < a.F; ++f) {
+        const float4* U = a.U + ((long)(f * a.P + qz) * (2 * a.h) + 2 * qy) * (2 * a.w) + qx;
+        float cglh = 0.f, wsum = 0.f;
+        if (interior) {
+            wsum = wsum_in;
+            for (int t = 0; t < n; ++t) {
+                const float4 A = stab[t], B = stab[n + t];
+                const float4 u = __ldg(U + __float_as_int(A.x));
+                const float dot = fmaf(u.x, A.y, fmaf(u.y, A.z, u.z * A.w));
+                if (dot < 0.f) cglh += tap_term(A, B, u);
+            }
+        } else {
+            for (int t = 0; t < n; ++t) {
+                const float4 B = stab[n + t];
+                const int pk = __float_as_int(B.w);
+                const int sx = (int)((unsigned)pk << 22) >> 22;
+                const int sy = (int)((unsigned)pk << 12) >> 22;
+                const int sz = pk >> 20;
+                const int ax = 2 * qx + sx, ay = 2 * qy + sy, az = qz + sz;
+                if (ax < 0 || ax > 2 * a.w - 2 || ay < 0 || ay > 2 * a.h - 2 || az < 1 || az > a.P - 1)
+                    continue;
+                wsum += B.y;
+                const float4 A = stab[t];
+                const float4 u = __ldg(U + __float_as_int(A.x));
+                const float dot = fmaf(u.x, A.y, fmaf(u.y, A.z, u.z * A.w));
+                if (dot < 0.f) cglh += tap_term(A, B, u);
+            }
+        }
+        const float cg = cglh_power(cglh / wsum, a.sens);
+        const float* ap = a.apx + (long)f * a.P * pl;
+        const float v_1 = sample2d(ap + (long)max(z0 - 1, 0) * pl, a.w, a.h, pxf, pyf);
+        const float v0 = sample2d(ap + (long)z0 * pl, a.w, a.h, pxf, pyf);
+        const float v1 = sample2d(ap + (long)(z0 + 1) * pl, a.w, a.h, pxf, pyf);
+        const float v2 = sample2d(ap + (long)min(z0 + 1, a.P - 1) * pl, a.w, a.h, pxf, pyf);
+        const float ca = -0.5f * v_1 + 1.5f * v0 - 1.5f * v1 + 0.5f * v2;
+        const float cb = v_1 - 2.5f * v0 + 2.0f * v1 - 0.5f * v2;
+        const float cc = -0.5f * v_1 + 0.5f * v1;
+        const float v = ca * z01 * z01 * z01 + cb * z01 * z01 + cc * z01 + v0;
+        const float x = a.int_weighting ? v * cg : cg;
+        s0 += x;
+        s1 += (double)x * x;
+        if (a.t0 + f > 0) s2 += (double)x * prev;
+        s3 += v;
+        prev = x;
+    }
+    if (!valid) return;
+    a.st.acc[idx] += s0;
+    a.st.acc[total + idx] += s1;
+    a.st.acc[2 * total + idx] += s2;
+    a.st.acc[3 * total + idx] += s3;
+    a.st.prev[idx] = prev;
+}
+
 }  // namespace
+
+cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, Rgc3dTables& t) {
+    // Tap geometry of rgc_3d_kernel with zero shift, for the voxel of each phase in the first
+    // input cell (Java float arithmetic as the reference: xc = (float)((xM + 0.5) / M)).
+    const int r0 = -(int)(2.0f * g.radius), r1 = (int)(2.0f * g.radius + 1);
+    const int k0 = -(int)g.radius, k1 = (int)g.radius + 1;
+    const int w2 = 2 * w, h2 = 2 * h, M3 = M * M * M;
+    std::vector<float4> A, B;
+    std::vector<int> start(M3 + 1, 0), meta(6 * M3, 0);
+    std::vector<float> wsum(M3, 0.f);
+    int maxn = 0;
+    for (int pz = 0; pz < M; ++pz)
+        for (int py = 0; py < M; ++py)
+            for (int px = 0; px < M; ++px) {
+                const int phase = (pz * M + py) * M + px;
+                start[phase] = (int)A.size();
+                const float xc = (float)(((double)px + 0.5) / M);
+                const float yc = (float)(((double)py + 0.5) / M);
+                const float zc = (float)(((double)pz + 0.5) / M);
+                const int kx = (int)(2.0f * xc), ky = (int)(2.0f * yc);
+                int mn[3] = {1 << 20, 1 << 20, 1 << 20}, mx[3] = {-(1 << 20), -(1 << 20), -(1 << 20)};
+                float ws = 0.f;
+                for (int j = r0; j <= r1; ++j) {
+                    const float vy = ((float)ky + (float)j) / 2.0f;
+                    for (int i = r0; i <= r1; ++i) {
+                        const float vx = ((float)kx + (float)i) / 2.0f;
+                        for (int k = k0; k <= k1; ++k) {
+                            const float vz = (float)((int)zc) + (float)k;
+                            const float dx = vx - xc, dy = vy - yc, dz = vz - zc;
+                            const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+                            if (!(d != 0.f && d <= g.tSO)) continue;
+                            const int sx = kx + i - 1, sy = ky + j - 1, sz = k;
+                            // column ax = 2 qx + sx sits at parity (sx & 1), index qx + floor(sx / 2)
+                            // (arithmetic shift; sx may be negative)
+                            const int off = sz * w2 * h2 + sy * w2 + (sx & 1) * w + (sx >> 1);
+                            float wt = d * expf(-(d * d) / g.tSS);
+                            wt = wt * wt * wt * wt;
+                            ws += wt;
+                            const int pk = (int)(((unsigned)sx & 0x3FFu) | (((unsigned)sy & 0x3FFu) << 10) |
+                                                 ((unsigned)sz << 20));
+                            float offf, pkf;
+                            std::memcpy(&offf, &off, 4);
+                            std::memcpy(&pkf, &pk, 4);
+                            A.push_back(make_float4(offf, dx, dy, dz));
+                            B.push_back(make_float4(d * d, wt, wt / d, pkf));
+                            const int sv[3] = {sx, sy, sz};
+                            for (int c = 0; c < 3; ++c) {
+                                mn[c] = std::min(mn[c], sv[c]);
+                                mx[c] = std::max(mx[c], sv[c]);
+                            }
+                        }
+                    }
+                }
+                wsum[phase] = ws;
+                for (int c = 0; c < 3; ++c) {
+                    meta[6 * phase + 2 * c] = mn[c];
+                    meta[6 * phase + 2 * c + 1] = mx[c];
+                }
+                maxn = std::max(maxn, (int)A.size() - start[phase]);
+            }
+    start[M3] = (int)A.size();
+    t.max_taps = maxn;
+    auto up = [](auto** d, const auto& v) -> cudaError_t {
+        cudaError_t e = cudaMalloc((void**)d, sizeof(v[0]) * std::max<size_t>(v.size(), 1));
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpy(*d, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice);
+    };
+    cudaError_t e;
+    if ((e = up(&t.taba, A)) != cudaSuccess || (e = up(&t.tabb, B)) != cudaSuccess ||
+        (e = up(&t.start, start)) != cudaSuccess || (e = up(&t.meta, meta)) != cudaSuccess ||
+        (e = up(&t.wsum, wsum)) != cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
+
+void rgc3d_tables_free(Rgc3dTables& t) {
+    cudaFree(t.taba);
+    cudaFree(t.tabb);
+    cudaFree(t.start);
+    cudaFree(t.meta);
+    cudaFree(t.wsum);
+    t = Rgc3dTables();
+}
+
+cudaError_t unit_grad3d(const float* gxi, const float* gyi, const float* gzi, int w, int h, int P,
+                        int F, float4* U, cudaStream_t stream) {
+    unit_grad3d_kernel<<<dim3((2 * w + 127) / 128, 2 * h, F * P), 128, 0, stream>>>(gxi, gyi, gzi, w, h, U);
+    return cudaGetLastError();
+}
+
+cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream) {
+    const size_t smem = sizeof(float4) * 2 * (size_t)a.tab.max_taps;
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (smem > 48 * 1024 && dev < 64 && !(configured & (1ull << dev))) {
+        if ((e = cudaFuncSetAttribute(rgc3d_tab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024)) != cudaSuccess)
+            return e;
+        configured |= 1ull << dev;
+    }
+    const dim3 grid((a.w + 31) / 32, (a.h + 7) / 8, a.M * a.M * a.P * a.M);
+    rgc3d_tab_kernel<<<grid, dim3(32, 8), smem, stream>>>(a);
+    return cudaGetLastError();
+}
 
 cudaError_t mfm_prepare(const void* raw, int is_u16, int W, int H, int P, int ws, int hs, int F,
                         const Mfm3dTables& t, float background, float* planes, float* apx,
