@@ -197,8 +197,9 @@ esrrf_status esrrf_handle::init_bic3d() {
         CK(cudaMalloc(&d_planes, sizeof(float) * F * P * plane));
         CK(cudaMalloc(&d_gz, sizeof(float) * F * P * plane));
         CK(cudaMalloc(&d_gzi, sizeof(float) * F * P * 4 * plane));
-        CK(cudaMalloc(&d_u3, sizeof(float4) * F * P * 4 * plane));
-        CK(rgc3d_tables_build(bgeo, M, ws, hs, t3d));
+        CK(rgc3d_tables_build(bgeo, M, ws, hs, P, t3d, stream));
+        CK(cudaMalloc(&d_u3, sizeof(float4) * rgc3d_field_float4s(t3d, F)));
+        CK(cudaMemsetAsync(d_u3, 0, sizeof(float4) * rgc3d_field_float4s(t3d, F), stream));  // zero halo
     }
     CK(cudaMalloc(&d_mpmap, sizeof(float) * 3 * M * M * M));
     return alloc_common(sizeof(float) * (size_t)W * H, (long)WM * HM * PM);
@@ -394,7 +395,7 @@ esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int
         bool no_drift = p.kernel == 0;
         for (int i = 0; i < 2 * F_now; ++i) no_drift = no_drift && sh[i] == 0.f;
         if (no_drift) {
-            CK(unit_grad3d(d_gxi, d_gyi, d_gzi, ws, hs, P, F_now, d_u3, stream));
+            CK(unit_grad3d(d_gxi, d_gyi, d_gzi, ws, hs, P, F_now, t3d, d_u3, stream));
             Rgc3dTabArgs ta{};
             ta.U = d_u3;
             ta.apx = d_fraw;

@@ -201,17 +201,23 @@ struct Mfm3dTables {
 // the disc (reference loop order j, i, k) are listed once: source offset into the unit-gradient
 // field, (dx, dy, dz), d^2, w, w/d, and the phase's interior sum of weights.
 struct Rgc3dTables {
-    float4* taba = nullptr;   // [taps] (offset as int bits, dx, dy, dz)
+    float4* taba = nullptr;   // [taps] (offset into the padded field as int bits, dx, dy, dz)
     float4* tabb = nullptr;   // [taps] (d^2, w, w/d, packed (sx, sy, sz) as int bits)
     int* start = nullptr;     // [M^3 + 1] first tap of each phase
-    int* meta = nullptr;      // [M^3][6] sx min/max, sy min/max, sz min/max
-    float* wsum = nullptr;    // [M^3] sum of w over the phase's taps
+    float* wsum = nullptr;    // [P M][h M][w M] sum of w over each voxel's in-range taps
     int max_taps = 0;
+    // zero halo of the unit-gradient field: 2x-grid columns (even) and rows, planes below/above
+    int padx = 0, pady = 0, padz_lo = 0, padz_hi = 0;
+    int W2p = 0, H2p = 0, Pp = 0;  // padded 2x-grid width, height and plane count
 };
-cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, Rgc3dTables& t);
+// Tables for planes of w x h pixels, P planes; the per-voxel sums of weights are computed on
+// `stream` (synchronised before returning).
+cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P, Rgc3dTables& t,
+                               cudaStream_t stream);
+size_t rgc3d_field_float4s(const Rgc3dTables& t, int F);
 void rgc3d_tables_free(Rgc3dTables& t);
 struct Rgc3dTabArgs {
-    const float4* U;     // [F][P][2h][2w] unit gradient, columns split by parity ([even | odd])
+    const float4* U;     // [F][Pp][H2p][W2p] padded unit gradient, columns split by parity
     const float* apx;    // [F][P][h][w] aligned planes
     int w, h, P, M, F, t0;
     float sens;
@@ -220,8 +226,10 @@ struct Rgc3dTabArgs {
     BlockState st;
 };
 // unit gradient field from the 2x-resampled components (Gx read at x+1, Gy at y+1, Gz in place)
+// into the interior of the padded field; zero where no tap may read (plane 0, last column and
+// row).  The halo is zeroed once, when the field is allocated.
 cudaError_t unit_grad3d(const float* gxi, const float* gyi, const float* gzi, int w, int h, int P,
-                        int F, float4* U, cudaStream_t stream);
+                        int F, const Rgc3dTables& t, float4* U, cudaStream_t stream);
 cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream);
 
 // camera frames [F][H][W] -> planes [F][P][hs][ws] ((p - background) / coeff), aligned planes,

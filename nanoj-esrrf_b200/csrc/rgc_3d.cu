@@ -180,18 +180,23 @@ __global__ void __launch_bounds__(256) rgc_3d_kernel(Rgc3dArgs a) {
 // Unit gradient of each 2x-grid source point: the reference reads Gx at (x+1, y), Gy at (x, y+1)
 // and Gz at (x, y) of the 2x-resampled components (live3DSRRF.cl RGC; for an in-bounds tap the
 // clamps never bind), so the tap test and |d x G| / |G| = |d x g| only need g = G / |G|.
-// Columns are stored split by parity so that a warp's 32 consecutive voxels read 32 consecutive
-// entries.
+// The field is written into the interior of a zero halo, columns split by parity so that a warp's
+// 32 consecutive voxels read 32 consecutive entries.  Every point no tap may read (outside the
+// volume, the last 2x-grid column and row, plane 0, which the reference never takes a tap from
+// since it requires vz > 0) holds a zero gradient: never inward, so out-of-range taps add
+// nothing, as the reference skips them.
 __global__ void unit_grad3d_kernel(const float* __restrict__ gxi, const float* __restrict__ gyi,
-                                   const float* __restrict__ gzi, int w, int h, float4* __restrict__ U) {
+                                   const float* __restrict__ gzi, int w, int h, int P, int padx,
+                                   int pady, int padz_lo, int W2p, int H2p, int Pp,
+                                   float4* __restrict__ U) {
     const int ax = blockIdx.x * blockDim.x + threadIdx.x;
     const int ay = blockIdx.y;
-    const long fz = blockIdx.z;  // frame * P + plane
+    const int f = blockIdx.z / P, az = blockIdx.z % P;
     const int w2 = 2 * w, h2 = 2 * h;
     if (ax >= w2) return;
     float4 u = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (ax < w2 - 1 && ay < h2 - 1) {
-        const long pl = fz * (long)w2 * h2;
+    if (az > 0 && ax < w2 - 1 && ay < h2 - 1) {
+        const long pl = (long)blockIdx.z * w2 * h2;
         const float Gx = __ldg(gxi + pl + (long)ay * w2 + ax + 1);
         const float Gy = __ldg(gyi + pl + (long)(ay + 1) * w2 + ax);
         const float Gz = __ldg(gzi + pl + (long)ay * w2 + ax);
@@ -201,7 +206,8 @@ __global__ void unit_grad3d_kernel(const float* __restrict__ gxi, const float* _
             u = make_float4(Gx * inv, Gy * inv, Gz * inv, 0.f);
         }
     }
-    U[(fz * h2 + ay) * w2 + (ax & 1) * w + (ax >> 1)] = u;
+    const int xp = ax + padx;  // padx is even: same parity as ax
+    U[((long)(f * Pp + az + padz_lo) * H2p + ay + pady) * W2p + (xp & 1) * (W2p / 2) + (xp >> 1)] = u;
 }
 
 __device__ __forceinline__ float sqrt_approx(float x) {
@@ -219,11 +225,40 @@ __device__ __forceinline__ float tap_term(const float4& A, const float4& B, cons
     return fmaf(-B.z, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz * cz))), B.y);
 }
 
+__device__ __forceinline__ void unpack_offsets(float bits, int& sx, int& sy, int& sz) {
+    const int pk = __float_as_int(bits);
+    sx = (int)((unsigned)pk << 22) >> 22;
+    sy = (int)((unsigned)pk << 12) >> 22;
+    sz = pk >> 20;
+}
+
+// Sum of weights over each output voxel's in-range taps (the reference's Σw, in its tap order),
+// once per handle: it depends on the voxel's phase and on how close it is to the volume's faces.
+__global__ void wsum3d_kernel(Rgc3dTables t, int w, int h, int P, int M, float* __restrict__ out) {
+    const int WM = w * M, HM = h * M;
+    const long total = (long)WM * HM * P * M;
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int zM = (int)(idx / ((long)WM * HM));
+    const int yM = (int)((idx / WM) % HM), xM = (int)(idx % WM);
+    const int qx = xM / M, qy = yM / M, qz = zM / M;
+    const int phase = ((zM % M) * M + yM % M) * M + xM % M;
+    float ws = 0.f;
+    for (int k = t.start[phase]; k < t.start[phase + 1]; ++k) {
+        const float4 B = t.tabb[k];
+        int sx, sy, sz;
+        unpack_offsets(B.w, sx, sy, sz);
+        const int ax = 2 * qx + sx, ay = 2 * qy + sy, az = qz + sz;
+        if (ax < 0 || ax > 2 * w - 2 || ay < 0 || ay > 2 * h - 2 || az < 1 || az > P - 1) continue;
+        ws += B.y;
+    }
+    out[idx] = ws;
+}
+
 // One thread per output voxel; a CTA is 32 x 8 input cells of one (x, y) phase and one output
 // plane, so the whole CTA walks the same tap list (broadcast from shared memory) and a warp's
-// gradient reads are contiguous.  Warps whose taps all fall inside the volume skip the bounds
-// tests and use the phase's tabulated sum of weights; the others test each tap
-// (live3DSRRF.cl: 0 < vx < w, 0 < vy < h, 0 < vz < P) and sum their weights.
+// gradient reads are contiguous.  The zero halo makes every tap readable, so there are no bounds
+// tests; Σw comes from the per-voxel table.
 __global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
     extern __shared__ float4 stab[];  // [2 n]: A entries, then B entries
     const int M = a.M, M2 = M * M;
@@ -241,17 +276,15 @@ __global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
     const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
     const bool valid = qx_raw < a.w && qy_raw < a.h;
     const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
-    const int* meta = a.tab.meta + 6 * phase;
-    const int qa = blockIdx.x * 32, qb = min(blockIdx.x * 32 + 31, a.w - 1);
-    const bool interior = 2 * qa + meta[0] >= 0 && 2 * qb + meta[1] <= 2 * a.w - 2 &&
-                          2 * qy + meta[2] >= 0 && 2 * qy + meta[3] <= 2 * a.h - 2 &&
-                          qz + meta[4] >= 1 && qz + meta[5] <= a.P - 1;
     const int xM = qx * M + px, yM = qy * M + py;
     const int WM = a.w * M, HM = a.h * M;
     const long whM = (long)WM * HM, total = whM * a.P * M;
     const long idx = (long)zM * whM + (long)yM * WM + xM;
     const long pl = (long)a.w * a.h;
-    const float wsum_in = a.tab.wsum[phase];
+    const float wsum = a.tab.wsum[idx];
+    const long fstride = (long)a.tab.Pp * a.tab.H2p * a.tab.W2p;
+    const float4* U0 = a.U + ((long)(qz + a.tab.padz_lo) * a.tab.H2p + 2 * qy + a.tab.pady) * a.tab.W2p +
+                       a.tab.padx / 2 + qx;
     // intensity: cubic in z of four bicubic samples, the fourth plane repeating z0 + 1
     // (live3DSRRF.cl:434-456), no shift
     const float zc = (float)(((double)zM + 0.5) / M);
@@ -270,32 +303,14 @@ __global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
     double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
     float prev = valid ? a.st.prev[idx] : 0.f;
     for (int f = 0; f < a.F; ++f) {
-        const float4* U = a.U + ((long)(f * a.P + qz) * (2 * a.h) + 2 * qy) * (2 * a.w) + qx;
-        float cglh = 0.f, wsum = 0.f;
-        if (interior) {
-            wsum = wsum_in;
-            for (int t = 0; t < n; ++t) {
-                const float4 A = stab[t], B = stab[n + t];
-                const float4 u = __ldg(U + __float_as_int(A.x));
-                const float dot = fmaf(u.x, A.y, fmaf(u.y, A.z, u.z * A.w));
-                if (dot < 0.f) cglh += tap_term(A, B, u);
-            }
-        } else {
-            for (int t = 0; t < n; ++t) {
-                const float4 B = stab[n + t];
-                const int pk = __float_as_int(B.w);
-                const int sx = (int)((unsigned)pk << 22) >> 22;
-                const int sy = (int)((unsigned)pk << 12) >> 22;
-                const int sz = pk >> 20;
-                const int ax = 2 * qx + sx, ay = 2 * qy + sy, az = qz + sz;
-                if (ax < 0 || ax > 2 * a.w - 2 || ay < 0 || ay > 2 * a.h - 2 || az < 1 || az > a.P - 1)
-                    continue;
-                wsum += B.y;
-                const float4 A = stab[t];
-                const float4 u = __ldg(U + __float_as_int(A.x));
-                const float dot = fmaf(u.x, A.y, fmaf(u.y, A.z, u.z * A.w));
-                if (dot < 0.f) cglh += tap_term(A, B, u);
-            }
+        const float4* U = U0 + f * fstride;
+        float cglh = 0.f;
+#pragma unroll 2
+        for (int t = 0; t < n; ++t) {
+            const float4 A = stab[t];
+            const float4 u = __ldg(U + __float_as_int(A.x));
+            const float dot = fmaf(u.x, A.y, fmaf(u.y, A.z, u.z * A.w));
+            if (dot < 0.f) cglh += tap_term(A, stab[n + t], u);
         }
         const float cg = cglh_power(cglh / wsum, a.sens);
         const float* ap = a.apx + (long)f * a.P * pl;
@@ -324,27 +339,30 @@ __global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
 
 }  // namespace
 
-cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, Rgc3dTables& t) {
+cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P, Rgc3dTables& t,
+                               cudaStream_t stream) {
     // Tap geometry of rgc_3d_kernel with zero shift, for the voxel of each phase in the first
     // input cell (Java float arithmetic as the reference: xc = (float)((xM + 0.5) / M)).
     const int r0 = -(int)(2.0f * g.radius), r1 = (int)(2.0f * g.radius + 1);
     const int k0 = -(int)g.radius, k1 = (int)g.radius + 1;
-    const int w2 = 2 * w, h2 = 2 * h, M3 = M * M * M;
-    std::vector<float4> A, B;
-    std::vector<int> start(M3 + 1, 0), meta(6 * M3, 0);
-    std::vector<float> wsum(M3, 0.f);
+    const int M3 = M * M * M;
+    struct Tap {
+        int sx, sy, sz;
+        float dx, dy, dz, d, wt;
+    };
+    std::vector<Tap> taps;
+    std::vector<int> start(M3 + 1, 0);
+    int mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
     int maxn = 0;
     for (int pz = 0; pz < M; ++pz)
         for (int py = 0; py < M; ++py)
             for (int px = 0; px < M; ++px) {
                 const int phase = (pz * M + py) * M + px;
-                start[phase] = (int)A.size();
+                start[phase] = (int)taps.size();
                 const float xc = (float)(((double)px + 0.5) / M);
                 const float yc = (float)(((double)py + 0.5) / M);
                 const float zc = (float)(((double)pz + 0.5) / M);
                 const int kx = (int)(2.0f * xc), ky = (int)(2.0f * yc);
-                int mn[3] = {1 << 20, 1 << 20, 1 << 20}, mx[3] = {-(1 << 20), -(1 << 20), -(1 << 20)};
-                float ws = 0.f;
                 for (int j = r0; j <= r1; ++j) {
                     const float vy = ((float)ky + (float)j) / 2.0f;
                     for (int i = r0; i <= r1; ++i) {
@@ -354,36 +372,45 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, Rgc3dT
                             const float dx = vx - xc, dy = vy - yc, dz = vz - zc;
                             const float d = sqrtf(dx * dx + dy * dy + dz * dz);
                             if (!(d != 0.f && d <= g.tSO)) continue;
-                            const int sx = kx + i - 1, sy = ky + j - 1, sz = k;
-                            // column ax = 2 qx + sx sits at parity (sx & 1), index qx + floor(sx / 2)
-                            // (arithmetic shift; sx may be negative)
-                            const int off = sz * w2 * h2 + sy * w2 + (sx & 1) * w + (sx >> 1);
                             float wt = d * expf(-(d * d) / g.tSS);
                             wt = wt * wt * wt * wt;
-                            ws += wt;
-                            const int pk = (int)(((unsigned)sx & 0x3FFu) | (((unsigned)sy & 0x3FFu) << 10) |
-                                                 ((unsigned)sz << 20));
-                            float offf, pkf;
-                            std::memcpy(&offf, &off, 4);
-                            std::memcpy(&pkf, &pk, 4);
-                            A.push_back(make_float4(offf, dx, dy, dz));
-                            B.push_back(make_float4(d * d, wt, wt / d, pkf));
-                            const int sv[3] = {sx, sy, sz};
+                            const Tap tp{kx + i - 1, ky + j - 1, k, dx, dy, dz, d, wt};
+                            const int sv[3] = {tp.sx, tp.sy, tp.sz};
                             for (int c = 0; c < 3; ++c) {
                                 mn[c] = std::min(mn[c], sv[c]);
                                 mx[c] = std::max(mx[c], sv[c]);
                             }
+                            taps.push_back(tp);
                         }
                     }
                 }
-                wsum[phase] = ws;
-                for (int c = 0; c < 3; ++c) {
-                    meta[6 * phase + 2 * c] = mn[c];
-                    meta[6 * phase + 2 * c + 1] = mx[c];
-                }
-                maxn = std::max(maxn, (int)A.size() - start[phase]);
+                maxn = std::max(maxn, (int)taps.size() - start[phase]);
             }
-    start[M3] = (int)A.size();
+    start[M3] = (int)taps.size();
+    // zero halo: 2x-grid column ax = 2 qx + sx in [sx_min, 2w - 2 + sx_max], row likewise, plane
+    // qz + sz in [sz_min, P - 1 + sz_max]
+    t.padx = std::max(-mn[0], std::max(mx[0] - 1, 0));
+    t.padx += t.padx & 1;
+    t.pady = std::max(-mn[1], std::max(mx[1] - 1, 0));
+    t.padz_lo = std::max(-mn[2], 0);
+    t.padz_hi = std::max(mx[2], 0);
+    t.W2p = 2 * w + 2 * t.padx;
+    t.H2p = 2 * h + 2 * t.pady;
+    t.Pp = P + t.padz_lo + t.padz_hi;
+    std::vector<float4> A, B;
+    A.reserve(taps.size());
+    B.reserve(taps.size());
+    for (const Tap& tp : taps) {
+        // column 2 qx + padx + sx sits at parity (sx & 1), index qx + padx / 2 + floor(sx / 2)
+        const int off = tp.sz * t.W2p * t.H2p + tp.sy * t.W2p + (tp.sx & 1) * (t.W2p / 2) + (tp.sx >> 1);
+        const int pk = (int)(((unsigned)tp.sx & 0x3FFu) | (((unsigned)tp.sy & 0x3FFu) << 10) |
+                             ((unsigned)tp.sz << 20));
+        float offf, pkf;
+        std::memcpy(&offf, &off, 4);
+        std::memcpy(&pkf, &pk, 4);
+        A.push_back(make_float4(offf, tp.dx, tp.dy, tp.dz));
+        B.push_back(make_float4(tp.d * tp.d, tp.wt, tp.wt / tp.d, pkf));
+    }
     t.max_taps = maxn;
     auto up = [](auto** d, const auto& v) -> cudaError_t {
         cudaError_t e = cudaMalloc((void**)d, sizeof(v[0]) * std::max<size_t>(v.size(), 1));
@@ -392,24 +419,29 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, Rgc3dT
     };
     cudaError_t e;
     if ((e = up(&t.taba, A)) != cudaSuccess || (e = up(&t.tabb, B)) != cudaSuccess ||
-        (e = up(&t.start, start)) != cudaSuccess || (e = up(&t.meta, meta)) != cudaSuccess ||
-        (e = up(&t.wsum, wsum)) != cudaSuccess)
+        (e = up(&t.start, start)) != cudaSuccess)
         return e;
-    return cudaSuccess;
+    const long total = (long)w * M * h * M * P * M;
+    if ((e = cudaMalloc((void**)&t.wsum, sizeof(float) * total)) != cudaSuccess) return e;
+    wsum3d_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(t, w, h, P, M, t.wsum);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaStreamSynchronize(stream);
 }
+
+size_t rgc3d_field_float4s(const Rgc3dTables& t, int F) { return (size_t)F * t.Pp * t.H2p * t.W2p; }
 
 void rgc3d_tables_free(Rgc3dTables& t) {
     cudaFree(t.taba);
     cudaFree(t.tabb);
     cudaFree(t.start);
-    cudaFree(t.meta);
     cudaFree(t.wsum);
     t = Rgc3dTables();
 }
 
 cudaError_t unit_grad3d(const float* gxi, const float* gyi, const float* gzi, int w, int h, int P,
-                        int F, float4* U, cudaStream_t stream) {
-    unit_grad3d_kernel<<<dim3((2 * w + 127) / 128, 2 * h, F * P), 128, 0, stream>>>(gxi, gyi, gzi, w, h, U);
+                        int F, const Rgc3dTables& t, float4* U, cudaStream_t stream) {
+    unit_grad3d_kernel<<<dim3((2 * w + 127) / 128, 2 * h, F * P), 128, 0, stream>>>(
+        gxi, gyi, gzi, w, h, P, t.padx, t.pady, t.padz_lo, t.W2p, t.H2p, t.Pp, U);
     return cudaGetLastError();
 }
 
