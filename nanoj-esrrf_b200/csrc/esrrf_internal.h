@@ -209,12 +209,19 @@ struct Rgc3dTables {
     // zero halo of the unit-gradient field: 2x-grid columns (even) and rows, planes below/above
     int padx = 0, pady = 0, padz_lo = 0, padz_hi = 0;
     int W2p = 0, H2p = 0, Pp = 0;  // padded 2x-grid width, height and plane count
+    // z-blocked form (M <= 5): per lateral phase the union over z-phases of the taps, each entry
+    // [offset, dx, dy, then (dz, w, w/d) per z-phase (w = 0: not a tap of that z-phase)], padded
+    // to whole float4s
+    float4* ztab = nullptr;
+    int* zstart = nullptr;    // [M^2 + 1] first entry of each lateral phase
+    int zmax_taps = 0, zes = 0;  // largest entry count of a phase; float4s per entry
 };
 // Tables for planes of w x h pixels, P planes; the per-voxel sums of weights are computed on
 // `stream` (synchronised before returning).
 cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P, Rgc3dTables& t,
                                cudaStream_t stream);
 size_t rgc3d_field_float4s(const Rgc3dTables& t, int F);
+bool rgc3d_one_voxel();
 void rgc3d_tables_free(Rgc3dTables& t);
 struct Rgc3dTabArgs {
     const float4* U;     // [F][Pp][H2p][W2p] padded unit gradient, columns split by parity

@@ -10,6 +10,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -337,6 +338,127 @@ __global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
     a.st.prev[idx] = prev;
 }
 
+// The M voxels of one input cell and lateral phase that differ only in their z-phase read the
+// same gradient sources (the source offsets do not depend on the z-phase), so one thread computes
+// all of them: one gradient load per tap, the dz-free products shared, a (dz, w, w/d) triple per
+// z-phase.  Otherwise as rgc3d_tab_kernel.
+template <int MZ>
+__global__ void __launch_bounds__(256) rgc3d_zb_kernel(Rgc3dTabArgs a) {
+    extern __shared__ float4 sz4[];  // [n][es] entries
+    constexpr int M = MZ, M2 = MZ * MZ;
+    const int es = a.tab.zes;
+    const int qz = blockIdx.z / M2, lp = blockIdx.z % M2;
+    const int px = lp % M, py = lp / M;
+    const int t0 = a.tab.zstart[lp], n = a.tab.zstart[lp + 1] - t0;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < n * es; i += 256) sz4[i] = a.tab.ztab[(long)t0 * es + i];
+    __syncthreads();
+    const float* sf = reinterpret_cast<const float*>(sz4);
+    const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
+    const bool valid = qx_raw < a.w && qy_raw < a.h;
+    const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
+    const int xM = qx * M + px, yM = qy * M + py;
+    const int WM = a.w * M, HM = a.h * M;
+    const long whM = (long)WM * HM, total = whM * a.P * M;
+    const long pl = (long)a.w * a.h;
+    const long fstride = (long)a.tab.Pp * a.tab.H2p * a.tab.W2p;
+    const float4* U0 = a.U + ((long)(qz + a.tab.padz_lo) * a.tab.H2p + 2 * qy + a.tab.pady) * a.tab.W2p +
+                       a.tab.padx / 2 + qx;
+    const float pxf = (float)xM / (float)M - 0.5f;
+    const float pyf = (float)yM / (float)M - 0.5f;
+    long idx[MZ];
+    float wsum[MZ], prev[MZ], z01[MZ];
+    int z0[MZ];
+    double s0[MZ], s1[MZ], s2[MZ], s3[MZ];
+#pragma unroll
+    for (int p = 0; p < MZ; ++p) {
+        const int zM = qz * M + p;
+        idx[p] = (long)zM * whM + (long)yM * WM + xM;
+        wsum[p] = a.tab.wsum[idx[p]];
+        prev[p] = valid ? a.st.prev[idx[p]] : 0.f;
+        // intensity: cubic in z of four bicubic samples, the fourth plane repeating z0 + 1
+        // (live3DSRRF.cl:434-456), no shift
+        const float zc = (float)(((double)zM + 0.5) / M);
+        const float zcof = zc - 0.5f;
+        z0[p] = zcof < 0 ? 0 : (zcof >= (float)(a.P - 1) ? a.P - 2 : (int)floorf(zcof));
+        z01[p] = zc - (float)(z0[p] + 0.5f);
+        s0[p] = s1[p] = s2[p] = s3[p] = 0.0;
+    }
+    for (int f = 0; f < a.F; ++f) {
+        const float4* U = U0 + f * fstride;
+        float cg[MZ];
+#pragma unroll
+        for (int p = 0; p < MZ; ++p) cg[p] = 0.f;
+        for (int t = 0; t < n; ++t) {
+            const float* e = sf + (long)t * es * 4;
+            const float4 u = __ldg(U + __float_as_int(e[0]));
+            const float dx = e[1], dy = e[2];
+            const float part = fmaf(u.x, dx, u.y * dy);
+            const float cz = fmaf(dx, u.y, -dy * u.x);  // dx gy - dy gx
+            const float czz = cz * cz, dyuz = dy * u.z, dxuz = dx * u.z;
+#pragma unroll
+            for (int p = 0; p < MZ; ++p) {
+                const float dz = e[3 + 3 * p], w = e[4 + 3 * p], wd = e[5 + 3 * p];
+                const float dot = fmaf(u.z, dz, part);
+                if (dot < 0.f) {
+                    const float cx = fmaf(-dz, u.y, dyuz);  // dy gz - dz gy
+                    const float cy = fmaf(dz, u.x, -dxuz);  // dz gx - dx gz
+                    cg[p] += fmaf(-wd, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, czz))), w);
+                }
+            }
+        }
+        const float* ap = a.apx + (long)f * a.P * pl;
+#pragma unroll
+        for (int p = 0; p < MZ; ++p) {
+            const float c = cglh_power(cg[p] / wsum[p], a.sens);
+            const int zb = z0[p];
+            const float v_1 = sample2d(ap + (long)max(zb - 1, 0) * pl, a.w, a.h, pxf, pyf);
+            const float v0 = sample2d(ap + (long)zb * pl, a.w, a.h, pxf, pyf);
+            const float v1 = sample2d(ap + (long)(zb + 1) * pl, a.w, a.h, pxf, pyf);
+            const float v2 = sample2d(ap + (long)min(zb + 1, a.P - 1) * pl, a.w, a.h, pxf, pyf);
+            const float ca = -0.5f * v_1 + 1.5f * v0 - 1.5f * v1 + 0.5f * v2;
+            const float cb = v_1 - 2.5f * v0 + 2.0f * v1 - 0.5f * v2;
+            const float cc = -0.5f * v_1 + 0.5f * v1;
+            const float zz = z01[p];
+            const float v = ca * zz * zz * zz + cb * zz * zz + cc * zz + v0;
+            const float x = a.int_weighting ? v * c : c;
+            s0[p] += x;
+            s1[p] += (double)x * x;
+            if (a.t0 + f > 0) s2[p] += (double)x * prev[p];
+            s3[p] += v;
+            prev[p] = x;
+        }
+    }
+    if (!valid) return;
+#pragma unroll
+    for (int p = 0; p < MZ; ++p) {
+        a.st.acc[idx[p]] += s0[p];
+        a.st.acc[total + idx[p]] += s1[p];
+        a.st.acc[2 * total + idx[p]] += s2[p];
+        a.st.acc[3 * total + idx[p]] += s3[p];
+        a.st.prev[idx[p]] = prev[p];
+    }
+}
+
+template <int MZ>
+cudaError_t launch_zb(const Rgc3dTabArgs& a, cudaStream_t stream) {
+    const size_t smem = sizeof(float4) * (size_t)a.tab.zmax_taps * a.tab.zes;
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (smem > 48 * 1024 && dev < 64 && !(configured & (1ull << dev))) {
+        if ((e = cudaFuncSetAttribute(rgc3d_zb_kernel<MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024)) != cudaSuccess)
+            return e;
+        configured |= 1ull << dev;
+    }
+    const dim3 grid((a.w + 31) / 32, (a.h + 7) / 8, MZ * MZ * a.P);
+    rgc3d_zb_kernel<MZ><<<grid, dim3(32, 8), smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P, Rgc3dTables& t,
@@ -412,6 +534,55 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
         B.push_back(make_float4(tp.d * tp.d, tp.wt, tp.wt / tp.d, pkf));
     }
     t.max_taps = maxn;
+    // z-blocked entries: per lateral phase, the (j, i, k) taps valid for at least one z-phase
+    std::vector<float4> Z;
+    std::vector<int> zstart(M * M + 1, 0);
+    if (M <= 5) {
+        t.zes = (3 + 3 * M + 3) / 4;
+        int zmax = 0;
+        for (int py = 0; py < M; ++py)
+            for (int px = 0; px < M; ++px) {
+                const int lp = py * M + px;
+                zstart[lp] = (int)(Z.size() / t.zes);
+                const float xc = (float)(((double)px + 0.5) / M);
+                const float yc = (float)(((double)py + 0.5) / M);
+                const int kx = (int)(2.0f * xc), ky = (int)(2.0f * yc);
+                for (int j = r0; j <= r1; ++j) {
+                    const float vy = ((float)ky + (float)j) / 2.0f;
+                    for (int i = r0; i <= r1; ++i) {
+                        const float vx = ((float)kx + (float)i) / 2.0f;
+                        for (int k = k0; k <= k1; ++k) {
+                            std::vector<float> ent(4 * t.zes, 0.f);
+                            bool any = false;
+                            const float dx = vx - xc, dy = vy - yc;
+                            for (int pz = 0; pz < M; ++pz) {
+                                const float zc = (float)(((double)pz + 0.5) / M);
+                                const float dz = ((float)((int)zc) + (float)k) - zc;
+                                const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+                                ent[3 + 3 * pz] = dz;
+                                if (!(d != 0.f && d <= g.tSO)) continue;
+                                float wt = d * expf(-(d * d) / g.tSS);
+                                wt = wt * wt * wt * wt;
+                                ent[4 + 3 * pz] = wt;
+                                ent[5 + 3 * pz] = wt / d;
+                                any = true;
+                            }
+                            if (!any) continue;
+                            const int sx = kx + i - 1, sy = ky + j - 1, sz = k;
+                            const int off = sz * t.W2p * t.H2p + sy * t.W2p + (sx & 1) * (t.W2p / 2) + (sx >> 1);
+                            std::memcpy(&ent[0], &off, 4);
+                            ent[1] = dx;
+                            ent[2] = dy;
+                            for (int q = 0; q < t.zes; ++q)
+                                Z.push_back(make_float4(ent[4 * q], ent[4 * q + 1], ent[4 * q + 2], ent[4 * q + 3]));
+                        }
+                    }
+                }
+                zmax = std::max(zmax, (int)(Z.size() / t.zes) - zstart[lp]);
+            }
+        zstart[M * M] = (int)(Z.size() / t.zes);
+        t.zmax_taps = zmax;
+    }
     auto up = [](auto** d, const auto& v) -> cudaError_t {
         cudaError_t e = cudaMalloc((void**)d, sizeof(v[0]) * std::max<size_t>(v.size(), 1));
         if (e != cudaSuccess || v.empty()) return e;
@@ -421,11 +592,19 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
     if ((e = up(&t.taba, A)) != cudaSuccess || (e = up(&t.tabb, B)) != cudaSuccess ||
         (e = up(&t.start, start)) != cudaSuccess)
         return e;
+    if (M <= 5 && ((e = up(&t.ztab, Z)) != cudaSuccess || (e = up(&t.zstart, zstart)) != cudaSuccess))
+        return e;
     const long total = (long)w * M * h * M * P * M;
     if ((e = cudaMalloc((void**)&t.wsum, sizeof(float) * total)) != cudaSuccess) return e;
     wsum3d_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(t, w, h, P, M, t.wsum);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return cudaStreamSynchronize(stream);
+}
+
+// ESRRF_RGC3D=voxel selects the one-voxel-per-thread form (kept for comparison and tests).
+bool rgc3d_one_voxel() {
+    const char* s = std::getenv("ESRRF_RGC3D");
+    return s && std::strcmp(s, "voxel") == 0;
 }
 
 size_t rgc3d_field_float4s(const Rgc3dTables& t, int F) { return (size_t)F * t.Pp * t.H2p * t.W2p; }
@@ -435,6 +614,8 @@ void rgc3d_tables_free(Rgc3dTables& t) {
     cudaFree(t.tabb);
     cudaFree(t.start);
     cudaFree(t.wsum);
+    cudaFree(t.ztab);
+    cudaFree(t.zstart);
     t = Rgc3dTables();
 }
 
@@ -446,6 +627,15 @@ cudaError_t unit_grad3d(const float* gxi, const float* gyi, const float* gzi, in
 }
 
 cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream) {
+    if (a.tab.ztab && !rgc3d_one_voxel()) {
+        switch (a.M) {
+            case 2: return launch_zb<2>(a, stream);
+            case 3: return launch_zb<3>(a, stream);
+            case 4: return launch_zb<4>(a, stream);
+            case 5: return launch_zb<5>(a, stream);
+            default: break;
+        }
+    }
     const size_t smem = sizeof(float4) * 2 * (size_t)a.tab.max_taps;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static unsigned long long configured = 0;

@@ -108,21 +108,27 @@ def test_3d_mfm_normalisation_and_nine_planes(esrrf_mod, oracle_mod):
     assert_close(got, ref, "mfm 9 planes")
 
 
-@pytest.mark.parametrize("M,fwhm,S", [(2, 2.0, 2), (4, 1.0, 1), (3, 2.5, 1)])
-def test_3d_tabulated_taps_radii(esrrf_mod, oracle_mod, M, fwhm, S):
-    """Blocks without drift take the tabulated-tap 3-D kernel (taps listed per sub-pixel phase,
-    unit-gradient field, interior warps without bounds tests): checked against the oracle at
-    several magnifications and radii, on a volume small enough that most warps touch an edge
-    and large enough that some do not."""
+@pytest.mark.parametrize("M,fwhm,S,form", [(2, 2.0, 2, "zblock"), (4, 1.0, 1, "zblock"),
+                                            (3, 2.5, 1, "zblock"), (5, 1.5, 1, "zblock"),
+                                            (3, 1.5, 2, "voxel"), (4, 1.0, 1, "voxel")])
+def test_3d_tabulated_taps_radii(esrrf_mod, oracle_mod, monkeypatch, M, fwhm, S, form):
+    """Blocks without drift take the tabulated-tap 3-D kernels (taps listed per sub-pixel phase,
+    zero-halo unit-gradient field, tabulated sums of weights), z-blocked (the M z-phases of a
+    cell in one thread) or one voxel per thread (ESRRF_RGC3D=voxel): checked against the oracle
+    at several magnifications and radii, on volumes where most voxels have taps beyond a face."""
     from esrrf import synth
-    P, h, w, n = 5, 40, 36, 3
+    if form == "voxel":
+        monkeypatch.setenv("ESRRF_RGC3D", "voxel")
+    else:
+        monkeypatch.delenv("ESRRF_RGC3D", raising=False)
+    P, h, w, n = (5, 40, 36, 3) if M < 5 else (3, 20, 18, 3)
     planes = synth.small_stack(7 + M, n, h, w, planes=P).astype(np.float32)
     roi = np.array([4, 0, 8, 5, 1], np.float32)
     zeros = np.zeros(P, np.float32)
     ref = oracle_mod.block3d(planes, M, fwhm, S, zeros, zeros, zeros, mp_correction=False)
     got, _ = run(esrrf_mod, tile_planes(planes, roi), M, fwhm, S, mp=False,
                  calib=calib(P, zeros, zeros, zeros, roi))
-    assert_close(got, ref, f"3d M{M} fwhm{fwhm}")
+    assert_close(got, ref, f"3d M{M} fwhm{fwhm} {form}")
 
 
 def test_3d_drift_per_voxel_kernel(esrrf_mod, oracle_mod):
