@@ -50,15 +50,93 @@ struct AdjLayout {
 struct AdjAArgs {
     const float* I;      // [F][H][W] interpolated frames of the chunk
     const float* a;      // [H][W] dL/dR / T
-    const float4* tab;   // [ii][jj] (w, w/d, kappa = 4 d^2 / tSS^2, 0)
+    const float4* tab;   // [ii][jj] (w, w/d, kappa = 4 d^2 / tSS^2, 0); the taps use w and w/d
     const float* wsum;   // [H][W]
     const float* dwsum;  // [H][W] d(sum of weights)/dtSS
+    const int* jr;       // [S][2] disc chord (first, last tap row) of each tap column
     int W, H, F, r0;
+    float kscale;        // 4 / tSS^2: dw/dtSS = w 4 d^2 / tSS^2
     float sens;
     float* b;            // [F][H][W] dL/dN
     float* gI;           // [F][H][W] initialised with the intensity-weighting term
     double* acc;         // [2]: dL/dS, dL/dtSS
 };
+
+// One tap column of kernel A restricted to its disc chord [LO, HI] (compile-time, as in the fused
+// forward kernel).  The per-output dot product stays (three weight arrays already fill the
+// registers; the forward kernel's per-row threshold spills here).
+template <int S, int LO, int HI>
+__device__ __forceinline__ void chord_a(const float2* __restrict__ col, float fi, const float (&w)[S],
+                                        const float (&wd)[S], float (&acc)[kK], float (&acc2)[kK]) {
+    constexpr int EW = AdjLayout<S>::EW;
+    constexpr float fr0 = -(float)((S - 2) / 2);
+#pragma unroll
+    for (int rr = LO; rr <= HI + kK - 1; ++rr) {
+        const float2 e = col[rr * EW];
+        const float fr = fr0 + (float)rr;
+        const float dot0 = fmaf(e.y, fr, e.x * fi);
+        const float cr0 = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;
+            if (jj >= LO && jj <= HI) {
+                const float dk = k == 0 ? dot0 : fmaf(-(float)k, e.y, dot0);
+                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
+                if (dk < 0.f) {
+                    acc[k] += t;
+                    const float j = fr0 + (float)jj;
+                    acc2[k] = fmaf(j * j, t, acc2[k]);  // j^2 t; i^2 t is added per column
+                }
+            }
+        }
+    }
+}
+
+// The whole box, rows checked by weight (any chord shape; the disc gives the two forms below).
+template <int S>
+__device__ __forceinline__ void box_a(const float2* __restrict__ col, float fi, const float (&w)[S],
+                                      const float (&wd)[S], float (&acc)[kK], float (&acc2)[kK]) {
+    constexpr int EW = AdjLayout<S>::EW;
+    constexpr float fr0 = -(float)((S - 2) / 2);
+#pragma unroll
+    for (int rr = 0; rr < S + kK - 1; ++rr) {
+        const float2 e = col[rr * EW];
+        const float frr = fr0 + (float)rr;
+        const float dot0 = fmaf(e.y, frr, e.x * fi);
+        const float cr0 = fmaf(-e.x, frr, e.y * fi);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;
+            if (jj >= 0 && jj < S) {
+                const float dk = k == 0 ? dot0 : fmaf(-(float)k, e.y, dot0);
+                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
+                if (dk < 0.f) {
+                    acc[k] += t;
+                    const float j = fr0 + (float)jj;
+                    acc2[k] = fmaf(j * j, t, acc2[k]);  // j^2 t; i^2 t is added per column
+                }
+            }
+        }
+    }
+}
+
+// A column's chord in the box [-R, R+1] is the whole box or tap rows [LO, S - 2 - LO].
+template <int S, int LO>
+__device__ __forceinline__ void dispatch_a(const float2* __restrict__ col, float fi, int lo, int hi,
+                                           const float (&w)[S], const float (&wd)[S], float (&acc)[kK],
+                                           float (&acc2)[kK]) {
+    if constexpr (LO <= (S - 2) / 2) {
+        if (lo == LO && hi == S - 2 - LO) {
+            chord_a<S, LO, S - 2 - LO>(col, fi, w, wd, acc, acc2);
+            return;
+        }
+        dispatch_a<S, LO + 1>(col, fi, lo, hi, w, wd, acc, acc2);
+    } else {
+        box_a<S>(col, fi, w, wd, acc, acc2);
+    }
+}
 
 // Kernel A: forward tap loop with a second accumulator for dN/dtSS.
 template <int S>
@@ -113,36 +191,26 @@ __global__ void __launch_bounds__(256, 2) adj_a_kernel(AdjAArgs g) {
 #pragma unroll
         for (int k = 0; k < kK; ++k) acc[k] = acc2[k] = 0.f;
         for (int ii = 0; ii < S; ++ii) {
+            const int lo = __ldg(g.jr + 2 * ii), hi = __ldg(g.jr + 2 * ii + 1);
+            if (lo > hi) continue;  // no tap of the disc in this column
             const float fi = fr0 + (float)ii;
-            float w[S], wd[S], kap[S];
+            float w[S], wd[S], before[kK];
 #pragma unroll
             for (int jj = 0; jj < S; ++jj) {
                 const float4 t = stab[ii * S + jj];
                 w[jj] = t.x;
                 wd[jj] = t.y;
-                kap[jj] = t.z;
             }
+#pragma unroll
+            for (int k = 0; k < kK; ++k) before[k] = acc[k];
             const float2* col = sE + (ty * kK) * EW + tx + ii;
+            if (lo == 0 && hi == S - 1)
+                chord_a<S, 0, S - 1>(col, fi, w, wd, acc, acc2);
+            else
+                dispatch_a<S, 0>(col, fi, lo, hi, w, wd, acc, acc2);
+            // d^2 = i^2 + j^2: the column's i^2 times its inward sum
 #pragma unroll
-            for (int rr = 0; rr < S + kK - 1; ++rr) {
-                const float2 e = col[rr * EW];
-                const float frr = fr0 + (float)rr;
-                const float dot0 = fmaf(e.y, frr, e.x * fi);
-                const float cr0 = fmaf(-e.x, frr, e.y * fi);
-#pragma unroll
-                for (int k = 0; k < kK; ++k) {
-                    const int jj = rr - k;
-                    if (jj >= 0 && jj < S) {
-                        const float dk = k == 0 ? dot0 : fmaf(-(float)k, e.y, dot0);
-                        const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
-                        const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
-                        if (dk < 0.f) {
-                            acc[k] += t;
-                            acc2[k] = fmaf(kap[jj], t, acc2[k]);
-                        }
-                    }
-                }
-            }
+            for (int k = 0; k < kK; ++k) acc2[k] = fmaf(fi * fi, acc[k] - before[k], acc2[k]);
         }
 #pragma unroll
         for (int k = 0; k < kK; ++k) {
@@ -159,7 +227,7 @@ __global__ void __launch_bounds__(256, 2) adj_a_kernel(AdjAArgs g) {
                 dC = av * v * g.sens * Cs / C;
                 b = dC / ws;
                 dS += (double)av * v * Cs * lc;
-                dT += (double)b * (acc2[k] - C * __ldg(g.dwsum + pix));
+                dT += (double)b * (acc2[k] * g.kscale - C * __ldg(g.dwsum + pix));
             }
             g.gI[(long)f * wh + pix] = av * Cs;
             g.b[(long)f * wh + pix] = b;
@@ -201,9 +269,57 @@ struct AdjBArgs {
     const float* I;     // [F][H][W]
     const float* b;     // [F][H][W]
     const float* wdB;   // [ii'][jj'] = w/d of tap (r1 - ii', r1 - jj')
+    const int* jr;      // [S][2] disc chord of each tap column, kernel A's (forward) order
     int W, H, F, r1;
     float* gI;          // [F][H][W], accumulated atomically
 };
+
+// One column ii' of kernel B's gather over its chord of tap rows [LO, HI] (jj' = r1 - t_y).
+template <int S, int LO, int HI>
+__device__ __forceinline__ void chord_b(const float* __restrict__ col, float tx_f, const float (&wd)[S],
+                                        const float (&gx)[kK], const float (&gy)[kK], const float (&Ak)[kK],
+                                        const float (&Bk)[kK], float (&Sx)[kK], float (&Tx)[kK],
+                                        float (&Sy)[kK]) {
+    constexpr int BW = AdjBLayout<S>::BW;
+#pragma unroll
+    for (int rr = LO; rr <= HI + kK - 1; ++rr) {
+        const float bv = col[rr * BW];
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;  // t_y = r1 - jj = r1 + k - rr
+            if (jj >= LO && jj <= HI) {
+                const float dot = fmaf(-gy[k], (float)rr, Ak[k]);
+                const float c = fmaf(gx[k], (float)rr, Bk[k]);
+                if (dot < 0.f) {
+                    // (w/d) b sgn(c): flip the sign bit of (w/d) b by that of c
+                    const float sv = __int_as_float(__float_as_int(wd[jj] * bv) ^
+                                                    (__float_as_int(c) & 0x80000000));
+                    Sx[k] += sv;
+                    Tx[k] = fmaf(sv, (float)rr, Tx[k]);
+                    Sy[k] = fmaf(sv, tx_f, Sy[k]);
+                }
+            }
+        }
+    }
+}
+
+// Kernel B's column ii' is the forward column S - 1 - ii' read from the other end, so its
+// chords are the whole box or tap rows [LO + 1, S - 1 - LO]; any other shape takes the box.
+template <int S, int LO>
+__device__ __forceinline__ void dispatch_b(const float* __restrict__ col, float tx_f, int lo, int hi,
+                                           const float (&wd)[S], const float (&gx)[kK], const float (&gy)[kK],
+                                           const float (&Ak)[kK], const float (&Bk)[kK], float (&Sx)[kK],
+                                           float (&Tx)[kK], float (&Sy)[kK]) {
+    if constexpr (LO <= (S - 2) / 2) {
+        if (lo == LO + 1 && hi == S - 1 - LO) {
+            chord_b<S, LO + 1, S - 1 - LO>(col, tx_f, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);
+            return;
+        }
+        dispatch_b<S, LO + 1>(col, tx_f, lo, hi, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);
+    } else {
+        chord_b<S, 0, S - 1>(col, tx_f, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);  // zero w/d off the disc
+    }
+}
 
 // Kernel B: per tap source, gather over the taps of the outputs it feeds.
 template <int S>
@@ -263,6 +379,10 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
 #pragma unroll
         for (int k = 0; k < kK; ++k) Sx[k] = Tx[k] = Sy[k] = 0.f;
         for (int ii = 0; ii < S; ++ii) {   // ii' : t_x = r1 - ii'
+            // forward column S - 1 - ii', rows reflected
+            const int lof = __ldg(g.jr + 2 * (S - 1 - ii)), hif = __ldg(g.jr + 2 * (S - 1 - ii) + 1);
+            if (lof > hif) continue;  // no tap of the disc in this column
+            const int lo = S - 1 - hif, hi = S - 1 - lof;
             const float tx_f = fr1 - (float)ii;
             float wd[S];
 #pragma unroll
@@ -274,26 +394,10 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
                 Bk[k] = fmaf(gy[k], tx_f, -gx[k] * (fr1 + (float)k));
             }
             const float* col = sB + (ty * kK) * BW + tx + ii;
-#pragma unroll
-            for (int rr = 0; rr < S + kK - 1; ++rr) {
-                const float bv = col[rr * BW];
-#pragma unroll
-                for (int k = 0; k < kK; ++k) {
-                    const int jj = rr - k;  // t_y = r1 - jj = r1 + k - rr
-                    if (jj >= 0 && jj < S) {
-                        const float dot = fmaf(-gy[k], (float)rr, Ak[k]);
-                        const float c = fmaf(gx[k], (float)rr, Bk[k]);
-                        if (dot < 0.f) {
-                            // (w/d) b sgn(c): flip the sign bit of (w/d) b by that of c
-                            const float sv = __int_as_float(__float_as_int(wd[jj] * bv) ^
-                                                            (__float_as_int(c) & 0x80000000));
-                            Sx[k] += sv;
-                            Tx[k] = fmaf(sv, (float)rr, Tx[k]);
-                            Sy[k] = fmaf(sv, tx_f, Sy[k]);
-                        }
-                    }
-                }
-            }
+            if (lo == 0 && hi == S - 1)
+                chord_b<S, 0, S - 1>(col, tx_f, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);
+            else
+                dispatch_b<S, 0>(col, tx_f, lo, hi, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);
         }
         // project onto the tangent of the unit vector and scatter through the Roberts cross
 #pragma unroll
@@ -634,6 +738,8 @@ esrrf_status esrrf_adjoint::backward(const float* frames, float fwhm, float sens
         A.tab = tabA;
         A.wsum = tables.wsum;
         A.dwsum = dwsum;
+        A.jr = tables.jrange;
+        A.kscale = (float)(4.0 / ((double)geo.tSS * (double)geo.tSS));
         A.W = WM;
         A.H = HM;
         A.F = n;
@@ -646,6 +752,7 @@ esrrf_status esrrf_adjoint::backward(const float* frames, float fwhm, float sens
         B.I = A.I;
         B.b = bbuf;
         B.wdB = wdB;
+        B.jr = tables.jrange;
         B.W = WM;
         B.H = HM;
         B.F = n;
