@@ -366,34 +366,46 @@ __global__ void __launch_bounds__(256) adj_proj_kernel(const float* __restrict__
 //   dwy[m] = s_a (Dy' Gc)[m] - s_a (Dy' Gu)[(N-m)%N]
 //   dwx[m] = s_a (Dx' Gtc)[m] - s_a (Dx' Gtu)[(N-m)%N]
 //   dq     = s (cy.Gc - uy.(Gc + Gu) - cy.Gu)
-// Grid (ceil(2N/256), F); thread m < N computes dwy[m], N <= m < 2N computes dwx[m - N];
-// block 0 also reduces dq.  dx is Dx row-major [WM][N] (scaled like dxT).
+// Grid (ceil(2N/32), F); output m < N is dwy[m], N <= m < 2N is dwx[m - N]; block 0 also
+// reduces dq.  dx is Dx row-major [WM][N] (scaled like dxT).
 __global__ void __launch_bounds__(256) adj_rank1_kernel(const float* __restrict__ proj,
                                                         const float* __restrict__ dy,
                                                         const float* __restrict__ dx, int N, int HM,
                                                         int WM, const float* __restrict__ cy,
                                                         const float* __restrict__ uy, float s_axis,
                                                         float s, float* __restrict__ dvec) {
+    // 32 outputs per block (one per lane); the 8 warps split the rows and reduce in shared memory
     const int f = blockIdx.y;
     const float* pr = proj + (long)f * (2 * HM + 2 * WM);
     float* dv = dvec + (long)f * (2 * N + 1);
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int m = blockIdx.x * 32 + lane;
+    __shared__ float ra[8][32], rb[8][32];
+    float a = 0.f, b = 0.f;
     if (m < N) {
         const int mf = (N - m) & (N - 1);
-        float a = 0.f, b = 0.f;
-        for (int y = 0; y < HM; ++y) {
+        for (int y = wq; y < HM; y += 8) {
             a = fmaf(dy[(long)y * N + m], pr[y], a);
             b = fmaf(dy[(long)y * N + mf], pr[HM + y], b);
         }
-        dv[m] = s_axis * (a - b);
     } else if (m < 2 * N) {
         const int mm = m - N, mf = (N - mm) & (N - 1);
-        float a = 0.f, b = 0.f;
-        for (int x = 0; x < WM; ++x) {
+        for (int x = wq; x < WM; x += 8) {
             a = fmaf(dx[(long)x * N + mm], pr[2 * HM + x], a);
             b = fmaf(dx[(long)x * N + mf], pr[2 * HM + WM + x], b);
         }
-        dv[N + mm] = s_axis * (a - b);
+    }
+    ra[wq][lane] = a;
+    rb[wq][lane] = b;
+    __syncthreads();
+    if (wq == 0 && m < 2 * N) {
+        float A = 0.f, B = 0.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            A += ra[i][lane];
+            B += rb[i][lane];
+        }
+        dv[m] = s_axis * (A - B);  // dv[m] (m < N) or dv[N + mm]
     }
     if (blockIdx.x == 0) {
         __shared__ float red[8];
@@ -455,7 +467,7 @@ cudaError_t interp_adjoint_run(const InterpPlan& p, const float* dx, const float
     gemm_kernel<4><<<dim3((g.Nc + 127) / 128, (g.Mr + 127) / 128, F), 256, 0, stream>>>(g);
     adj_proj_kernel<<<dim3((p.HM + p.WM + 7) / 8, F), 256, 0, stream>>>(gI, p.HM, p.WM, p.cx, p.ux,
                                                                          p.cy, p.uy, proj);
-    adj_rank1_kernel<<<dim3((2 * N + 255) / 256, F), 256, 0, stream>>>(
+    adj_rank1_kernel<<<dim3((2 * N + 31) / 32, F), 256, 0, stream>>>(
         proj, p.dy, dx, N, p.HM, p.WM, p.cy, p.uy, (float)p.s_axis, (float)p.s, dvec);
     adj_scatter_kernel<<<dim3((N + 255) / 256, N, F), 256, 0, stream>>>(
         gX, dvec, N, p.w, p.h, p.srcx, p.srcy, p.identity_pad ? 1 : 0, graw);
