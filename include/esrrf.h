@@ -206,6 +206,31 @@ esrrf_status esrrf_sweep_launch_count(const esrrf_sweep* s, int* launches);
 const char* esrrf_sweep_last_error(const esrrf_sweep* s);
 esrrf_status esrrf_sweep_destroy(esrrf_sweep* s);
 
+/* ---- SQUIRREL metrics ----------------------------------------------------------------------------
+ * Replaces ErrorMapLiveSRRF.optimise + calculateErrorMap (ErrorMapLiveSRRF.java:81-193) as the
+ * parameter sweep applies them to every reconstruction (gui/ParametersSweep_.java:468-519): for
+ * each super-resolved image and its reference (the INT slice of the same block), the blur sigma in
+ * [0, 4 / 2.35482 M] pixels minimising the RMSE of the blurred, intensity-fitted image (Brent
+ * search), the fit's alpha and beta, RSE (that RMSE), RSP (its Pearson coefficient) and optionally
+ * the error map |ref - blur(alpha SR + beta)|. */
+typedef struct {
+    int width, height;     /* super-resolved image size in pixels */
+    int magnification;     /* M: sigma bound 4 / 2.35482 M pixels; fixed sigma and crop x M */
+    int fix_sigma;         /* 1: sigma = fixed_sigma x M, no search */
+    float fixed_sigma;     /* input pixels */
+    int crop;              /* border of this many input pixels (x M) left out of everything */
+    void* stream;          /* cudaStream_t for the work (NULL: the default stream) */
+} esrrf_squirrel_params;
+
+/* d_base: device floats; image i is [height][width] at d_base + sr_offsets[i], its reference at
+ * d_base + ref_offsets[i] (host arrays; references may repeat).  Host outputs (each may be NULL):
+ * sigma, alpha, beta, rse, rsp [n].  d_error_maps (device, may be NULL): [n][h'][w'], the cropped
+ * size.  Returns when the results are on the host. */
+esrrf_status esrrf_squirrel(const esrrf_squirrel_params* p, int n, const float* d_base,
+                            const size_t* sr_offsets, const size_t* ref_offsets, float* sigma,
+                            float* alpha, float* beta, float* rse, float* rsp, float* d_error_maps);
+const char* esrrf_squirrel_last_error(void);
+
 /* ---- Differentiable eSRRF ---------------------------------------------------------------------
  * A fidelity loss of the 2-D FHT-path AVG reconstruction and its hand-written adjoint; there is
  * no counterpart in the reference's OpenCL path (the closest is the post-hoc error map of

@@ -284,6 +284,23 @@ class Sweep:
                         out[(int(M), float(r), int(S), (int(self.bstart[bi]), int(self.blen[bi])))] = blk[si, bi]
         return out
 
+    def squirrel(self, results, fixed_sigma=None, crop=0, device=0):
+        """SQUIRREL metrics of every AVG, VAR and TAC2 reconstruction of `results` (run's dict)
+        against the INT slice of the same block, as ParametersSweep_ scores its reconstructions
+        (gui/ParametersSweep_.java:468-519): {key: {"AVG"|"VAR"|"TAC2": {sigma, alpha, beta,
+        rse, rsp}}}, one batched call per magnification."""
+        out = {}
+        for M in sorted({k[0] for k in results}):
+            keys = [k for k in results if k[0] == M]
+            sr = np.stack([results[k][c] for k in keys for c in range(3)])
+            ref = np.stack([results[k][3] for k in keys])
+            m = squirrel(sr, ref, M, fixed_sigma=fixed_sigma, crop=crop,
+                         ref_index=[i // 3 for i in range(3 * len(keys))], device=device)
+            for i, k in enumerate(keys):
+                out[k] = {name: {f: float(m[f][3 * i + c]) for f in ("sigma", "alpha", "beta", "rse", "rsp")}
+                          for c, name in enumerate(("AVG", "VAR", "TAC2"))}
+        return out
+
     def run(self, stack):
         a = np.asarray(stack)
         if a.dtype == np.uint16:
@@ -320,6 +337,56 @@ def rolling(stack, magnification, fwhm, sensitivity, blocks, int_weighting=True)
         return {k[3]: v.copy() for k, v in res.items()}
     finally:
         sw.release()
+
+
+def squirrel(sr, ref, magnification, fixed_sigma=None, crop=0, error_maps=False, ref_index=None,
+             device=0):
+    """SQUIRREL metrics (esrrf_squirrel; ErrorMapLiveSRRF.optimise + calculateErrorMap,
+    ErrorMapLiveSRRF.java:81-193) of super-resolved images against references.
+
+    sr: [n][H][W]; ref: [n][H][W], [H][W] (one reference for all) or, with ref_index ([n] ints),
+    [m][H][W] with image i scored against ref[ref_index[i]]; numpy arrays or torch CUDA tensors.
+    fixed_sigma (input pixels) skips the sigma search; crop: border in input pixels.  Returns a
+    dict of numpy arrays sigma, alpha, beta, rse, rsp ([n]) and, with error_maps, "error_map"
+    [n][H'][W'] (the cropped size)."""
+    import torch
+
+    from ._lib import EsrrfSquirrelParams
+
+    dev = f"cuda:{device}"
+    srt = torch.as_tensor(sr, dtype=torch.float32, device=dev).contiguous()
+    if srt.dim() == 2:
+        srt = srt[None]
+    reft = torch.as_tensor(ref, dtype=torch.float32, device=dev).contiguous()
+    if reft.dim() == 2:
+        reft = reft[None]
+    n, H, W = srt.shape
+    if ref_index is None:
+        if reft.shape[0] not in (1, n):
+            raise EsrrfError("ref must be [H][W] or [n][H][W] like sr (or give ref_index)")
+        ref_index = [i if reft.shape[0] == n else 0 for i in range(n)]
+    ref_index = [int(r) for r in ref_index]
+    if reft.shape[-2:] != (H, W) or len(ref_index) != n or min(ref_index) < 0 or max(ref_index) >= reft.shape[0]:
+        raise EsrrfError("ref images must match sr in size and ref_index must select them")
+    both = torch.cat([srt.reshape(-1), reft.reshape(-1)])
+    P = H * W
+    sro = (ctypes.c_size_t * n)(*[i * P for i in range(n)])
+    rfo = (ctypes.c_size_t * n)(*[n * P + r * P for r in ref_index])
+    cb = int(crop) * int(magnification) if crop else 0
+    maps = torch.empty((n, H - 2 * cb, W - 2 * cb), dtype=torch.float32, device=dev) if error_maps else None
+    out = {k: np.empty(n, np.float32) for k in ("sigma", "alpha", "beta", "rse", "rsp")}
+    fp = ctypes.POINTER(ctypes.c_float)
+    p = EsrrfSquirrelParams(W, H, int(magnification), int(fixed_sigma is not None),
+                            float(fixed_sigma or 0.0), int(crop),
+                            ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream))
+    with torch.cuda.device(device):
+        _lib.check(None, lib().esrrf_squirrel(ctypes.byref(p), n, ctypes.c_void_p(both.data_ptr()), sro, rfo,
+                                              *[out[k].ctypes.data_as(fp) for k in ("sigma", "alpha", "beta", "rse", "rsp")],
+                                              ctypes.c_void_p(maps.data_ptr()) if maps is not None else None),
+                   squirrel=True)
+    if maps is not None:
+        out["error_map"] = maps.cpu().numpy()
+    return out
 
 
 class Adjoint:

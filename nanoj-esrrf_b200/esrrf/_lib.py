@@ -92,6 +92,23 @@ class EsrrfSweepParams(ctypes.Structure):
     ]
 
 
+class EsrrfSquirrelParams(ctypes.Structure):
+    """esrrf_squirrel_params (include/esrrf.h)."""
+
+    _fields_ = [
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("magnification", ctypes.c_int),
+        ("fix_sigma", ctypes.c_int), ("fixed_sigma", ctypes.c_float), ("crop", ctypes.c_int),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+SIGNATURES.update({
+    "esrrf_squirrel": (_c.c_int, [_c.POINTER(EsrrfSquirrelParams), _c.c_int, _c.c_void_p,
+                                  _c.POINTER(_c.c_size_t), _c.POINTER(_c.c_size_t), _f32p, _f32p,
+                                  _f32p, _f32p, _f32p, _c.c_void_p]),
+    "esrrf_squirrel_last_error": (_c.c_char_p, []),
+})
+
 SIGNATURES.update({
     "esrrf_sweep_create": (_c.c_int, [_c.POINTER(EsrrfSweepParams), _c.POINTER(_c.c_void_p)]),
     "esrrf_sweep_output_layout": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_size_t),
@@ -129,9 +146,13 @@ def lib():
     return _LIB
 
 
-def check(handle, rc: int, sweep: bool = False, adjoint: bool = False) -> None:
+def check(handle, rc: int, sweep: bool = False, adjoint: bool = False, squirrel: bool = False) -> None:
     if rc == 0:
         return
+    if squirrel:
+        msg = lib().esrrf_squirrel_last_error()
+        msg = msg.decode() if msg else ""
+        raise EsrrfError(f"esrrf status {STATUS.get(rc, rc)}: {msg}")
     fn = lib().esrrf_adjoint_last_error if adjoint else (
         lib().esrrf_sweep_last_error if sweep else lib().esrrf_last_error)
     msg = fn(handle)
