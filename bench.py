@@ -411,6 +411,51 @@ def run_sweep(args, world, rank, local):
     esrrf._lib.check(sw.handle, L.esrrf_sweep_run(sw.handle, ctypes.c_void_p(h_stack.data_ptr()), 1,
                                                   ctypes.c_void_p(h_out.data_ptr())), sweep=True)
     e2e = time.perf_counter() - t0
+
+    # SQUIRREL scoring of every reconstruction (AVG, VAR, TAC2 against the block's INT slice),
+    # on the sweep's device-resident output, one batched call per magnification
+    def squirrel_all():
+        fp = ctypes.POINTER(ctypes.c_float)
+        n_img, nR, nS, nB = 0, len(SWEEP_RADII), len(SWEEP_SENS), len(SWEEP_BLOCKS)
+        for mi, M in enumerate(SWEEP_MAGS):
+            P = h * M * w * M
+            sro, rfo = [], []
+            for ri in range(nR):
+                base = sw.offsets[mi * nR + ri]
+                for si in range(nS):
+                    for bi in range(nB):
+                        blk = base + (si * nB + bi) * 4 * P
+                        for c in range(3):
+                            sro.append(blk + c * P)
+                            rfo.append(blk + 3 * P)
+            n = len(sro)
+            outs = [np.empty(n, np.float32) for _ in range(5)]
+            p = esrrf._lib.EsrrfSquirrelParams(w * M, h * M, M, 0, 0.0, 0,
+                                               ctypes.c_void_p(torch.cuda.current_stream(local).cuda_stream))
+            esrrf._lib.check(None, L.esrrf_squirrel(ctypes.byref(p), n, ctypes.c_void_p(d_out.data_ptr()),
+                                                    (ctypes.c_size_t * n)(*sro), (ctypes.c_size_t * n)(*rfo),
+                                                    *[o.ctypes.data_as(fp) for o in outs], None), squirrel=True)
+            n_img += n
+        return n_img
+
+    sq_images, sq_s = 0, None
+    if rank == 0:
+        step()
+        torch.cuda.synchronize()
+        squirrel_all()  # warm-up
+        t0 = time.perf_counter()
+        sq_images = squirrel_all()
+        sq_s = time.perf_counter() - t0
+        # CPU stand-in: the float64 restatement on two reconstructions (one per magnification)
+        from oracle import squirrel_oracle as Q
+        flat = d_out.cpu().numpy()
+        t0 = time.perf_counter()
+        for mi, M in enumerate(SWEEP_MAGS):
+            P = h * M * w * M
+            base = sw.offsets[mi * len(SWEEP_RADII) + 4]
+            img = flat[base:base + 4 * P].reshape(4, h * M, w * M)
+            Q.squirrel(img[0], img[3], M)
+        sq_cpu_per_image = (time.perf_counter() - t0) / len(SWEEP_MAGS)
     sw.release()
 
     def single_combo_loop(kernel, subset=None):
@@ -456,6 +501,12 @@ def run_sweep(args, world, rank, local):
         "e2e": {"value": combos / e2e, "unit": "combos/s", "h2d_bytes_per_step": int(stack.nbytes),
                 "d2h_bytes_per_step": int(h_out.numel() * 4)},
         "gpu_launches": launches, "clocks": clk.summary(),
+        "squirrel": {"images": sq_images, "seconds": sq_s, "images_per_s": sq_images / sq_s,
+                     "what": "RSE, RSP (Brent-optimised blur sigma, alpha/beta fit) of every AVG, "
+                             "VAR and TAC2 reconstruction against its block's INT slice",
+                     "cpu_port_seconds_per_image": sq_cpu_per_image,
+                     "cpu_note": "float64 numpy restatement, one image of each magnification; the "
+                                 "reference's own ImageJ/commons-math path needs a JVM"},
     }
     print(json.dumps(line))
 
