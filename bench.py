@@ -41,6 +41,7 @@ WORKLOADS = {
     "sweep256": ("sweep256", 0),  # batched parameter sweep (88 combinations, uneven blocks)
     "mfm3d": ("mfm3d", 200),     # 3-D MFM path, 9 planes
     "adjoint256": ("adjoint256", 100),  # differentiable eSRRF: loss + gradients
+    "drift512": ("fht512", 100),  # drift estimation per block of the headline stack
 }
 SWEEP_RADII = [0.5 + 0.25 * i for i in range(11)]
 SWEEP_SENS = [1, 2, 3, 4]
@@ -185,6 +186,20 @@ def run_reference(args, world, rank):
 
     name, nf = WORKLOADS[args.workload]
     wl = synth.WORKLOADS[name]
+    if args.workload == "drift512":
+        stack = synth.make_stack(name, frames=20)
+        vals = [drift_cpu_sample(stack, 20) for _ in range(args.warmup + args.steps)][args.warmup:]
+        v = statistics.median([r["value"] for r in vals])
+        print(json.dumps({
+            "impl": "reference", "metric": "frames/s (drift estimation)", "value": v, "unit": "frames/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * 20 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "drift512: 512x512 uint16 frames against a reference frame "
+                                   "(bounded sample: 20 frames per step)"},
+            "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "frames/s"},
+            "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
     stack = synth.make_stack(name, frames=max(2, args.steps + args.warmup))
     M, fwhm, S = wl.magnification, wl.fwhm, wl.sensitivity
     vals = []
@@ -615,6 +630,96 @@ def run_3d(args, world, rank, local):
         "gpu_launches": launches[0] // max(1, args.steps), "clocks": clk.summary()}))
 
 
+def drift_cpu_sample(stack, n):
+    """The float64 numpy-FFT restatement (oracle/drift_oracle.py) on n frames, timed."""
+    from oracle import drift_oracle as D
+
+    t0 = time.perf_counter()
+    D.estimate_drift(stack[:n].astype(np.float64))
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "frames/s", "cores": 1, "kind": "port",
+            "sample": f"{n} frames of {stack.shape[2]}x{stack.shape[1]} against the first: numpy FFT "
+                      f"(one thread), window, arg-max, quadratic fit; {dt:.2f} s"}
+
+
+def run_drift(args, world, rank, local):
+    """Drift estimation over the headline stack (512x512x500 uint16): one esrrf_estimate_drift call
+    per block of 100 frames against the block's first frame, as the live plugin does per SR frame
+    (LiveSRRF_optimised_.java:283-288).  Lags |s| <= 31."""
+    import ctypes
+
+    import torch
+
+    import esrrf
+    from esrrf import synth
+
+    torch.cuda.set_device(local)
+    stack = synth.make_stack("fht512", frames=args.frames)
+    n, h, w = stack.shape
+    blk = args.block or 100
+    blocks = [(i, min(blk, n - i)) for i in range(0, n, blk)]
+    d = torch.from_numpy(stack.view(np.int16)).to(f"cuda:{local}")
+    L = esrrf.lib()
+    R = esrrf.drift_window(w, h)
+    sx = np.empty(blk, np.float32)
+    sy = np.empty(blk, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    stream = torch.cuda.current_stream(local)
+
+    def call(ptr, i0, cnt):
+        esrrf._lib.check(None, L.esrrf_estimate_drift(
+            ctypes.c_void_p(ptr + 2 * i0 * h * w), 1, cnt, w, h, 0, R, sx.ctypes.data_as(fp),
+            sy.ctypes.data_as(fp), None, ctypes.c_void_p(stream.cuda_stream)), drift=True)
+
+    def step():
+        for i0, cnt in blocks:
+            call(d.data_ptr(), i0, cnt)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t_step = max_over_ranks(world, e0.elapsed_time(e1) / 1e3 / args.steps)
+    # end to end: each block copied from pinned host memory, then estimated
+    h_st = torch.from_numpy(stack.view(np.int16)).pin_memory()
+    d_blk = torch.empty((blk, h, w), dtype=torch.int16, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i0, cnt in blocks:
+        d_blk[:cnt].copy_(h_st[i0:i0 + cnt], non_blocking=True)
+        call(d_blk.data_ptr(), 0, cnt)
+    e2e = time.perf_counter() - t0
+    if rank != 0:
+        return
+    cpu = None if args.no_cpu_baseline or world > 1 else drift_cpu_sample(stack, 40)
+    side = 2 * R + 1
+    flop = 2.0 * h * w * side * side * n  # one FMA per pixel per lag
+    achieved = flop / t_step / 1e12
+    print(json.dumps({
+        "metric": "frames/s (drift estimation)", "value": world * n / t_step, "unit": "frames/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"drift512: {w}x{h}x{n} uint16, blocks of {blk}, lags |s| <= {R}, "
+                               "reference = each block's first frame",
+                   "l2": "frames (262 MB) larger than L2"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": FP32_PEAK_NOMINAL_TFLOPS,
+                     "unit": "TFLOP/s", "frac": achieved / FP32_PEAK_NOMINAL_TFLOPS, "traffic": None,
+                     "note": "2 flops per pixel per lag over whole calls (4 kernels + 8 B/frame read "
+                             "back); peak = nominal FP32 FMA rate at 1965 MHz"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n / e2e, "unit": "frames/s", "h2d_bytes_per_step": int(stack.nbytes),
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": 4 * len(blocks), "clocks": clk.summary()}))
+
+
 def run_adjoint(args, world, rank, local):
     """Differentiable eSRRF on 256x256x100, M4: forward (loss) time, loss-and-gradient time, their
     ratio, and a gradient search on (radius, sensitivity, re-blur sigma) beside a grid search."""
@@ -706,6 +811,8 @@ def main():
             run_3d(args, world, rank, local)
         elif args.workload == "adjoint256":
             run_adjoint(args, world, rank, local)
+        elif args.workload == "drift512":
+            run_drift(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -231,6 +231,24 @@ esrrf_status esrrf_squirrel(const esrrf_squirrel_params* p, int n, const float* 
                             float* alpha, float* beta, float* rse, float* rsp, float* d_error_maps);
 const char* esrrf_squirrel_last_error(void);
 
+/* ---- Drift (vibration) estimation ---------------------------------------------------------------
+ * Replaces XYShiftCalculator.calculateShiftArray (XYShiftCalculator.java:26-48), whose shifts the
+ * plugins hand to loadDriftXYGPUbuffer (gui/ParametersSweep_.java:282-290,
+ * gui/LiveSRRF_optimised_.java:283-305), i.e. to esrrf_set_drift.  For each frame f, the circular
+ * cross-correlation C_f(s) = sum_p (ref(p) - mean ref) frame_f(p + s) over the lags |sx|, |sy| <= R,
+ * its arg-max and the stationary point of the least-squares quadratic through the 3 x 3 samples
+ * around it.  shift_x/shift_y[f] is the displacement of frame f's content relative to the reference
+ * frame, the value esrrf_set_drift takes for that frame.  The reference searches the whole map;
+ * here R = max_shift (<= 0: 31), at most (min(width, height) - 1) / 2 (the whole map). */
+esrrf_status esrrf_drift_window(int width, int height, int max_shift, int* radius);
+/* d_frames: device, n_frames x height x width (uint16 if is_u16, else float32); ref_frame indexes
+ * into them.  shift_x, shift_y: host [n_frames].  d_ccm (device, may be NULL): [n_frames][2R+1][2R+1],
+ * C_f at lag (sy, sx) in row sy + R, column sx + R.  Returns when the shifts are on the host. */
+esrrf_status esrrf_estimate_drift(const void* d_frames, int is_u16, int n_frames, int width, int height,
+                                  int ref_frame, int max_shift, float* shift_x, float* shift_y,
+                                  float* d_ccm, void* stream);
+const char* esrrf_drift_last_error(void);
+
 /* ---- Differentiable eSRRF ---------------------------------------------------------------------
  * A fidelity loss of the 2-D FHT-path AVG reconstruction and its hand-written adjoint; there is
  * no counterpart in the reference's OpenCL path (the closest is the post-hoc error map of

@@ -389,6 +389,82 @@ def squirrel(sr, ref, magnification, fixed_sigma=None, crop=0, error_maps=False,
     return out
 
 
+def _device_frames(frames, device):
+    """[T][H][W] frames on cuda:device as (tensor, is_u16); uint16 travels as its int16 bit pattern."""
+    import torch
+
+    dev = f"cuda:{device}"
+    if isinstance(frames, torch.Tensor):
+        t = frames
+        if t.dtype in (torch.int16, torch.uint16):
+            return t.to(dev).view(torch.int16).contiguous(), 1
+        return t.to(device=dev, dtype=torch.float32).contiguous(), 0
+    a = np.ascontiguousarray(frames)
+    if a.dtype == np.uint16:
+        return torch.from_numpy(a.view(np.int16)).to(dev), 1
+    return torch.from_numpy(a.astype(np.float32, copy=False)).to(dev), 0
+
+
+def drift_window(width, height, max_shift=None) -> int:
+    """Lag radius R that estimate_drift searches (esrrf_drift_window)."""
+    R = ctypes.c_int()
+    _lib.check(None, lib().esrrf_drift_window(int(width), int(height), int(max_shift or 0), ctypes.byref(R)),
+               drift=True)
+    return R.value
+
+
+def estimate_drift(frames, ref_frame=0, max_shift=None, return_map=False, device=0):
+    """Drift of every frame relative to frames[ref_frame] (esrrf_estimate_drift; the restatement of
+    XYShiftCalculator.calculateShiftArray, XYShiftCalculator.java:26-48).
+
+    frames: [T][H][W] uint16 or float32, numpy or torch.  Returns (shift_x, shift_y) float32 [T], the
+    displacement of each frame's content relative to the reference frame (what
+    LiveSRRF_CL.loadDriftXYGPUbuffer takes); with return_map also the cross-correlation maps
+    [T][2R+1][2R+1] (lag (sy, sx) at [sy + R][sx + R])."""
+    import torch
+
+    t, is_u16 = _device_frames(frames, device)
+    if t.dim() == 2:
+        t = t[None]
+    n, H, W = t.shape
+    R = drift_window(W, H, max_shift)
+    sx = np.empty(n, np.float32)
+    sy = np.empty(n, np.float32)
+    ccm = torch.empty((n, 2 * R + 1, 2 * R + 1), dtype=torch.float32, device=t.device) if return_map else None
+    fp = ctypes.POINTER(ctypes.c_float)
+    with torch.cuda.device(device):
+        _lib.check(None, lib().esrrf_estimate_drift(
+            ctypes.c_void_p(t.data_ptr()), is_u16, n, W, H, int(ref_frame), int(max_shift or 0),
+            sx.ctypes.data_as(fp), sy.ctypes.data_as(fp),
+            ctypes.c_void_p(ccm.data_ptr()) if ccm is not None else None,
+            ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)), drift=True)
+    if return_map:
+        return sx, sy, ccm.cpu().numpy()
+    return sx, sy
+
+
+class XYShiftCalculator:
+    """Mirror of nanoj.liveSRRF.XYShiftCalculator (XYShiftCalculator.java:12-48) on the GPU.
+
+    calculateShiftArray(indexStart, nFrameForSRRF) takes the 1-based stack index of the block's
+    first frame (the reference frame, as ImageJ's getProcessor does) and fills shiftX and shiftY
+    for the nFrameForSRRF frames from there."""
+
+    def __init__(self, imp, prof=None, max_shift=None, device=0):
+        self.ims = imp
+        self.max_shift = max_shift
+        self.device = device
+        self.shiftX = None
+        self.shiftY = None
+
+    def calculateShiftArray(self, indexStart, nFrameForSRRF):
+        i0 = int(indexStart) - 1
+        if i0 < 0 or i0 + int(nFrameForSRRF) > len(self.ims):
+            raise EsrrfError("indexStart/nFrameForSRRF outside the stack")
+        self.shiftX, self.shiftY = estimate_drift(self.ims[i0:i0 + int(nFrameForSRRF)], 0, self.max_shift,
+                                                  device=self.device)
+
+
 class Adjoint:
     """Differentiable eSRRF (esrrf_adjoint_*, esrrf_loss_and_grad): a re-blur fidelity loss of the
     2-D FHT-path AVG reconstruction and its gradients w.r.t. radius, a real sensitivity, the

@@ -107,6 +107,10 @@ SIGNATURES.update({
                                   _c.POINTER(_c.c_size_t), _c.POINTER(_c.c_size_t), _f32p, _f32p,
                                   _f32p, _f32p, _f32p, _c.c_void_p]),
     "esrrf_squirrel_last_error": (_c.c_char_p, []),
+    "esrrf_drift_window": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.POINTER(_c.c_int)]),
+    "esrrf_estimate_drift": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_int,
+                                        _c.c_int, _f32p, _f32p, _c.c_void_p, _c.c_void_p]),
+    "esrrf_drift_last_error": (_c.c_char_p, []),
 })
 
 SIGNATURES.update({
@@ -146,11 +150,12 @@ def lib():
     return _LIB
 
 
-def check(handle, rc: int, sweep: bool = False, adjoint: bool = False, squirrel: bool = False) -> None:
+def check(handle, rc: int, sweep: bool = False, adjoint: bool = False, squirrel: bool = False,
+          drift: bool = False) -> None:
     if rc == 0:
         return
-    if squirrel:
-        msg = lib().esrrf_squirrel_last_error()
+    if squirrel or drift:
+        msg = (lib().esrrf_drift_last_error if drift else lib().esrrf_squirrel_last_error)()
         msg = msg.decode() if msg else ""
         raise EsrrfError(f"esrrf status {STATUS.get(rc, rc)}: {msg}")
     fn = lib().esrrf_adjoint_last_error if adjoint else (

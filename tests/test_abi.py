@@ -90,3 +90,12 @@ def test_no_cpu_fallback_without_library(monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", "/nonexistent/libesrrf.so")
     with pytest.raises(_lib.EsrrfError):
         _lib.lib()
+
+
+def test_drift_window_matches_oracle(esrrf_mod):
+    """esrrf_drift_window is host arithmetic only (no device work): same lag radius as the oracle."""
+    from oracle import drift_oracle as D
+    for w, h, ms in [(512, 512, None), (20, 17, None), (200, 180, 80), (200, 180, 500), (3, 3, None)]:
+        assert esrrf_mod.drift_window(w, h, ms) == D.window(w, h, ms)
+    with pytest.raises(esrrf_mod.EsrrfError):
+        esrrf_mod.drift_window(2, 64)
