@@ -1,8 +1,8 @@
 """GPU tests of esrrf_estimate_drift (restatement of XYShiftCalculator.calculateShiftArray,
 XYShiftCalculator.java:26-48) against the float64 oracle (oracle/drift_oracle.py).
 
-Maps: within 2e-6 of each map's largest magnitude (FP32 products summed per 32 x 32 tile, tiles in
-FP64).  Shifts: within 1e-3 px of the oracle's (the quadratic fit reads differences of neighbouring
+Maps: within 1e-6 of each map's largest magnitude (each 32-pixel row of products summed in FP32,
+rows in FP64; an emulation of that order gives 1.4e-7 on the first case).  Shifts: within 1e-3 px of the oracle's (the quadratic fit reads differences of neighbouring
 map values).  Cases: uint16 and float32 frames, sizes that are not multiples of the tiles, a window
 clamped by a small frame, a window of several lag tiles, a reference frame other than the first.
 The mirror class and the shifts' use by the engine (loadDriftXYGPUbuffer) are covered end to end."""
@@ -41,7 +41,7 @@ def test_drift_matches_oracle(esrrf_mod, w, h, T, ms, ref, u16):
     assert maps.shape == want.shape
     for t in range(T):
         err = np.abs(maps[t] - want[t]).max() / np.abs(want[t]).max()
-        assert err < 2e-6, (t, err)
+        assert err < 1e-6, (t, err)
     ox, oy = D.peaks(want, R)
     np.testing.assert_allclose(sx, ox, atol=1e-3)
     np.testing.assert_allclose(sy, oy, atol=1e-3)
@@ -76,9 +76,14 @@ def test_xyshiftcalculator_mirror(esrrf_mod):
 
 def test_estimated_drift_drives_the_engine(esrrf_mod, oracle_mod):
     """Shifts estimated on the GPU, loaded with loadDriftXYGPUbuffer, give the oracle's
-    drift-corrected block for the same shifts; and the correction re-aligns a drifting stack."""
+    drift-corrected block for the same shifts; and the correction re-aligns a drifting stack.
+
+    The stack carries camera noise (sigma 10 ADU): on noise-free spots over a flat background the
+    gradient directions in the flat regions come from rounding alone, and a 2e-7 perturbation of
+    the interpolated frames moves the VAR slice by 1e-2 of its range in the oracle itself."""
     f, shifts = stack(48, 40, 6, 5)
-    raw = np.round(f).astype(np.uint16)
+    f = f + np.random.default_rng(1).normal(0, 10, f.shape)
+    raw = np.round(np.clip(f, 0, None)).astype(np.uint16)
     sx, sy = esrrf_mod.estimate_drift(raw)
     eng = esrrf_mod.LiveSRRF_CL()
     eng.initialise(48, 40, 2, 1.5, 2, 6, 6)
