@@ -67,9 +67,25 @@ class LiveSRRF_CL:
                    doMPmapCorrection=False, doFHTinterpolation=True, calibTable3DSRRF=None,
                    axialOffset=0.0, pixelSize=0.1, kernel="fused", framesPerLaunch=0,
                    fhtScale="mean_preserving"):
-        """Same arguments as the reference.  ``calibTable3DSRRF`` replaces the .njt path: a
-        mapping with the table's keys (CALIB_KEYS); ``None`` means 2-D."""
+        """Same arguments as the reference.  ``calibTable3DSRRF``: the calibration table as a path
+        (read by calibration.load_calibration_table: ImageJ's text export of the table) or a
+        mapping with the table's keys (CALIB_KEYS); ``None`` means 2-D.  As the reference does
+        (LiveSRRF_CL.java:232-238), a table whose axial positions do not sum to zero replaces
+        axialOffset by their regression slope; axialOffset and dimensionRatioXYvsZ are kept on the
+        object."""
+        from . import calibration as _cal
+
         self.release()
+        if calibTable3DSRRF is not None and isinstance(calibTable3DSRRF, (str, bytes, os.PathLike)):
+            calibTable3DSRRF = _cal.load_calibration_table(calibTable3DSRRF)
+        if calibTable3DSRRF is not None:
+            geo = _cal.table_geometry(calibTable3DSRRF, width, height, magnification, axialOffset,
+                                      pixelSize)
+            axialOffset = geo["axialOffset"]
+            self.dimensionRatioXYvsZ = geo["dimensionRatioXYvsZ"]
+        else:
+            self.dimensionRatioXYvsZ = None
+        self.axialOffset = float(axialOffset)
         p = default_params()
         p.width, p.height = int(width), int(height)
         p.magnification = int(magnification)

@@ -146,3 +146,35 @@ def test_3d_drift_per_voxel_kernel(esrrf_mod, oracle_mod):
     got, _ = run(esrrf_mod, tile_planes(planes, roi), M, 1.5, 1, mp=False,
                  calib=calib(P, zeros, zeros, zeros, roi), drift=(dx, dy))
     assert_close(got, ref, "3d drift")
+
+
+def test_3d_calibration_table_from_file(esrrf_mod, tmp_path):
+    """The table read from its text export (the reference takes a path, LiveSRRF_CL.java:210-222)
+    gives the same reconstruction as the same table passed as a mapping, and initialise derives
+    the axial offset from the axial positions as the reference does."""
+    from esrrf import calibration as C
+    from esrrf import synth
+    P, h, w, n, M = 9, 48, 48, 4, 2
+    planes = synth.small_stack(7, n, h, w, planes=P).astype(np.float32)
+    roi = np.array([4, 0, 1, 2, 3, 5, 6, 7, 8], np.float64)
+    table = C.make_calibration_table(
+        shift_x=np.linspace(-0.3, 0.3, P), shift_y=np.linspace(0.2, -0.2, P), theta=np.linspace(-1, 1, P),
+        axial_positions=np.linspace(-400, 400, P) + 3.0, nominal_axial_positions=np.linspace(-400, 400, P),
+        roi_locations=roi, intensity_scaling=np.linspace(0.8, 1.2, P), background_level=90.0)
+    cam = tile_planes(planes * np.asarray(table["Intensity scaling"], np.float32)[None, :, None, None] + 90.0,
+                      table["ROI #"].astype(np.float32))
+    path = tmp_path / "beads - MFM_CalibrationTable.csv"
+    C.save_calibration_table(path, table)
+    a, _ = run(esrrf_mod, cam, M, 1.5, 1, mp=False, calib={k: table[k].astype(np.float32) for k in table})
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(cam.shape[-1], cam.shape[-2], M, 1.5, 1, n, n, doMPmapCorrection=False,
+                   doFHTinterpolation=False, calibTable3DSRRF=str(path), axialOffset=250.0, pixelSize=0.1)
+    try:
+        eng.resetFramePosition()
+        assert not eng.calculateSRRF(cam)
+        b = eng.readSRRFbuffer().copy()
+        assert eng.axialOffset == float(np.float32(C.axial_offset(table["Axial positions"])))
+        assert eng.nPlanes == P
+    finally:
+        eng.release()
+    np.testing.assert_array_equal(a, b)
