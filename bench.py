@@ -471,6 +471,46 @@ def run_sweep(args, world, rank, local):
             img = flat[base:base + 4 * P].reshape(4, h * M, w * M)
             Q.squirrel(img[0], img[3], M)
         sq_cpu_per_image = (time.perf_counter() - t0) / len(SWEEP_MAGS)
+
+    # FRC resolution of every combination and cumulant (264 pairs): the [0,100) and [101,200)
+    # blocks stand in for the odd/even reconstructions of the reference's FRC mode (same sizes)
+    def frc_all():
+        fp = ctypes.POINTER(ctypes.c_float)
+        n_pairs, nR, nS, nB = 0, len(SWEEP_RADII), len(SWEEP_SENS), len(SWEEP_BLOCKS)
+        for mi, M in enumerate(SWEEP_MAGS):
+            P = h * M * w * M
+            ao, bo = [], []
+            for ri in range(nR):
+                base = sw.offsets[mi * nR + ri]
+                for si in range(nS):
+                    for c in range(3):
+                        ao.append(base + (si * nB + 3) * 4 * P + c * P)
+                        bo.append(base + (si * nB + 2) * 4 * P + c * P)
+            n = len(ao)
+            fire = np.empty(n, np.float32)
+            p = esrrf._lib.EsrrfFrcParams(w * M, h * M, 1.0 / M,
+                                          ctypes.c_void_p(torch.cuda.current_stream(local).cuda_stream))
+            esrrf._lib.check(None, L.esrrf_frc(ctypes.byref(p), n, ctypes.c_void_p(d_out.data_ptr()),
+                                               (ctypes.c_size_t * n)(*ao), (ctypes.c_size_t * n)(*bo),
+                                               fire.ctypes.data_as(fp), None), frc=True)
+            n_pairs += n
+        return n_pairs
+
+    frc_pairs, frc_s, frc_cpu_per_pair = 0, None, None
+    if rank == 0:
+        frc_all()  # warm-up
+        t0 = time.perf_counter()
+        frc_pairs = frc_all()
+        frc_s = time.perf_counter() - t0
+        from oracle import frc_oracle as FO
+        t0 = time.perf_counter()
+        for mi, M in enumerate(SWEEP_MAGS):
+            P = h * M * w * M
+            base = sw.offsets[mi * len(SWEEP_RADII) + 4]
+            a = flat[base + 3 * 4 * P:base + 3 * 4 * P + P].reshape(h * M, w * M)
+            b = flat[base + 2 * 4 * P:base + 2 * 4 * P + P].reshape(h * M, w * M)
+            FO.fire(a, b)
+        frc_cpu_per_pair = (time.perf_counter() - t0) / len(SWEEP_MAGS)
     sw.release()
 
     def single_combo_loop(kernel, subset=None):
@@ -522,6 +562,11 @@ def run_sweep(args, world, rank, local):
                      "cpu_port_seconds_per_image": sq_cpu_per_image,
                      "cpu_note": "float64 numpy restatement, one image of each magnification; the "
                                  "reference's own ImageJ/commons-math path needs a JVM"},
+        "frc": {"pairs": frc_pairs, "seconds": frc_s, "pairs_per_s": frc_pairs / frc_s if frc_s else None,
+                "what": "FIRE resolution (1/7 threshold) of AVG, VAR and TAC2 of every combination, "
+                        "blocks [0,100) vs [101,200) standing in for the odd/even halves",
+                "cpu_port_seconds_per_pair": frc_cpu_per_pair,
+                "cpu_note": "float64 numpy restatement (numpy FFT, one thread), one pair per magnification"},
     }
     print(json.dumps(line))
 

@@ -249,6 +249,27 @@ esrrf_status esrrf_estimate_drift(const void* d_frames, int is_u16, int n_frames
                                   float* d_ccm, void* stream);
 const char* esrrf_drift_last_error(void);
 
+/* ---- Fourier ring correlation ------------------------------------------------------------------
+ * Replaces the FRC resolution of the parameter sweep (gui/ParametersSweep_.java:403-447:
+ * FRC.calculateFireNumber(odd, even, FIXED_1_OVER_7) x the reconstruction's pixel size) for a batch
+ * of image pairs.  NanoJ-Core's FRC is not in the reference tree; the method restated: each image
+ * minus its mean times a Tukey window (tapers over the outer eighth of each axis), zero-padded to
+ * N x N (N the next power of two >= max(width, height, 32)); FRC(r) = sum Re(F1 conj F2) /
+ * sqrt(sum |F1|^2 sum |F2|^2) over rings r = round(|(u, v)|) = 0 .. N/2; FIRE = N / q x pixel_size,
+ * q the first crossing of 1/7 (linear between rings, r >= 2); NaN if FRC(1) < 1/7 or no crossing. */
+typedef struct {
+    int width, height;  /* image size in pixels */
+    float pixel_size;   /* the resolution's unit per pixel (1: pixels) */
+    void* stream;       /* cudaStream_t (NULL: the default stream) */
+} esrrf_frc_params;
+
+esrrf_status esrrf_frc_size(int width, int height, int* padded_size, int* n_rings);
+/* d_base: device floats; pair i is the [height][width] images at d_base + a_offsets[i] and
+ * d_base + b_offsets[i] (host arrays).  fire: host [n].  curves (host, may be NULL): [n][n_rings]. */
+esrrf_status esrrf_frc(const esrrf_frc_params* p, int n, const float* d_base, const size_t* a_offsets,
+                       const size_t* b_offsets, float* fire, float* curves);
+const char* esrrf_frc_last_error(void);
+
 /* ---- Differentiable eSRRF ---------------------------------------------------------------------
  * A fidelity loss of the 2-D FHT-path AVG reconstruction and its hand-written adjoint; there is
  * no counterpart in the reference's OpenCL path (the closest is the post-hoc error map of

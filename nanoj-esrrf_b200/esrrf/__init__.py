@@ -405,6 +405,78 @@ def squirrel(sr, ref, magnification, fixed_sigma=None, crop=0, error_maps=False,
     return out
 
 
+def frc_size(width, height):
+    """(padded size N, number of rings N/2 + 1) of esrrf_frc for images of this size."""
+    N, R = ctypes.c_int(), ctypes.c_int()
+    _lib.check(None, lib().esrrf_frc_size(int(width), int(height), ctypes.byref(N), ctypes.byref(R)),
+               frc=True)
+    return N.value, R.value
+
+
+def frc(a, b, pixel_size=1.0, curves=False, device=0):
+    """FIRE resolution (esrrf_frc) of image pairs: a, b [n][H][W] or [H][W], numpy or torch CUDA.
+    Returns float32 [n] in pixel_size units (NaN: no 1/7 crossing), with curves also the FRC
+    curves [n][N/2 + 1]."""
+    import torch
+
+    from ._lib import EsrrfFrcParams
+
+    dev = f"cuda:{device}"
+    at = torch.as_tensor(a, dtype=torch.float32, device=dev).contiguous()
+    bt = torch.as_tensor(b, dtype=torch.float32, device=dev).contiguous()
+    if at.dim() == 2:
+        at, bt = at[None], bt[None]
+    if at.shape != bt.shape:
+        raise EsrrfError("frc: the two image stacks differ in shape")
+    n, H, W = at.shape
+    _, R = frc_size(W, H)
+    both = torch.cat([at.reshape(-1), bt.reshape(-1)])
+    P = H * W
+    ao = (ctypes.c_size_t * n)(*[i * P for i in range(n)])
+    bo = (ctypes.c_size_t * n)(*[(n + i) * P for i in range(n)])
+    fire = np.empty(n, np.float32)
+    cv = np.empty((n, R), np.float32) if curves else None
+    fp = ctypes.POINTER(ctypes.c_float)
+    p = EsrrfFrcParams(W, H, float(pixel_size), ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream))
+    with torch.cuda.device(device):
+        _lib.check(None, lib().esrrf_frc(ctypes.byref(p), n, ctypes.c_void_p(both.data_ptr()), ao, bo,
+                                         fire.ctypes.data_as(fp), cv.ctypes.data_as(fp) if cv is not None else None),
+                   frc=True)
+    return (fire, cv) if curves else fire
+
+
+def sweep_frc(stack, magnifications, radii, sensitivities, n_frames, pixel_size=1.0, int_weighting=True,
+              device=0):
+    """The sweep's FRC mode (gui/ParametersSweep_.java:403-447): every (M, radius, S) reconstructed
+    from the odd frames (1, 3, 5, ... in ImageJ's 1-based numbering) and from the even frames of the
+    first 2 n_frames, and the FIRE resolution of each AVG, VAR and TAC2 pair in units of
+    pixel_size / M (the raw pixel size divided by the magnification, as the reference's output
+    calibration).  Returns ({(M, radius, S): {"AVG"|"VAR"|"TAC2": resolution}}, odd results, even
+    results); like the reference, the even-frame reconstructions are the sweep's images."""
+    a = np.asarray(stack)
+    if a.shape[0] < 2 * int(n_frames):
+        raise EsrrfError(f"FRC mode needs {2 * int(n_frames)} frames, the stack has {a.shape[0]}")
+    halves = []
+    for start in (0, 1):
+        sub = np.ascontiguousarray(a[start:2 * int(n_frames):2])
+        sw = Sweep(a.shape[-1], a.shape[-2], sub.shape[0], magnifications, radii, sensitivities,
+                   [(0, sub.shape[0])], int_weighting=int_weighting, device=device)
+        try:
+            halves.append({k[:3]: v.copy() for k, v in sw.run(sub).items()})
+        finally:
+            sw.release()
+    odd, even = halves
+    out = {}
+    for M in sorted({k[0] for k in odd}):
+        keys = [k for k in odd if k[0] == M]
+        A = np.stack([odd[k][c] for k in keys for c in range(3)])
+        B = np.stack([even[k][c] for k in keys for c in range(3)])
+        res = frc(A, B, pixel_size=float(pixel_size) / M, device=device)
+        for i, k in enumerate(keys):
+            out[k] = {name: float(res[3 * i + c]) for c, name in enumerate(("AVG", "VAR", "TAC2"))}
+    return out, odd, even
+
+
 def _device_frames(frames, device):
     """[T][H][W] frames on cuda:device as (tensor, is_u16); uint16 travels as its int16 bit pattern."""
     import torch

@@ -102,6 +102,13 @@ class EsrrfSquirrelParams(ctypes.Structure):
     ]
 
 
+class EsrrfFrcParams(ctypes.Structure):
+    """esrrf_frc_params (include/esrrf.h)."""
+
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("pixel_size", ctypes.c_float),
+                ("stream", ctypes.c_void_p)]
+
+
 SIGNATURES.update({
     "esrrf_squirrel": (_c.c_int, [_c.POINTER(EsrrfSquirrelParams), _c.c_int, _c.c_void_p,
                                   _c.POINTER(_c.c_size_t), _c.POINTER(_c.c_size_t), _f32p, _f32p,
@@ -111,6 +118,10 @@ SIGNATURES.update({
     "esrrf_estimate_drift": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_int,
                                         _c.c_int, _f32p, _f32p, _c.c_void_p, _c.c_void_p]),
     "esrrf_drift_last_error": (_c.c_char_p, []),
+    "esrrf_frc_size": (_c.c_int, [_c.c_int, _c.c_int, _c.POINTER(_c.c_int), _c.POINTER(_c.c_int)]),
+    "esrrf_frc": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.POINTER(_c.c_size_t),
+                             _c.POINTER(_c.c_size_t), _f32p, _f32p]),
+    "esrrf_frc_last_error": (_c.c_char_p, []),
 })
 
 SIGNATURES.update({
@@ -151,11 +162,12 @@ def lib():
 
 
 def check(handle, rc: int, sweep: bool = False, adjoint: bool = False, squirrel: bool = False,
-          drift: bool = False) -> None:
+          drift: bool = False, frc: bool = False) -> None:
     if rc == 0:
         return
-    if squirrel or drift:
-        msg = (lib().esrrf_drift_last_error if drift else lib().esrrf_squirrel_last_error)()
+    if squirrel or drift or frc:
+        msg = (lib().esrrf_drift_last_error if drift else
+               lib().esrrf_frc_last_error if frc else lib().esrrf_squirrel_last_error)()
         msg = msg.decode() if msg else ""
         raise EsrrfError(f"esrrf status {STATUS.get(rc, rc)}: {msg}")
     fn = lib().esrrf_adjoint_last_error if adjoint else (
