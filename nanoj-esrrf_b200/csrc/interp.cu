@@ -76,13 +76,14 @@ __global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u
         const int y = base + warp * 4 + r;
         if (y >= N) break;
         const long rowoff = (long)srcy[y] * w;
-        double acc = 0.0;
+        double acc = 0.0, tot = 0.0;
+        // unrolled: several independent loads in flight per lane (the loop is latency bound)
+#pragma unroll 8
         for (int x = lane; x < N; x += 32) {
             const float v = load_raw(frame, is_u16, rowoff + srcx[x]);
             acc += (x & 1) ? -(double)v : (double)v;
+            tot += (double)v;
         }
-        double tot = 0.0;
-        for (int x = lane; x < N; x += 32) tot += (double)load_raw(frame, is_u16, rowoff + srcx[x]);
         for (int o = 16; o > 0; o >>= 1) {
             acc += __shfl_xor_sync(0xffffffffu, acc, o);
             tot += __shfl_xor_sync(0xffffffffu, tot, o);
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u
     double acc = 0.0;
     if (x < N) {
         const int sx = srcx[x];
+#pragma unroll 8
         for (int y = warp; y < N; y += 8) {
             const float v = load_raw(frame, is_u16, (long)srcy[y] * w + sx);
             acc += (y & 1) ? -(double)v : (double)v;
@@ -119,8 +121,11 @@ __global__ void __launch_bounds__(256) rank1_vectors_kernel(
     const float* __restrict__ alt, const float* __restrict__ dyT, const float* __restrict__ dxT,
     const float* __restrict__ cx, const float* __restrict__ ux, const float* __restrict__ cy,
     int N, int HM, int WM, float s_axis, float s, float* __restrict__ vec) {
+    // grid ((HM + WM + 31) / 32, frames): 32 outputs per CTA (lane = output), the 8 warps each
+    // summing every 8th term, partial sums combined in warp order
     extern __shared__ float wsh[];  // [2N]: wy then wx
     __shared__ float qred[8], mred[8];
+    __shared__ float part[2][8][33];
     const int f = blockIdx.y;
     const float* a = alt + (long)f * (3 * N + 1);
     float qp = 0.f, mp = 0.f;  // q = sum_y (-1)^y wy[y]; frame sum from the row sums
@@ -146,29 +151,46 @@ __global__ void __launch_bounds__(256) rank1_vectors_kernel(
         q += qred[i];
         msum += mred[i];
     }
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int e = blockIdx.x * 32 + lane;
     float* v = vec + (long)f * (2 * HM + 2 * WM + 1);
     // The dense passes interpolate X - c (c = frame mean) and add c s N^2 back: the map sends a
     // constant to (s N^2) times it, and the alternating sums of a constant vanish (N even), so
     // this only shrinks the GEMM summands.
-    if (e == 0) v[2 * HM + 2 * WM] = msum / ((float)N * (float)N);
+    if (blockIdx.x == 0 && threadIdx.x == 0) v[2 * HM + 2 * WM] = msum / ((float)N * (float)N);
+    float d0 = 0.f, d1 = 0.f;
     if (e < HM) {
-        float d0 = 0.f, d1 = 0.f;
-        for (int y = 0; y < N; ++y) {
+#pragma unroll 4
+        for (int y = warp; y < N; y += 8) {
             const float dv = dyT[(long)y * HM + e];
             d0 = fmaf(dv, wsh[y], d0);
             d1 = fmaf(dv, wsh[(N - y) & (N - 1)], d1);
         }
-        v[e] = s_axis * d0;
-        v[HM + e] = s_axis * d1 + s * q * cy[e];
     } else if (e < HM + WM) {
         const int n = e - HM;
-        float d0 = 0.f, d1 = 0.f;
-        for (int x = 0; x < N; ++x) {
+#pragma unroll 4
+        for (int x = warp; x < N; x += 8) {
             const float dv = dxT[(long)x * WM + n];
             d0 = fmaf(dv, wsh[N + x], d0);
             d1 = fmaf(dv, wsh[N + ((N - x) & (N - 1))], d1);
         }
+    }
+    part[0][warp][lane] = d0;
+    part[1][warp][lane] = d1;
+    __syncthreads();
+    if (warp != 0) return;
+    d0 = 0.f;
+    d1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        d0 += part[0][k][lane];
+        d1 += part[1][k][lane];
+    }
+    if (e < HM) {
+        v[e] = s_axis * d0;
+        v[HM + e] = s_axis * d1 + s * q * cy[e];
+    } else if (e < HM + WM) {
+        const int n = e - HM;
         v[2 * HM + n] = s_axis * d0 + s * q * cx[n];
         v[2 * HM + WM + n] = s_axis * d1 + s * q * (cx[n] + ux[n]);
     }
@@ -567,7 +589,7 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
     alt_sums_kernel<<<dim3((N + 31) / 32, F), 256, 0, stream>>>(raw, is_u16 ? 1 : 0, p.w, p.h, N,
                                                                p.srcx, p.srcy, sc.alt);
     {
-        dim3 grid((p.HM + p.WM + 255) / 256, F);
+        dim3 grid((p.HM + p.WM + 31) / 32, F);
         rank1_vectors_kernel<<<grid, 256, sizeof(float) * 2 * N, stream>>>(
             sc.alt, p.dyT, p.dxT, p.cx, p.ux, p.cy, N, p.HM, p.WM, (float)p.s_axis, (float)p.s,
             sc.vec);
