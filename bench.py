@@ -291,12 +291,15 @@ def run_ours(args, world, rank, local):
     h_out = torch.empty((n_blocks, 4, HM, WM), dtype=torch.float32).pin_memory()
 
     def step_e2e():
+        # each block's read-back is queued (esrrf_read_srrf_async) and overlaps the next block's
+        # upload and kernels; finishQueue waits for all of it
         base = h_stack.data_ptr()
         for b in range(n_blocks):
             esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
             esrrf._lib.check(H, L.esrrf_calculate_srrf_u16(
                 H, ctypes.c_void_p(base + b * nf * frame_bytes), nf))
-            esrrf._lib.check(H, L.esrrf_read_srrf(H, ctypes.c_void_p(h_out[b].data_ptr())))
+            esrrf._lib.check(H, L.esrrf_read_srrf_async(H, ctypes.c_void_p(h_out[b].data_ptr())))
+        esrrf._lib.check(H, L.esrrf_finish_queue(H))
 
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):

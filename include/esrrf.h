@@ -136,6 +136,12 @@ esrrf_status esrrf_calculate_srrf_f32_device(esrrf_handle* h, const float* d_fra
 esrrf_status esrrf_read_srrf(esrrf_handle* h, float* out);
 /* Same into device memory. */
 esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* d_out);
+/* Queued form of esrrf_read_srrf (no reference counterpart; the reference reads synchronously):
+ * finalises the block into one of two device output slots and queues the copy to host `out` on
+ * its own stream, returning at once, so that the next block's frames (reset + push) overlap the
+ * copy.  `out` must stay valid (and should be pinned for the copy to overlap) until
+ * esrrf_finish_queue returns; a third read waits for the first one's copy. */
+esrrf_status esrrf_read_srrf_async(esrrf_handle* h, float* out);
 
 /* Output geometry (public fields widthS/heightS/nPlanes/nPlanesM, LiveSRRF_CL.java:41-45). */
 esrrf_status esrrf_output_shape(const esrrf_handle* h, int* width_m, int* height_m,
@@ -145,7 +151,10 @@ esrrf_status esrrf_output_shape(const esrrf_handle* h, int* width_m, int* height
  * frame of the last push ([2 or 3][planes][h'][w'] float, h'/w' as in the reference). */
 esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len);
 
-/* Replaces finishQueue (LiveSRRF_CL.java:1009-1015): waits for the handle's stream. */
+/* Replaces finishQueue (LiveSRRF_CL.java:1009-1015): waits for every queued kernel, input copy
+ * and read-back of the handle; ESRRF_ERR_TIMEOUT if a bounded tensor-core wait gave up.  The
+ * pushes (esrrf_calculate_srrf_*) from host memory return once their frames are copied; the
+ * kernels of the last frames may still run until a read or this call. */
 esrrf_status esrrf_finish_queue(esrrf_handle* h);
 
 /* Thread-safe cancellation (replaces the IJ.escapePressed() polling, LiveSRRF_CL.java:731-734). */

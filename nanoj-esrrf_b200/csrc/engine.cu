@@ -104,6 +104,7 @@ esrrf_status esrrf_handle::init(const esrrf_params& params) {
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&read_stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&ev_a));
     CK(cudaEventCreate(&ev_b));
     CK(cudaEventCreate(&ev_c));
@@ -111,6 +112,8 @@ esrrf_status esrrf_handle::init(const esrrf_params& params) {
         CK(cudaEventCreateWithFlags(&ev_host_free[b], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_copied[b], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ev_dev_free[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_fin[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_read_done[b], cudaEventDisableTiming));
     }
     drift_x.assign(p.n_frame_for_srrf, 0.f);
     drift_y.assign(p.n_frame_for_srrf, 0.f);
@@ -233,6 +236,7 @@ void esrrf_handle::release() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     if (copy_stream) cudaStreamSynchronize(copy_stream);
+    if (read_stream) cudaStreamSynchronize(read_stream);
     interp_plan_destroy(plan);
     fht_fused_tables_free(tables);
     cudaFree(scratch.rowT);
@@ -249,10 +253,16 @@ void esrrf_handle::release() {
         if (ev_host_free[b]) cudaEventDestroy(ev_host_free[b]);
         if (ev_copied[b]) cudaEventDestroy(ev_copied[b]);
         if (ev_dev_free[b]) cudaEventDestroy(ev_dev_free[b]);
+        if (ev_fin[b]) cudaEventDestroy(ev_fin[b]);
+        if (ev_read_done[b]) cudaEventDestroy(ev_read_done[b]);
+        ev_fin[b] = ev_read_done[b] = nullptr;
+        read_pending[b] = false;
     }
     cudaFree(st.acc);
     cudaFree(st.prev);
     cudaFree(d_out);
+    cudaFree(d_out2);
+    d_out2 = nullptr;
     rgc3d_tables_free(t3d);
     cudaFree(d_u3);
     for (float* b : {d_fraw, d_planes, d_gz, d_gxi, d_gyi, d_gzi, d_mpmap, mfm.coeff, mfm.cos_t,
@@ -267,7 +277,8 @@ void esrrf_handle::release() {
     if (ev_c) cudaEventDestroy(ev_c);
     if (stream && own_stream) cudaStreamDestroy(stream);
     if (copy_stream) cudaStreamDestroy(copy_stream);
-    stream = copy_stream = nullptr;
+    if (read_stream) cudaStreamDestroy(read_stream);
+    stream = copy_stream = read_stream = nullptr;
 }
 
 esrrf_status esrrf_handle::reset_block() {
@@ -467,21 +478,20 @@ esrrf_status esrrf_handle::calculate(const void* frames, bool is_u16, int n, boo
     const bool pinned = cudaPointerGetAttributes(&attr, frames) == cudaSuccess &&
                         attr.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    int chunk = 0;
-    for (int s = 0; s < n; s += F, ++chunk) {
+    for (int s = 0; s < n; s += F, ++chunk_seq) {
         if (cancel.exchange(0)) {
             cudaStreamSynchronize(copy_stream);
             cudaStreamSynchronize(stream);
             return ESRRF_CANCELLED;
         }
-        const int b = chunk & 1;
+        const int b = (int)(chunk_seq & 1);
         const int F_now = std::min(F, n - s);
         const char* src = (const char*)frames + fbytes * s;
-        if (chunk >= 2) CK(cudaStreamWaitEvent(copy_stream, ev_dev_free[b], 0));
+        if (chunk_seq >= 2) CK(cudaStreamWaitEvent(copy_stream, ev_dev_free[b], 0));
         if (pinned) {
             CK(cudaMemcpyAsync(d_raw[b], src, fbytes * F_now, cudaMemcpyHostToDevice, copy_stream));
         } else {
-            if (chunk >= 2) CK(cudaEventSynchronize(ev_host_free[b]));
+            if (chunk_seq >= 2) CK(cudaEventSynchronize(ev_host_free[b]));
             memcpy(h_stage[b], src, fbytes * F_now);
             CK(cudaMemcpyAsync(d_raw[b], h_stage[b], fbytes * F_now, cudaMemcpyHostToDevice, copy_stream));
             CK(cudaEventRecord(ev_host_free[b], copy_stream));
@@ -492,8 +502,14 @@ esrrf_status esrrf_handle::calculate(const void* frames, bool is_u16, int n, boo
         if (r != ESRRF_OK) return r;
         CK(cudaEventRecord(ev_dev_free[b], stream));
     }
-    CK(cudaStreamSynchronize(stream));
-    if (timing) collect_timing();
+    // The caller's frames are consumed once their copies are done; the last chunks' kernels may
+    // still run (reads, resets and drift uploads queue behind them on the same stream).
+    if (timing) {
+        CK(cudaStreamSynchronize(stream));
+        collect_timing();
+    } else {
+        CK(cudaStreamSynchronize(copy_stream));
+    }
     return ESRRF_OK;
 }
 
@@ -501,6 +517,8 @@ esrrf_status esrrf_handle::read(float* out, bool on_device) {
     esrrf_handle* h = this;
     CK(cudaSetDevice(device));
     if (frame_in_block == 0) return fail(ESRRF_ERR_STATE, "no frames accumulated in this block");
+    // slot 0 may still be the source of a queued read-back
+    if (read_pending[0]) CK(cudaStreamWaitEvent(stream, ev_read_done[0], 0));
     // kernelCalculateVar + NaN->0 (LiveSRRF_CL.java:749-794) on the block accumulated so far.
     CK(finalize_block(st, p.n_frame_for_srrf, mode == Mode::kBIC ? 1 : 0, d_out, stream));
     // MP map correction runs on the bicubic and 3-D paths only (LiveSRRF_CL.java:762-770)
@@ -511,6 +529,43 @@ esrrf_status esrrf_handle::read(float* out, bool on_device) {
                        stream));
     bool tc_failed = false;
     CK(interp_tc_check(plan, stream, &tc_failed));  // synchronises the stream
+    if (tc_failed)
+        return fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
+    return ESRRF_OK;
+}
+
+// The block's cumulants into one of two output slots and a device-to-host copy of it queued on
+// read_stream; returns at once.  The next block's frames can be pushed while the copy runs.
+esrrf_status esrrf_handle::read_async(float* out) {
+    esrrf_handle* h = this;
+    CK(cudaSetDevice(device));
+    if (frame_in_block == 0) return fail(ESRRF_ERR_STATE, "no frames accumulated in this block");
+    const size_t bytes = sizeof(float) * 4 * (size_t)st.pixels;
+    if (!d_out2) CK(cudaMalloc(&d_out2, bytes));
+    const int s = read_slot;
+    read_slot ^= 1;
+    float* dst = s ? d_out2 : d_out;
+    if (read_pending[s]) CK(cudaStreamWaitEvent(stream, ev_read_done[s], 0));
+    CK(finalize_block(st, p.n_frame_for_srrf, mode == Mode::kBIC ? 1 : 0, dst, stream));
+    if (p.mp_correction && mode != Mode::kFHT)
+        CK(mp_correct(dst, ws, hs, P, p.magnification, mode == Mode::k3D ? 1 : 0, d_mpmap, stream));
+    CK(cudaEventRecord(ev_fin[s], stream));
+    CK(cudaStreamWaitEvent(read_stream, ev_fin[s], 0));
+    CK(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, read_stream));
+    CK(cudaEventRecord(ev_read_done[s], read_stream));
+    read_pending[s] = true;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_handle::drain() {
+    esrrf_handle* h = this;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamSynchronize(copy_stream));
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaStreamSynchronize(read_stream));
+    read_pending[0] = read_pending[1] = false;
+    bool tc_failed = false;
+    CK(interp_tc_check(plan, stream, &tc_failed));
     if (tc_failed)
         return fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
     return ESRRF_OK;
@@ -690,11 +745,12 @@ esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len) {
 
 esrrf_status esrrf_finish_queue(esrrf_handle* h) {
     if (!h) return ESRRF_ERR_INVALID;
-    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess) {
-        cudaGetLastError();
-        return h->fail(ESRRF_ERR_CUDA, "stream synchronisation failed");
-    }
-    return ESRRF_OK;
+    return h->drain();
+}
+
+esrrf_status esrrf_read_srrf_async(esrrf_handle* h, float* out) {
+    if (!h || !out) return ESRRF_ERR_INVALID;
+    return h->read_async(out);
 }
 
 esrrf_status esrrf_request_cancel(esrrf_handle* h) {

@@ -54,9 +54,20 @@ struct esrrf_handle {
     cudaEvent_t ev_copied[2] = {nullptr, nullptr};
     cudaEvent_t ev_dev_free[2] = {nullptr, nullptr};
 
+    long chunk_seq = 0;  // host chunks staged so far: a staging buffer is reused only after the
+                         // kernels of its previous chunk (possibly from an earlier call) are done
+
     // block accumulators and output
     esrrf::BlockState st;
     float* d_out = nullptr;
+    // queued read-back (esrrf_read_srrf_async): two output slots, slot 0 = d_out; the
+    // device-to-host copies run on read_stream and overlap the next block's kernels
+    float* d_out2 = nullptr;
+    cudaStream_t read_stream = nullptr;
+    cudaEvent_t ev_fin[2] = {nullptr, nullptr};
+    cudaEvent_t ev_read_done[2] = {nullptr, nullptr};
+    bool read_pending[2] = {false, false};
+    int read_slot = 0;
     int frame_in_block = 0;     // nCurrentFrame[0] of the reference
     std::vector<float> drift_x, drift_y;
 
@@ -85,6 +96,8 @@ struct esrrf_handle {
     esrrf_status process_chunk_bic3d(const void* src, bool is_u16, int F_now,
                                      const std::vector<float>& sh);
     esrrf_status read(float* out, bool on_device);
+    esrrf_status read_async(float* host_out);
+    esrrf_status drain();  // every queued kernel and copy done, tensor-core wait flag checked
     esrrf_status fail(esrrf_status s, const std::string& msg);
     esrrf_status fail_cuda(cudaError_t e, const char* what, int line);
 };

@@ -167,6 +167,18 @@ class LiveSRRF_CL:
         self.imsSRRF = out
         return out
 
+    def readSRRFbufferAsync(self, out):
+        """Queued read-back of the block into `out` (a C-contiguous float32 array of
+        [4 x planesM][heightM][widthM], pinned for overlap), valid once finishQueue() returns;
+        the next block can be pushed meanwhile (esrrf_read_srrf_async)."""
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float32 and out.flags.c_contiguous):
+            raise EsrrfError("readSRRFbufferAsync needs a C-contiguous float32 array")
+        wm, hm, pm = self._shape
+        if out.size != 4 * pm * hm * wm:
+            raise EsrrfError(f"output holds {out.size} floats, the block {4 * pm * hm * wm}")
+        _lib.check(self._h, lib().esrrf_read_srrf_async(self._h, out.ctypes.data_as(ctypes.c_void_p)))
+        self._async_out = out
+
     # -- LiveSRRF_CL.readGradientBuffers (LiveSRRF_CL.java:797-879)
     def readGradientBuffers(self):
         wm, hm, pm = self._shape
