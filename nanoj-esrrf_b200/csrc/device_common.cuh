@@ -61,6 +61,42 @@ __device__ __forceinline__ float sample2d(const float* __restrict__ a, int w, in
     return lower + yf * (upper - lower);
 }
 
+// sample2d at one position (x, y) of four planes a + plane[k] * pl: the support, the branch and the
+// 4 x 4 cubic weights are shared, each plane keeps sample2d's own accumulation order.
+__device__ __forceinline__ void sample2d_x4(const float* __restrict__ a, long pl, const int (&plane)[4],
+                                            int w, int h, float x, float y, float (&out)[4]) {
+    const int u0 = (int)floorf(x);
+    const int v0 = (int)floorf(y);
+    if (u0 > 0 && u0 < w - 2 && v0 > 0 && v0 < h - 2) {
+        int us[4];
+        float cx[4];
+#pragma unroll
+        for (int i = 0; i <= 3; i++) {
+            us[i] = min(max(u0 - 1 + i, 0), w - 1);
+            cx[i] = cubic(x - (float)us[i]);
+        }
+        float q[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int j = 0; j <= 3; j++) {
+            const int v = min(max(v0 - 1 + j, 0), h - 1);
+            const float cy = cubic(y - (float)v);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const float* r = a + plane[k] * pl + (long)v * w;
+                float p = 0.0f;
+#pragma unroll
+                for (int i = 0; i <= 3; i++) p = p + __ldg(r + us[i]) * cx[i];
+                q[k] = q[k] + p * cy;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) out[k] = q[k];
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] = sample2d(a + plane[k] * pl, w, h, x, y);
+}
+
 __device__ __forceinline__ float load_px(const void* raw, int is_u16, long idx) {
     return is_u16 ? (float)__ldg((const unsigned short*)raw + idx) : __ldg((const float*)raw + idx);
 }

@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(256) rgc3d_tab_kernel(Rgc3dTabArgs a) {
 // all of them: one gradient load per tap, the dz-free products shared, a (dz, w, w/d) triple per
 // z-phase.  Otherwise as rgc3d_tab_kernel.
 template <int MZ>
-__global__ void __launch_bounds__(256) rgc3d_zb_kernel(Rgc3dTabArgs a) {
+__global__ void __launch_bounds__(256, 2) rgc3d_zb_kernel(Rgc3dTabArgs a) {
     extern __shared__ float4 sz4[];  // [n][es] entries
     constexpr int M = MZ, M2 = MZ * MZ;
     const int es = a.tab.zes;
@@ -384,6 +384,15 @@ __global__ void __launch_bounds__(256) rgc3d_zb_kernel(Rgc3dTabArgs a) {
         z01[p] = zc - (float)(z0[p] + 0.5f);
         s0[p] = s1[p] = s2[p] = s3[p] = 0.0;
     }
+    // the z-phases' base planes z0 take at most two consecutive values, so their z-cubics read
+    // the four planes zlo - 1 .. zlo + 2 (clamped): phase p uses S[d], S[d + 1], S[d + 2] twice,
+    // d = z0[p] - zlo
+    int zlo = z0[0];
+#pragma unroll
+    for (int p = 1; p < MZ; ++p) zlo = min(zlo, z0[p]);
+    int splane[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) splane[k] = min(max(zlo - 1 + k, 0), a.P - 1);
     for (int f = 0; f < a.F; ++f) {
         const float4* U = U0 + f * fstride;
         float cg[MZ];
@@ -408,14 +417,16 @@ __global__ void __launch_bounds__(256) rgc3d_zb_kernel(Rgc3dTabArgs a) {
             }
         }
         const float* ap = a.apx + (long)f * a.P * pl;
+        float S[4];
+        dev::sample2d_x4(ap, pl, splane, a.w, a.h, pxf, pyf, S);
 #pragma unroll
         for (int p = 0; p < MZ; ++p) {
             const float c = cglh_power(cg[p] / wsum[p], a.sens);
-            const int zb = z0[p];
-            const float v_1 = sample2d(ap + (long)max(zb - 1, 0) * pl, a.w, a.h, pxf, pyf);
-            const float v0 = sample2d(ap + (long)zb * pl, a.w, a.h, pxf, pyf);
-            const float v1 = sample2d(ap + (long)(zb + 1) * pl, a.w, a.h, pxf, pyf);
-            const float v2 = sample2d(ap + (long)min(zb + 1, a.P - 1) * pl, a.w, a.h, pxf, pyf);
+            const bool d1 = z0[p] != zlo;
+            const float v_1 = d1 ? S[1] : S[0];
+            const float v0 = d1 ? S[2] : S[1];
+            const float v1 = d1 ? S[3] : S[2];
+            const float v2 = v1;
             const float ca = -0.5f * v_1 + 1.5f * v0 - 1.5f * v1 + 0.5f * v2;
             const float cb = v_1 - 2.5f * v0 + 2.0f * v1 - 0.5f * v2;
             const float cc = -0.5f * v_1 + 0.5f * v1;
