@@ -215,6 +215,14 @@ struct Rgc3dTables {
     float4* ztab = nullptr;
     int* zstart = nullptr;    // [M^2 + 1] first entry of each lateral phase
     int zmax_taps = 0, zes = 0;  // largest entry count of a phase; float4s per entry
+    // slab-staged form: a phase's entries are ordered by plane offset sz = zk0 .. zk0 + znz - 1;
+    // zseg[lp (znz + 1) + s] is the first entry of plane s; zsoff[entry] the entry's offset in a
+    // CTA's slab of the field (rows 2 qy + sy - sl_symin, per parity columns qx + (sx >> 1) -
+    // sl_fxmin, both parities side by side in a row of 2 sl_nx float4s)
+    int* zseg = nullptr;
+    int* zsoff = nullptr;
+    int zk0 = 0, znz = 0;
+    int sl_symin = 0, sl_fxmin = 0, sl_rows = 0, sl_nx = 0;
 };
 // Tables for planes of w x h pixels, P planes; the per-voxel sums of weights are computed on
 // `stream` (synchronised before returning).

@@ -451,6 +451,191 @@ __global__ void __launch_bounds__(256, 2) rgc3d_zb_kernel(Rgc3dTabArgs a) {
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    // 16-byte asynchronous copy; valid = false writes zeros and reads nothing
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+// rgc3d_zb_kernel with the unit-gradient field staged in shared memory one plane offset at a
+// time: the entries of a lateral phase are ordered by sz, and for each (frame, sz) the CTA's slab
+// of that plane (its 8 cell rows' 2x-grid rows plus the tap reach, both parity halves of its 32
+// cell columns plus the reach) is copied with cp.async into one of two buffers while the taps of
+// the previous slab run.  Per-thread arithmetic and tap order within a plane as rgc3d_zb_kernel.
+template <int MZ>
+__global__ void __launch_bounds__(256, 2) rgc3d_zs_kernel(Rgc3dTabArgs a) {
+    extern __shared__ float4 sm4[];
+    constexpr int M = MZ, M2 = MZ * MZ;
+    const int es = a.tab.zes, nz = a.tab.znz;
+    const int qz = blockIdx.z / M2, lp = blockIdx.z % M2;
+    const int px = lp % M, py = lp / M;
+    const int t0 = a.tab.zstart[lp], n = a.tab.zstart[lp + 1] - t0;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int row2 = 2 * a.tab.sl_nx;                       // float4s per slab row
+    const int slab = a.tab.sl_rows * row2;                  // float4s per slab
+    float4* stab = sm4;                                     // [n][es]
+    int* sseg = reinterpret_cast<int*>(sm4 + a.tab.zmax_taps * es);  // [nz + 1]
+    float4* sbuf = sm4 + a.tab.zmax_taps * es + (nz + 4) / 4;        // [2][slab]
+    for (int i = tid; i < n * es; i += 256) {
+        float4 v = a.tab.ztab[(long)t0 * es + i];
+        if (i % es == 0) v.x = __int_as_float(a.tab.zsoff[t0 + i / es]);  // offset in the slab
+        stab[i] = v;
+    }
+    for (int i = tid; i <= nz; i += 256) sseg[i] = a.tab.zseg[lp * (nz + 1) + i];
+    const float* sf = reinterpret_cast<const float*>(stab);
+    const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
+    const bool valid = qx_raw < a.w && qy_raw < a.h;
+    const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
+    const int xM = qx * M + px, yM = qy * M + py;
+    const int WM = a.w * M, HM = a.h * M;
+    const long whM = (long)WM * HM, total = whM * a.P * M;
+    const long pl = (long)a.w * a.h;
+    const long fstride = (long)a.tab.Pp * a.tab.H2p * a.tab.W2p;
+    const int half = a.tab.W2p / 2;
+    const int row0 = 2 * blockIdx.y * 8 + a.tab.pady + a.tab.sl_symin;
+    const int cin0 = a.tab.padx / 2 + blockIdx.x * 32 + a.tab.sl_fxmin;
+    const int tbase = 2 * threadIdx.y * row2 + threadIdx.x;  // this thread's cell in the slab
+    const float pxf = (float)xM / (float)M - 0.5f;
+    const float pyf = (float)yM / (float)M - 0.5f;
+    long idx[MZ];
+    float wsum[MZ], prev[MZ], z01[MZ];
+    int z0[MZ];
+    float s0[MZ], s1[MZ], s2[MZ], s3[MZ];  // this launch's frames (at most a few) in FP32
+#pragma unroll
+    for (int p = 0; p < MZ; ++p) {
+        const int zM = qz * M + p;
+        idx[p] = (long)zM * whM + (long)yM * WM + xM;
+        wsum[p] = a.tab.wsum[idx[p]];
+        prev[p] = valid ? a.st.prev[idx[p]] : 0.f;
+        const float zc = (float)(((double)zM + 0.5) / M);
+        const float zcof = zc - 0.5f;
+        z0[p] = zcof < 0 ? 0 : (zcof >= (float)(a.P - 1) ? a.P - 2 : (int)floorf(zcof));
+        z01[p] = zc - (float)(z0[p] + 0.5f);
+        s0[p] = s1[p] = s2[p] = s3[p] = 0.f;
+    }
+    int zlo = z0[0];
+#pragma unroll
+    for (int p = 1; p < MZ; ++p) zlo = min(zlo, z0[p]);
+    int splane[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) splane[k] = min(max(zlo - 1 + k, 0), a.P - 1);
+
+    const int st_ly = tid / row2, st_rem = tid - st_ly * row2;
+    const int st_dly = 256 / row2, st_drem = 256 - st_dly * row2;
+    // slab g = (frame g / nz, plane offset zk0 + g % nz) into buffer g & 1
+    auto stage = [&](int g) {
+        const int f = g / nz, sidx = g - f * nz;
+        const int plane = qz + a.tab.padz_lo + a.tab.zk0 + sidx;
+        const float4* Uf = a.U + f * fstride + (long)plane * a.tab.H2p * a.tab.W2p;
+        float4* dst = sbuf + (g & 1) * slab;
+        // element i = tid + 256 k of the slab: (row ly, position rem in the row) advanced without
+        // divisions (st_ly, st_rem: this thread's first element, 256 = st_dly rows + st_drem)
+        int ly = st_ly, rem = st_rem;
+        for (int i = tid; i < slab; i += 256) {
+            const int par = rem >= a.tab.sl_nx ? 1 : 0, lx = rem - par * a.tab.sl_nx;
+            const int row = row0 + ly, cin = cin0 + lx;
+            const bool in = row < a.tab.H2p && cin < half;
+            cp_async16(dst + i, in ? (const void*)(Uf + (long)row * a.tab.W2p + par * half + cin) : (const void*)a.U, in);
+            ly += st_dly;
+            rem += st_drem;
+            if (rem >= row2) {
+                rem -= row2;
+                ++ly;
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int G = a.F * nz;
+    if (G > 0) stage(0);
+    float cg[MZ];
+    for (int g = 0; g < G; ++g) {
+        const int f = g / nz, sidx = g - f * nz;
+        if (sidx == 0) {
+#pragma unroll
+            for (int p = 0; p < MZ; ++p) cg[p] = 0.f;
+        }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // slab g landed everywhere; buffer (g + 1) & 1 is no longer read
+        if (g + 1 < G) stage(g + 1);
+        const float4* sl = sbuf + (g & 1) * slab + tbase;
+        const int tb = sseg[sidx], te = sseg[sidx + 1];
+        for (int t = tb; t < te; ++t) {
+            const float* e = sf + (long)t * es * 4;
+            const float4 u = sl[__float_as_int(e[0])];
+            const float dx = e[1], dy = e[2];
+            const float part = fmaf(u.x, dx, u.y * dy);
+            const float cz = fmaf(dx, u.y, -dy * u.x);  // dx gy - dy gx
+            const float czz = cz * cz, dyuz = dy * u.z, dxuz = dx * u.z;
+#pragma unroll
+            for (int p = 0; p < MZ; ++p) {
+                const float dz = e[3 + 3 * p], w = e[4 + 3 * p], wd = e[5 + 3 * p];
+                const float dot = fmaf(u.z, dz, part);
+                if (dot < 0.f) {
+                    const float cx = fmaf(-dz, u.y, dyuz);  // dy gz - dz gy
+                    const float cy = fmaf(dz, u.x, -dxuz);  // dz gx - dx gz
+                    cg[p] += fmaf(-wd, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, czz))), w);
+                }
+            }
+        }
+        if (sidx != nz - 1) continue;
+        const float* ap = a.apx + (long)f * a.P * pl;
+        float S[4];
+        dev::sample2d_x4(ap, pl, splane, a.w, a.h, pxf, pyf, S);
+#pragma unroll
+        for (int p = 0; p < MZ; ++p) {
+            const float c = cglh_power(cg[p] / wsum[p], a.sens);
+            const bool d1 = z0[p] != zlo;
+            const float v_1 = d1 ? S[1] : S[0];
+            const float v0 = d1 ? S[2] : S[1];
+            const float v1 = d1 ? S[3] : S[2];
+            const float v2 = v1;
+            const float ca = -0.5f * v_1 + 1.5f * v0 - 1.5f * v1 + 0.5f * v2;
+            const float cb = v_1 - 2.5f * v0 + 2.0f * v1 - 0.5f * v2;
+            const float cc = -0.5f * v_1 + 0.5f * v1;
+            const float zz = z01[p];
+            const float v = ca * zz * zz * zz + cb * zz * zz + cc * zz + v0;
+            const float x = a.int_weighting ? v * c : c;
+            s0[p] += x;
+            s1[p] = fmaf(x, x, s1[p]);
+            if (a.t0 + f > 0) s2[p] = fmaf(x, prev[p], s2[p]);
+            s3[p] += v;
+            prev[p] = x;
+        }
+    }
+    if (!valid) return;
+#pragma unroll
+    for (int p = 0; p < MZ; ++p) {
+        a.st.acc[idx[p]] += (double)s0[p];
+        a.st.acc[total + idx[p]] += (double)s1[p];
+        a.st.acc[2 * total + idx[p]] += (double)s2[p];
+        a.st.acc[3 * total + idx[p]] += (double)s3[p];
+        a.st.prev[idx[p]] = prev[p];
+    }
+}
+
+size_t zs_smem_bytes(const Rgc3dTables& t) {
+    return sizeof(float4) * ((size_t)t.zmax_taps * t.zes + (t.znz + 4) / 4 + 2 * (size_t)t.sl_rows * 2 * t.sl_nx);
+}
+
+template <int MZ>
+cudaError_t launch_zs(const Rgc3dTabArgs& a, cudaStream_t stream) {
+    const size_t smem = zs_smem_bytes(a.tab);
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && !(configured & (1ull << dev))) {
+        if ((e = cudaFuncSetAttribute(rgc3d_zs_kernel<MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      112 * 1024)) != cudaSuccess)
+            return e;
+        configured |= 1ull << dev;
+    }
+    const dim3 grid((a.w + 31) / 32, (a.h + 7) / 8, MZ * MZ * a.P);
+    rgc3d_zs_kernel<MZ><<<grid, dim3(32, 8), smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
 template <int MZ>
 cudaError_t launch_zb(const Rgc3dTabArgs& a, cudaStream_t stream) {
     const size_t smem = sizeof(float4) * (size_t)a.tab.zmax_taps * a.tab.zes;
@@ -548,6 +733,7 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
     // z-blocked entries: per lateral phase, the (j, i, k) taps valid for at least one z-phase
     std::vector<float4> Z;
     std::vector<int> zstart(M * M + 1, 0);
+    std::vector<int> zsx, zsy, zsz, zsoff, zseg;
     if (M <= 5) {
         t.zes = (3 + 3 * M + 3) / 4;
         int zmax = 0;
@@ -558,11 +744,11 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
                 const float xc = (float)(((double)px + 0.5) / M);
                 const float yc = (float)(((double)py + 0.5) / M);
                 const int kx = (int)(2.0f * xc), ky = (int)(2.0f * yc);
-                for (int j = r0; j <= r1; ++j) {
-                    const float vy = ((float)ky + (float)j) / 2.0f;
-                    for (int i = r0; i <= r1; ++i) {
-                        const float vx = ((float)kx + (float)i) / 2.0f;
-                        for (int k = k0; k <= k1; ++k) {
+                for (int k = k0; k <= k1; ++k) {  // entries ordered by plane offset
+                    for (int j = r0; j <= r1; ++j) {
+                        const float vy = ((float)ky + (float)j) / 2.0f;
+                        for (int i = r0; i <= r1; ++i) {
+                            const float vx = ((float)kx + (float)i) / 2.0f;
                             std::vector<float> ent(4 * t.zes, 0.f);
                             bool any = false;
                             const float dx = vx - xc, dy = vy - yc;
@@ -586,6 +772,9 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
                             ent[2] = dy;
                             for (int q = 0; q < t.zes; ++q)
                                 Z.push_back(make_float4(ent[4 * q], ent[4 * q + 1], ent[4 * q + 2], ent[4 * q + 3]));
+                            zsx.push_back(sx);
+                            zsy.push_back(sy);
+                            zsz.push_back(sz);
                         }
                     }
                 }
@@ -593,6 +782,36 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
             }
         zstart[M * M] = (int)(Z.size() / t.zes);
         t.zmax_taps = zmax;
+        // slab geometry: rows 2 qy + sy over the CTA's 8 cell rows, per parity columns
+        // qx + (sx >> 1) over its 32 cell columns
+        int symin = 0, symax = 0, fxmin = 0, fxmax = 0, szmin = k1, szmax = k0;
+        for (size_t e = 0; e < zsx.size(); ++e) {
+            symin = std::min(symin, zsy[e]);
+            symax = std::max(symax, zsy[e]);
+            fxmin = std::min(fxmin, zsx[e] >> 1);
+            fxmax = std::max(fxmax, zsx[e] >> 1);
+            szmin = std::min(szmin, zsz[e]);
+            szmax = std::max(szmax, zsz[e]);
+        }
+        // plane offsets of actual entries only: they lie inside the field's z padding
+        t.zk0 = szmin;
+        t.znz = std::max(szmax - szmin + 1, 1);
+        zseg.assign((size_t)M * M * (t.znz + 1), 0);
+        for (int lp = 0; lp < M * M; ++lp) {
+            const int e0 = zstart[lp], e1 = zstart[lp + 1];
+            for (int sidx = 0; sidx <= t.znz; ++sidx) {
+                int e = e0;
+                while (e < e1 && zsz[e] - szmin < sidx) ++e;
+                zseg[(size_t)lp * (t.znz + 1) + sidx] = e - e0;
+            }
+        }
+        t.sl_symin = symin;
+        t.sl_fxmin = fxmin;
+        t.sl_rows = 2 * 7 + symax - symin + 1;
+        t.sl_nx = 31 + fxmax - fxmin + 1;
+        zsoff.resize(zsx.size());
+        for (size_t e = 0; e < zsx.size(); ++e)
+            zsoff[e] = (zsy[e] - symin) * 2 * t.sl_nx + (zsx[e] & 1) * t.sl_nx + ((zsx[e] >> 1) - fxmin);
     }
     auto up = [](auto** d, const auto& v) -> cudaError_t {
         cudaError_t e = cudaMalloc((void**)d, sizeof(v[0]) * std::max<size_t>(v.size(), 1));
@@ -603,7 +822,8 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
     if ((e = up(&t.taba, A)) != cudaSuccess || (e = up(&t.tabb, B)) != cudaSuccess ||
         (e = up(&t.start, start)) != cudaSuccess)
         return e;
-    if (M <= 5 && ((e = up(&t.ztab, Z)) != cudaSuccess || (e = up(&t.zstart, zstart)) != cudaSuccess))
+    if (M <= 5 && ((e = up(&t.ztab, Z)) != cudaSuccess || (e = up(&t.zstart, zstart)) != cudaSuccess ||
+                   (e = up(&t.zseg, zseg)) != cudaSuccess || (e = up(&t.zsoff, zsoff)) != cudaSuccess))
         return e;
     const long total = (long)w * M * h * M * P * M;
     if ((e = cudaMalloc((void**)&t.wsum, sizeof(float) * total)) != cudaSuccess) return e;
@@ -627,6 +847,8 @@ void rgc3d_tables_free(Rgc3dTables& t) {
     cudaFree(t.wsum);
     cudaFree(t.ztab);
     cudaFree(t.zstart);
+    cudaFree(t.zseg);
+    cudaFree(t.zsoff);
     t = Rgc3dTables();
 }
 
@@ -639,11 +861,15 @@ cudaError_t unit_grad3d(const float* gxi, const float* gyi, const float* gzi, in
 
 cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream) {
     if (a.tab.ztab && !rgc3d_one_voxel()) {
+        // slab-staged form where two CTAs' shared memory fits an SM (ESRRF_RGC3D=zb: the form
+        // that reads the field through the L1 cache)
+        const char* form = std::getenv("ESRRF_RGC3D");
+        const bool slab = zs_smem_bytes(a.tab) <= 112 * 1024 && !(form && std::strcmp(form, "zb") == 0);
         switch (a.M) {
-            case 2: return launch_zb<2>(a, stream);
-            case 3: return launch_zb<3>(a, stream);
-            case 4: return launch_zb<4>(a, stream);
-            case 5: return launch_zb<5>(a, stream);
+            case 2: return slab ? launch_zs<2>(a, stream) : launch_zb<2>(a, stream);
+            case 3: return slab ? launch_zs<3>(a, stream) : launch_zb<3>(a, stream);
+            case 4: return slab ? launch_zs<4>(a, stream) : launch_zb<4>(a, stream);
+            case 5: return slab ? launch_zs<5>(a, stream) : launch_zb<5>(a, stream);
             default: break;
         }
     }

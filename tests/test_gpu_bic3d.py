@@ -110,15 +110,18 @@ def test_3d_mfm_normalisation_and_nine_planes(esrrf_mod, oracle_mod):
 
 @pytest.mark.parametrize("M,fwhm,S,form", [(2, 2.0, 2, "zblock"), (4, 1.0, 1, "zblock"),
                                             (3, 2.5, 1, "zblock"), (5, 1.5, 1, "zblock"),
+                                            (3, 1.5, 2, "zb"), (2, 2.0, 2, "zb"),
                                             (3, 1.5, 2, "voxel"), (4, 1.0, 1, "voxel")])
 def test_3d_tabulated_taps_radii(esrrf_mod, oracle_mod, monkeypatch, M, fwhm, S, form):
     """Blocks without drift take the tabulated-tap 3-D kernels (taps listed per sub-pixel phase,
     zero-halo unit-gradient field, tabulated sums of weights), z-blocked (the M z-phases of a
-    cell in one thread) or one voxel per thread (ESRRF_RGC3D=voxel): checked against the oracle
-    at several magnifications and radii, on volumes where most voxels have taps beyond a face."""
+    cell in one thread; the field staged in shared memory one plane offset at a time, or read
+    through the L1 cache with ESRRF_RGC3D=zb) or one voxel per thread (ESRRF_RGC3D=voxel):
+    checked against the oracle at several magnifications and radii, on volumes where most voxels
+    have taps beyond a face."""
     from esrrf import synth
-    if form == "voxel":
-        monkeypatch.setenv("ESRRF_RGC3D", "voxel")
+    if form in ("voxel", "zb"):
+        monkeypatch.setenv("ESRRF_RGC3D", form)
     else:
         monkeypatch.delenv("ESRRF_RGC3D", raising=False)
     P, h, w, n = (5, 40, 36, 3) if M < 5 else (3, 20, 18, 3)
