@@ -104,6 +104,11 @@ class ClockSampler:
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
+        # the first nvidia-smi call initialises its driver session, which can take seconds and
+        # stall CUDA calls meanwhile: let it finish before the timed region starts
+        t0 = time.perf_counter()
+        while not self.samples and time.perf_counter() - t0 < 15.0:
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *a):

@@ -63,8 +63,7 @@ struct AdjAArgs {
 };
 
 // One tap column of kernel A restricted to its disc chord [LO, HI] (compile-time, as in the fused
-// forward kernel).  The per-output dot product stays (three weight arrays already fill the
-// registers; the forward kernel's per-row threshold spills here).
+// forward kernel), with the forward kernel's per-row inward threshold.
 template <int S, int LO, int HI>
 __device__ __forceinline__ void chord_a(const float2* __restrict__ col, float fi, const float (&w)[S],
                                         const float (&wd)[S], float (&acc)[kK], float (&acc2)[kK]) {
@@ -74,16 +73,20 @@ __device__ __forceinline__ void chord_a(const float2* __restrict__ col, float fi
     for (int rr = LO; rr <= HI + kK - 1; ++rr) {
         const float2 e = col[rr * EW];
         const float fr = fr0 + (float)rr;
-        const float dot0 = fmaf(e.y, fr, e.x * fi);
+        // inward test g . (i, fr - k) < 0 as one threshold per source row (as the forward fused
+        // kernel): k > thr for gy > 0, k < thr for gy < 0, thr = fr + i gx / gy
+        float rgy;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
+        const float thr = fmaf(e.x * rgy, fi, fr);
+        const bool neg = e.y < 0.f;
         const float cr0 = fmaf(-e.x, fr, e.y * fi);
 #pragma unroll
         for (int k = 0; k < kK; ++k) {
             const int jj = rr - k;
             if (jj >= LO && jj <= HI) {
-                const float dk = k == 0 ? dot0 : fmaf(-(float)k, e.y, dot0);
                 const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
                 const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
-                if (dk < 0.f) {
+                if (((float)k > thr) != neg) {
                     acc[k] += t;
                     const float j = fr0 + (float)jj;
                     acc2[k] = fmaf(j * j, t, acc2[k]);  // j^2 t; i^2 t is added per column
