@@ -298,8 +298,7 @@ __device__ __forceinline__ void chord_b(const float* __restrict__ col, float tx_
                     const float sv = __int_as_float(__float_as_int(wd[jj] * bv) ^
                                                     (__float_as_int(c) & 0x80000000));
                     Sx[k] += sv;
-                    Tx[k] = fmaf(sv, (float)rr, Tx[k]);
-                    Sy[k] = fmaf(sv, tx_f, Sy[k]);
+                    Tx[k] = fmaf(sv, (float)rr, Tx[k]);  // Sy gets t_x times the column's sum of sv
                 }
             }
         }
@@ -397,10 +396,16 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
                 Bk[k] = fmaf(gy[k], tx_f, -gx[k] * (fr1 + (float)k));
             }
             const float* col = sB + (ty * kK) * BW + tx + ii;
+            float before[kK];
+#pragma unroll
+            for (int k = 0; k < kK; ++k) before[k] = Sx[k];
             if (lo == 0 && hi == S - 1)
                 chord_b<S, 0, S - 1>(col, tx_f, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);
             else
                 dispatch_b<S, 0>(col, tx_f, lo, hi, wd, gx, gy, Ak, Bk, Sx, Tx, Sy);
+            // t_x is the column's constant: Sy = sum sv t_x gains t_x (column sum of sv)
+#pragma unroll
+            for (int k = 0; k < kK; ++k) Sy[k] = fmaf(tx_f, Sx[k] - before[k], Sy[k]);
         }
         // project onto the tangent of the unit vector and scatter through the Roberts cross
 #pragma unroll
