@@ -1,14 +1,14 @@
 """Error of each cumulant against the FP64 oracle on the 512x512 M4 workload's settings
 (radius 1.5, S2, AVG/VAR/TAC2/INT) over a 128x128 crop of its stack, next to the error of the
 reference's own FP32 kernel arithmetic (the restatement, bit-exact to it) against the same FP64
-oracle.  Writes the figures to gpurun_out/precision_fht512.json when that folder exists."""
+oracle.  Writes the figures as JSON to the file named by ESRRF_PRECISION_JSON when it is set."""
 import json
 import os
 
 import numpy as np
 import pytest
 
-from conftest import ROOT, rel_err
+from conftest import rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -31,9 +31,9 @@ def test_cumulant_errors_against_fp64(esrrf_mod, oracle_mod):
     names = ["AVG", "VAR", "TAC2", "INT"]
     res = {n: {"gpu_vs_fp64": rel_err(gpu[k], f64[k]), "ref_fp32_vs_fp64": rel_err(f32[k], f64[k])}
            for k, n in enumerate(names)}
-    out = os.path.join(ROOT, "gpurun_out")
-    if os.path.isdir(out):
-        with open(os.path.join(out, "precision_fht512.json"), "w") as f:
+    out = os.environ.get("ESRRF_PRECISION_JSON")
+    if out:
+        with open(out, "w") as f:
             json.dump(res, f, indent=1)
     for n in names:
         assert res[n]["gpu_vs_fp64"] < 1e-4, (n, res[n])
