@@ -269,6 +269,9 @@ def run_ours(args, world, rank, local):
     eng.initialise(w, h, M, fwhm, S, nf, nf, chosenDevice=local, kernel=args.kernel,
                    framesPerLaunch=args.frames_per_launch)
     H = eng.handle
+    fpl = ctypes.c_int()
+    esrrf._lib.check(H, L.esrrf_frames_per_launch(H, ctypes.byref(fpl)))
+    F = fpl.value  # frames per fused launch (the engine's choice unless --frames-per-launch)
     eng.setTiming(True)
     WM, HM = w * M, h * M
 
@@ -349,7 +352,6 @@ def run_ours(args, world, rank, local):
     e2e_value = world * mpxf / e2e_step
 
     # roofline of the dominant kernel (fused RGC), per launch
-    F = args.frames_per_launch or 8
     launches_rgc = args.steps * n_blocks * ((nf + F - 1) // F)
     avg_launch_s = (rgc_total_ms / 1000.0) / max(1, launches_rgc)
     taps = taps_per_pixel(M, fwhm)

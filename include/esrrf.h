@@ -74,7 +74,8 @@ typedef struct {
     int interp;           /* esrrf_interp; forced to BIC in 3-D (LiveSRRF_CL.java:166-168) */
     int fht_scale;        /* esrrf_fht_scale */
     int kernel;           /* 0: fused tile kernel where applicable, 1: plain per-pixel kernel */
-    int frames_per_launch;/* frames interpolated and reduced per fused launch; 0 = autotuned */
+    int frames_per_launch;/* frames per interpolation + RGC launch; 0: the block in equal launches of
+                             at most 50 frames (FHT path, within ~4 GB of frame buffers), else 8 */
     /* 3-D calibration, all arrays of length n_planes (NULL in 2-D). */
     int n_planes;
     const float* roi;
@@ -142,6 +143,10 @@ esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* d_out);
  * copy.  `out` must stay valid (and should be pinned for the copy to overlap) until
  * esrrf_finish_queue returns; a third read waits for the first one's copy. */
 esrrf_status esrrf_read_srrf_async(esrrf_handle* h, float* out);
+
+/* Frames (timepoints in 3-D) per interpolation + RGC launch: esrrf_params.frames_per_launch, or
+ * the value chosen when that is 0 (no reference counterpart: the reference launches per frame). */
+esrrf_status esrrf_frames_per_launch(const esrrf_handle* h, int* frames);
 
 /* Output geometry (public fields widthS/heightS/nPlanes/nPlanesM, LiveSRRF_CL.java:41-45). */
 esrrf_status esrrf_output_shape(const esrrf_handle* h, int* width_m, int* height_m,

@@ -118,6 +118,17 @@ esrrf_status esrrf_handle::init(const esrrf_params& params) {
     drift_x.assign(p.n_frame_for_srrf, 0.f);
     drift_y.assign(p.n_frame_for_srrf, 0.f);
     F = p.frames_per_launch > 0 ? p.frames_per_launch : 8;
+    if (p.frames_per_launch == 0 && mode == Mode::kFHT) {
+        // FHT path: the block in equal launches of at most 50 frames (fewer launches amortise the
+        // per-launch fold of the block accumulators and the last, partial launch: 100-frame blocks
+        // of 512 x 512 at M4 run 4 % faster than with 8), within ~4 GB of per-frame buffers
+        // (interpolated frames, their gradients, the interpolation scratch: ~5 output planes)
+        const double per_frame = 5.0 * sizeof(float) * (double)p.width * p.magnification * p.height * p.magnification;
+        const int fmax = (int)std::max(1.0, std::min(50.0, 4e9 / per_frame));
+        const int nb = std::max(1, p.n_frame_for_srrf);
+        const int launches = (nb + fmax - 1) / fmax;
+        F = (nb + launches - 1) / launches;
+    }
 
     if (mode == Mode::kFHT) return init_fht();
     return init_bic3d();
@@ -701,6 +712,12 @@ esrrf_status esrrf_read_srrf(esrrf_handle* h, float* out) {
 esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* out) {
     if (!h || !out) return ESRRF_ERR_INVALID;
     return h->read(out, true);
+}
+
+esrrf_status esrrf_frames_per_launch(const esrrf_handle* h, int* frames) {
+    if (!h || !frames) return ESRRF_ERR_INVALID;
+    *frames = h->F;
+    return ESRRF_OK;
 }
 
 esrrf_status esrrf_output_shape(const esrrf_handle* h, int* wm, int* hm, int* pm) {
