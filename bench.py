@@ -230,16 +230,16 @@ def run_reference(args, world, rank):
 TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md"}
 
 
-def read_traffic_summary(kernel):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (its
-    `traffic_bytes_per_launch:` line), if any."""
+def read_traffic_summary(kernel, key="traffic_bytes_per_launch"):
+    """A figure of the dominant kernel from the committed ncu summary (its `<key>:` line: DRAM
+    bytes per launch, or warp instructions per frame), if any."""
     name = TRAFFIC_SUMMARIES.get(kernel)
     if not name:
         return None
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
+                if line.startswith(key + ":"):
                     return float(line.split(":", 1)[1])
     except (OSError, ValueError):
         return None
@@ -365,6 +365,19 @@ def run_ours(args, world, rank, local):
     achieved_tflops = ops_launch / avg_launch_s / 1e12
     cpu = cpu_reference_sample(stack, M, fwhm, S, 1) if not args.no_cpu_baseline else None
     traffic = read_traffic_summary(f"rgc_{args.kernel}_{args.workload}")
+    # the kernel's real limit is instruction issue: warp instructions per launch (ncu count per
+    # frame x frames) over the live launch time, against one warp instruction per cycle per
+    # scheduler (148 SMs x 4) at the sampled SM clock
+    clocks = clk.summary()
+    ipf = read_traffic_summary(f"rgc_{args.kernel}_{args.workload}", "warp_instructions_per_frame")
+    roofline_issue = None
+    if ipf and avg_launch_s > 0:
+        mhz = clocks.get("sm_mhz") or 1965.0
+        peak_issue = 148 * 4 * mhz * 1e6
+        got = ipf * (nf / ((nf + F - 1) // F)) / avg_launch_s  # mean frames per launch
+        roofline_issue = {"achieved": got, "peak": peak_issue, "unit": "warp instructions/s",
+                          "frac": got / peak_issue, "instructions_per_frame": ipf,
+                          "source": "instructions per frame from the committed ncu summary, launch time live"}
     line = {
         "metric": "input Mpx*frames/s (eSRRF 2-D FHT path)",
         "value": value, "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps,
@@ -386,7 +399,8 @@ def run_ours(args, world, rank, local):
                           "unit": "TFLOP/s", "frac": achieved_tflops / FP32_PEAK_NOMINAL_TFLOPS,
                           "ops_per_launch": ops_launch, "taps_per_pixel": taps,
                           "convention": "22 FP32 ops per evaluated tap; nominal peak at 1965 MHz"},
-        "clocks": clk.summary(),
+        "roofline_issue": roofline_issue,
+        "clocks": clocks,
         "cpu_baseline": cpu,
         "wall_s_timed": wall,
     }
