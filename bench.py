@@ -300,14 +300,14 @@ def run_ours(args, world, rank, local):
 
     def step_e2e():
         # each block's read-back is queued (esrrf_read_srrf_async) and overlaps the next block's
-        # upload and kernels; finishQueue waits for all of it
+        # upload and kernels, across steps too, as for a continuous stream; finishQueue after the
+        # last step waits for every copy
         base = h_stack.data_ptr()
         for b in range(n_blocks):
             esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
             esrrf._lib.check(H, L.esrrf_calculate_srrf_u16(
                 H, ctypes.c_void_p(base + b * nf * frame_bytes), nf))
             esrrf._lib.check(H, L.esrrf_read_srrf_async(H, ctypes.c_void_p(h_out[b].data_ptr())))
-        esrrf._lib.check(H, L.esrrf_finish_queue(H))
 
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -336,11 +336,13 @@ def run_ours(args, world, rank, local):
     # end-to-end through the host API
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()
+    esrrf._lib.check(H, L.esrrf_finish_queue(H))
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step_e2e()
+    esrrf._lib.check(H, L.esrrf_finish_queue(H))  # every step's results are on the host
     torch.cuda.synchronize()
     e2e_step = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
     eng.release()
