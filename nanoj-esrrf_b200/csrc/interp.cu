@@ -59,47 +59,47 @@ __device__ __forceinline__ float load_raw(const void* raw, bool is_u16, long idx
 }
 
 // Alternating sums of the padded frame: wy[y] = sum_x (-1)^x X[y][x] and
-// wx[x] = sum_y (-1)^y X[y][x].  Grid (ceil(N/32), frames): each CTA owns 32 rows and 32 columns.
-__global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u16, int w, int h,
-                                                       int N, const int* __restrict__ srcx,
-                                                       const int* __restrict__ srcy,
-                                                       float* __restrict__ alt) {
+// wx[x] = sum_y (-1)^y X[y][x].  Grid (ceil(N/32), frames), 32 warps: each CTA owns 32 rows (one
+// per warp, lanes across the row) and 32 columns (lane = column, the warps splitting the rows),
+// so that many independent loads are in flight (the sums are latency bound, not bandwidth bound).
+__global__ void __launch_bounds__(1024) alt_sums_kernel(const void* raw, int is_u16, int w, int h,
+                                                        int N, const int* __restrict__ srcx,
+                                                        const int* __restrict__ srcy,
+                                                        float* __restrict__ alt) {
     const int f = blockIdx.y;
     const void* frame = is_u16 ? (const void*)((const unsigned short*)raw + (long)f * w * h)
                                : (const void*)((const float*)raw + (long)f * w * h);
     float* out = alt + (long)f * (3 * N + 1);
-    __shared__ double red[8][33];
+    __shared__ double red[32][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int base = blockIdx.x * 32;
-    // rows base .. base+31: four per warp, lanes across the row
-    for (int r = 0; r < 4; ++r) {
-        const int y = base + warp * 4 + r;
-        if (y >= N) break;
-        const long rowoff = (long)srcy[y] * w;
-        double acc = 0.0, tot = 0.0;
-        // unrolled: several independent loads in flight per lane (the loop is latency bound)
+    {
+        const int y = base + warp;
+        if (y < N) {
+            const long rowoff = (long)srcy[y] * w;
+            double acc = 0.0, tot = 0.0;
 #pragma unroll 8
-        for (int x = lane; x < N; x += 32) {
-            const float v = load_raw(frame, is_u16, rowoff + srcx[x]);
-            acc += (x & 1) ? -(double)v : (double)v;
-            tot += (double)v;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        }
-        if (lane == 0) {
-            out[y] = (float)acc;
-            out[2 * N + 1 + y] = (float)tot;  // plain row sum, for the frame mean
+            for (int x = lane; x < N; x += 32) {
+                const float v = load_raw(frame, is_u16, rowoff + srcx[x]);
+                acc += (x & 1) ? -(double)v : (double)v;
+                tot += (double)v;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            }
+            if (lane == 0) {
+                out[y] = (float)acc;
+                out[2 * N + 1 + y] = (float)tot;  // plain row sum, for the frame mean
+            }
         }
     }
-    // columns base .. base+31: lane = column, warps stride the rows
     const int x = base + lane;
     double acc = 0.0;
     if (x < N) {
         const int sx = srcx[x];
 #pragma unroll 8
-        for (int y = warp; y < N; y += 8) {
+        for (int y = warp; y < N; y += 32) {
             const float v = load_raw(frame, is_u16, (long)srcy[y] * w + sx);
             acc += (y & 1) ? -(double)v : (double)v;
         }
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256) alt_sums_kernel(const void* raw, int is_u
     __syncthreads();
     if (warp == 0 && x < N) {
         double t = 0.0;
-        for (int i = 0; i < 8; ++i) t += red[i][lane];
+        for (int i = 0; i < 32; ++i) t += red[i][lane];
         out[N + x] = (float)t;
     }
 }
@@ -586,7 +586,7 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
     if (F <= 0) return cudaSuccess;
     if (F > sc.capacity) return cudaErrorInvalidValue;
     const int N = p.N;
-    alt_sums_kernel<<<dim3((N + 31) / 32, F), 256, 0, stream>>>(raw, is_u16 ? 1 : 0, p.w, p.h, N,
+    alt_sums_kernel<<<dim3((N + 31) / 32, F), 1024, 0, stream>>>(raw, is_u16 ? 1 : 0, p.w, p.h, N,
                                                                p.srcx, p.srcy, sc.alt);
     {
         dim3 grid((p.HM + p.WM + 31) / 32, F);
