@@ -365,7 +365,7 @@ def run_ours(args, world, rank, local):
     achieved_gbs = alg_bytes_launch / avg_launch_s / 1e9
     ops_launch = F * WM * HM * taps * OPS_PER_TAP
     achieved_tflops = ops_launch / avg_launch_s / 1e12
-    cpu = cpu_reference_sample(stack, M, fwhm, S, 1) if not args.no_cpu_baseline else None
+    cpu = cpu_reference_sample(stack, M, fwhm, S, 1) if not args.no_cpu_baseline and world == 1 else None
     traffic = read_traffic_summary(f"rgc_{args.kernel}_{args.workload}")
     # the kernel's real limit is instruction issue: warp instructions per launch (ncu count per
     # frame x frames) over the live launch time, against one warp instruction per cycle per
