@@ -257,7 +257,10 @@ const char* esrrf_squirrel_last_error(void);
 esrrf_status esrrf_drift_window(int width, int height, int max_shift, int* radius);
 /* d_frames: device, n_frames x height x width (uint16 if is_u16, else float32); ref_frame indexes
  * into them.  shift_x, shift_y: host [n_frames].  d_ccm (device, may be NULL): [n_frames][2R+1][2R+1],
- * C_f at lag (sy, sx) in row sy + R, column sx + R.  Returns when the shifts are on the host. */
+ * C_f at lag (sy, sx) in row sy + R, column sx + R.  Returns when the shifts are on the host.
+ * Scratch (the partial maps, about n_frames (2R+1)^2 x 8 B x row tiles, at most ~1 GB) is one
+ * workspace per device, grown on demand and kept until the process exits; calls on one device
+ * are serialised on it.  Errors: esrrf_drift_last_error(). */
 esrrf_status esrrf_estimate_drift(const void* d_frames, int is_u16, int n_frames, int width, int height,
                                   int ref_frame, int max_shift, float* shift_x, float* shift_y,
                                   float* d_ccm, void* stream);

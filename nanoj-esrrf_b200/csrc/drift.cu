@@ -266,7 +266,7 @@ esrrf_status esrrf_estimate_drift(const void* d_frames, int is_u16, int n_frames
     const int n_lag = (side + kLag - 1) / kLag;
     const int n_rt = (height + kTY - 1) / kTY;
     int dev = 0;
-    cudaGetDevice(&dev);
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail("no current CUDA device", ESRRF_ERR_CUDA);
     // one block per (lag tile, frame, image row tile) -- the finest split measured fastest on a
     // B200 (100 frames of 512 x 512: 4.7 ms against 5.2 ms for 4 row tiles per block) -- unless the
     // per-stripe partial maps would pass 1 GB
