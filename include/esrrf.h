@@ -156,6 +156,18 @@ esrrf_status esrrf_output_shape(const esrrf_handle* h, int* width_m, int* height
  * frame of the last push ([2 or 3][planes][h'][w'] float, h'/w' as in the reference). */
 esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len);
 
+/* Replaces LiveSRRF_CL.readAlignedPixels (LiveSRRF_CL.java:881-906): the 3-D path's aligned planes
+ * (split, background-subtracted, scaled, rotated and shifted) of the first frame of the last group
+ * of frames on the device (a push of at most esrrf_frames_per_launch frames is one group),
+ * [n_planes][height / 3][width / 3] float, NaN -> 0.  ESRRF_ERR_STATE on the 2-D paths. */
+esrrf_status esrrf_read_aligned_pixels(esrrf_handle* h, float* out, size_t out_len);
+
+/* Replaces LiveSRRF_CL.readMPmaps (LiveSRRF_CL.java:909-935): the macro-pixel maps of the last read
+ * (each cumulant's mean over the image of every sub-pixel phase), [3][M][M] on the bicubic path,
+ * [3][M][M][M] (per cumulant M z-phase slices of M x M) in 3-D, NaN -> 0.  ESRRF_ERR_STATE without
+ * MP correction or on the FHT path (the reference builds the map on the bicubic paths only). */
+esrrf_status esrrf_read_mp_maps(esrrf_handle* h, float* out, size_t out_len);
+
 /* Replaces finishQueue (LiveSRRF_CL.java:1009-1015): waits for every queued kernel, input copy
  * and read-back of the handle; ESRRF_ERR_TIMEOUT if a bounded tensor-core wait gave up.  The
  * pushes (esrrf_calculate_srrf_*) from host memory return once their frames are copied; the

@@ -760,6 +760,40 @@ esrrf_status esrrf_read_gradients(esrrf_handle* h, float* out, size_t out_len) {
     return ESRRF_OK;
 }
 
+esrrf_status esrrf_read_aligned_pixels(esrrf_handle* h, float* out, size_t out_len) {
+    if (!h || !out) return ESRRF_ERR_INVALID;
+    if (h->mode != esrrf_handle::Mode::k3D) return h->fail(ESRRF_ERR_STATE, "aligned pixels exist on the 3-D path only");
+    if (cudaSetDevice(h->device) != cudaSuccess) return ESRRF_ERR_CUDA;
+    const size_t n = (size_t)h->P * h->ws * h->hs;  // first frame of the last push
+    if (out_len < n) return h->fail(ESRRF_ERR_INVALID, "output buffer too small");
+    if (cudaMemcpyAsync(out, h->d_fraw, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return h->fail(ESRRF_ERR_CUDA, "aligned-pixel read-back failed");
+    }
+    for (size_t i = 0; i < n; ++i)
+        if (std::isnan(out[i])) out[i] = 0.f;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_read_mp_maps(esrrf_handle* h, float* out, size_t out_len) {
+    if (!h || !out) return ESRRF_ERR_INVALID;
+    if (h->mode == esrrf_handle::Mode::kFHT || !h->p.mp_correction)
+        return h->fail(ESRRF_ERR_STATE, "MP maps exist on the bicubic and 3-D paths with MP correction only");
+    if (cudaSetDevice(h->device) != cudaSuccess) return ESRRF_ERR_CUDA;
+    const int M = h->p.magnification;
+    const size_t n = (size_t)3 * M * M * (h->mode == esrrf_handle::Mode::k3D ? M : 1);
+    if (out_len < n) return h->fail(ESRRF_ERR_INVALID, "output buffer too small");
+    if (cudaMemcpyAsync(out, h->d_mpmap, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return h->fail(ESRRF_ERR_CUDA, "MP map read-back failed");
+    }
+    for (size_t i = 0; i < n; ++i)
+        if (std::isnan(out[i])) out[i] = 0.f;
+    return ESRRF_OK;
+}
+
 esrrf_status esrrf_finish_queue(esrrf_handle* h) {
     if (!h) return ESRRF_ERR_INVALID;
     return h->drain();

@@ -187,6 +187,22 @@ class LiveSRRF_CL:
                                                        ctypes.c_size_t(out.size)))
         return out
 
+    # -- LiveSRRF_CL.readAlignedPixels (LiveSRRF_CL.java:881-906); 3-D only
+    def readAlignedPixels(self):
+        out = np.empty((self.nPlanes, self.heightS, self.widthS), np.float32)
+        _lib.check(self._h, lib().esrrf_read_aligned_pixels(self._h, out.ctypes.data_as(ctypes.c_void_p),
+                                                            ctypes.c_size_t(out.size)))
+        return out
+
+    # -- LiveSRRF_CL.readMPmaps (LiveSRRF_CL.java:909-935); bicubic and 3-D paths with MP correction
+    def readMPmaps(self):
+        M = int(self._params.magnification)
+        n = 3 * (M if self._params.n_planes > 0 else 1)
+        out = np.empty((n, M, M), np.float32)
+        _lib.check(self._h, lib().esrrf_read_mp_maps(self._h, out.ctypes.data_as(ctypes.c_void_p),
+                                                     ctypes.c_size_t(out.size)))
+        return out
+
     # -- LiveSRRF_CL.finishQueue (LiveSRRF_CL.java:1009-1015)
     def finishQueue(self):
         _lib.check(self._h, lib().esrrf_finish_queue(self._h))

@@ -63,6 +63,8 @@ SIGNATURES = {
     "esrrf_read_srrf": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
     "esrrf_read_srrf_async": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
     "esrrf_frames_per_launch": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
+    "esrrf_read_aligned_pixels": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_size_t]),
+    "esrrf_read_mp_maps": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_size_t]),
     "esrrf_read_srrf_device": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
     "esrrf_output_shape": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int), _c.POINTER(_c.c_int),
                                       _c.POINTER(_c.c_int)]),

@@ -181,3 +181,107 @@ def test_3d_calibration_table_from_file(esrrf_mod, tmp_path):
     finally:
         eng.release()
     np.testing.assert_array_equal(a, b)
+
+
+def test_3d_read_aligned_pixels(esrrf_mod, oracle_mod):
+    """readAlignedPixels (LiveSRRF_CL.java:881-906): the aligned planes of the first frame of the
+    last group on the GPU.  With no rotation they are the split, background-subtracted, scaled
+    planes (the oracle's reshape), moved by the integer calibration shifts."""
+    from esrrf import synth
+    P, h, w, n, M = 9, 40, 48, 5, 2
+    planes = synth.small_stack(5, n, h, w, planes=P).astype(np.float32)
+    roi = np.array([4, 0, 1, 2, 3, 5, 6, 7, 8], np.float32)
+    coeff = np.linspace(0.8, 1.2, P).astype(np.float32)
+    bg = 90.0
+    cam = tile_planes(planes * coeff[None, :, None, None] + bg, roi)
+    ref = oracle_mod.mfm_reshape(cam, P, roi, coeff, bg)[0]
+    zeros = np.zeros(P, np.float32)
+    sx = np.array([0, 1, -2, 0, 3, 0, -1, 2, 0], np.float32)
+    sy = np.array([0, 0, 1, -2, 0, 2, -1, 0, 1], np.float32)
+    for shx, shy in ((zeros, zeros), (sx, sy)):
+        eng = esrrf_mod.LiveSRRF_CL()
+        eng.initialise(w * 3, h * 3, M, 1.5, 1, n, n, doMPmapCorrection=False,
+                       doFHTinterpolation=False, calibTable3DSRRF=calib(P, zeros, shx, shy, roi, coeff, bg))
+        try:
+            eng.resetFramePosition()
+            assert not eng.calculateSRRF(cam)
+            got = eng.readAlignedPixels()
+        finally:
+            eng.release()
+        assert got.shape == (P, h, w)
+        for z in range(P):
+            ix, iy = int(shx[z]), int(shy[z])
+            # aligned(x, y) = plane(x - sx, y - sy); compare where the source stays 2 px inside
+            ys = slice(max(iy, 0) + 2, h + min(iy, 0) - 2)
+            xs = slice(max(ix, 0) + 2, w + min(ix, 0) - 2)
+            src = np.roll(ref[z], (iy, ix), axis=(0, 1))
+            np.testing.assert_allclose(got[z][ys, xs], src[ys, xs], rtol=1e-6, atol=1e-6 * np.abs(ref).max(),
+                                       err_msg=f"plane {z}")
+
+
+def test_2d_read_aligned_pixels_is_a_state_error(esrrf_mod):
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(32, 32, 2, 1.5, 1, 4, 4, doFHTinterpolation=False)
+    try:
+        with pytest.raises(esrrf_mod.EsrrfError):
+            eng.readAlignedPixels()
+    finally:
+        eng.release()
+
+
+@pytest.mark.parametrize("is3d", [False, True])
+def test_read_mp_maps(esrrf_mod, is3d):
+    """readMPmaps (LiveSRRF_CL.java:909-935): each cumulant's mean over the image at every
+    sub-pixel phase of the uncorrected reconstruction; the corrected output is the uncorrected one
+    divided by its phase's entry."""
+    from esrrf import synth
+    M, n = 3, 6
+    if is3d:
+        P, h, w = 4, 24, 32
+        planes = synth.small_stack(11, n, h, w, planes=P).astype(np.float32)
+        roi = np.array([0, 1, 2, 3], np.float32)
+        zeros = np.zeros(P, np.float32)
+        frames = tile_planes(planes, roi)
+        cal = calib(P, np.linspace(-0.5, 0.5, P).astype(np.float32), zeros, zeros, roi)
+    else:
+        P, h, w = 1, 36, 44
+        frames = synth.small_stack(11, n, h, w).astype(np.float32)
+        cal = None
+    raw, _ = run(esrrf_mod, frames, M, 1.5, 2, mp=False, calib=cal)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(frames.shape[-1], frames.shape[-2], M, 1.5, 2, n, n, doMPmapCorrection=True,
+                   doFHTinterpolation=False, calibTable3DSRRF=cal)
+    try:
+        eng.resetFramePosition()
+        assert not eng.calculateSRRF(frames)
+        corr = eng.readSRRFbuffer().copy()
+        maps = eng.readMPmaps()
+    finally:
+        eng.release()
+    PM = P * M if is3d else 1
+    raw = raw.reshape(4, PM, h * M, w * M).astype(np.float64)
+    corr = corr.reshape(4, PM, h * M, w * M)
+    assert maps.shape == (3 * (M if is3d else 1), M, M)
+    ref = np.empty((3, M if is3d else 1, M, M))
+    for c in range(3):
+        for pz in range(M if is3d else 1):
+            for py in range(M):
+                for px in range(M):
+                    ref[c, pz, py, px] = raw[c, pz::M, py::M, px::M].mean()
+    for c in range(3):
+        np.testing.assert_allclose(maps.reshape(ref.shape)[c], ref[c], rtol=2e-5,
+                                   atol=1e-5 * np.abs(ref[c]).max(), err_msg=f"map {c}")
+    for c in range(3):
+        m = ref[c][(np.arange(PM) % M)[:, None, None] if is3d else np.zeros((1, 1, 1), int),
+                   (np.arange(h * M) % M)[None, :, None], (np.arange(w * M) % M)[None, None, :]]
+        assert rel_err(corr[c], (raw[c] / m).astype(np.float32)) < TOL, f"cumulant {c}"
+
+
+def test_fht_read_mp_maps_is_a_state_error(esrrf_mod):
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(32, 32, 2, 1.5, 1, 4, 4, doMPmapCorrection=True, doFHTinterpolation=True)
+    try:
+        with pytest.raises(esrrf_mod.EsrrfError):
+            eng.readMPmaps()
+    finally:
+        eng.release()
