@@ -211,6 +211,13 @@ class LiveSRRF_CL:
         """Thread-safe counterpart of the reference's Escape-key polling."""
         _lib.check(self._h, lib().esrrf_request_cancel(self._h))
 
+    def framesPerLaunch(self) -> int:
+        """Frames one RGC launch processes (no reference counterpart: the reference launches per
+        frame); 0 at initialise picks the default split."""
+        f = ctypes.c_int()
+        _lib.check(self._h, lib().esrrf_frames_per_launch(self._h, ctypes.byref(f)))
+        return f.value
+
     def lastTiming(self):
         i, r, n = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
         _lib.check(self._h, lib().esrrf_last_timing(self._h, ctypes.byref(i), ctypes.byref(r),

@@ -117,6 +117,30 @@ def test_identical_frames_full_size(esrrf_mod):
     np.testing.assert_allclose(out[3], 300.0, rtol=1e-5)
 
 
+def test_launch_split_and_time_reversal_full_size(esrrf_mod):
+    """Size-independent properties of one 100-frame block at 512x512, M4 (the full block of the
+    500-frame workload): the cumulants do not depend on how the block is cut into launches (the
+    default 34 + 33 + 33, 8 per launch, uneven pushes of 17 + 50 + 33), and they are unchanged when
+    the frames are taken in reverse order -- AVG, VAR and INT are sums over frames and TAC2 sums the
+    products of adjacent frames, so a frame pair lost or counted twice at a launch edge shows."""
+    from esrrf import synth
+    raw = synth.make_stack("fht512", frames=100)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(512, 512, 4, 1.5, 2, 100, 100)
+    try:
+        assert eng.framesPerLaunch() == 34
+    finally:
+        eng.release()
+    a = run_engine(esrrf_mod, raw, 4, 1.5, 2)
+    b = run_engine(esrrf_mod, raw, 4, 1.5, 2, frames_per_launch=8)
+    c = run_engine(esrrf_mod, raw, 4, 1.5, 2, chunks=[17, 50, 33])
+    r = run_engine(esrrf_mod, np.ascontiguousarray(raw[::-1]), 4, 1.5, 2)
+    assert_close(b, a, tol=1e-5, what="8 per launch")
+    assert_close(c, a, tol=1e-5, what="uneven pushes")
+    assert_close(r, a, tol=1e-5, what="reversed")
+    assert np.abs(a[2]).max() > 0  # TAC2 carries signal in this block
+
+
 def test_block_overflow_and_cancel(esrrf_mod):
     from esrrf import EsrrfError, synth
     raw = synth.small_stack(24, 6, 16, 16)
