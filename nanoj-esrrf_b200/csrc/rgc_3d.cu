@@ -464,7 +464,7 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
 // cell columns plus the reach) is copied with cp.async into one of two buffers while the taps of
 // the previous slab run.  Per-thread arithmetic and tap order within a plane as rgc3d_zb_kernel.
 template <int MZ>
-__global__ void __launch_bounds__(256, 2) rgc3d_zs_kernel(Rgc3dTabArgs a) {
+__global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTabArgs a) {
     extern __shared__ float4 sm4[];
     constexpr int M = MZ, M2 = MZ * MZ;
     const int es = a.tab.zes, nz = a.tab.znz;
@@ -627,7 +627,9 @@ cudaError_t launch_zs(const Rgc3dTabArgs& a, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
     if (dev < 64 && !(configured & (1ull << dev))) {
         if ((e = cudaFuncSetAttribute(rgc3d_zs_kernel<MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      112 * 1024)) != cudaSuccess)
+                                      112 * 1024)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(rgc3d_zs_kernel<MZ>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
             return e;
         configured |= 1ull << dev;
     }
