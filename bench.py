@@ -42,6 +42,7 @@ WORKLOADS = {
     "mfm3d": ("mfm3d", 200),     # 3-D MFM path, 9 planes
     "adjoint256": ("adjoint256", 100),  # differentiable eSRRF: loss + gradients
     "drift512": ("fht512", 100),  # drift estimation per block of the headline stack
+    "bic512": ("fht512", 100),    # 2-D bicubic path with MP correction on the headline stack
 }
 SWEEP_RADII = [0.5 + 0.25 * i for i in range(11)]
 SWEEP_SENS = [1, 2, 3, 4]
@@ -74,6 +75,33 @@ def taps_per_pixel(M, fwhm):
             if d != 0 and d <= tSO:
                 n += 1
     return n
+
+
+def bic_taps_per_pixel(M, fwhm):
+    """Interior tap count of the 2-D bicubic path, averaged over the M x M sub-pixel phases: the
+    offsets of the 2x gradient grid around (xM + 0.5) / M inside the disc, zero excluded
+    (liveSRRF.cl:238-401 geometry, FP32 as the kernel evaluates it)."""
+    f = np.float32
+    gm = 2
+    sigma = f(fwhm) / f(2.354)
+    radius = f(int(f(gm * 2) * sigma)) / f(gm) + f(1)
+    tSO = f(2) * sigma + f(1)
+    r0, r1 = -int(f(gm) * radius), int(f(gm) * radius + f(1))
+    cell = 64  # any interior cell
+    total = 0
+    for py in range(M):
+        for px in range(M):
+            xc = f((cell * M + px + 0.5) / M)
+            yc = f((cell * M + py + 0.5) / M)
+            kx, ky = int(f(gm) * xc), int(f(gm) * yc)
+            for j in range(r0, r1 + 1):
+                dy = f(f(ky + j) / f(gm)) - yc
+                for i in range(r0, r1 + 1):
+                    dx = f(f(kx + i) / f(gm)) - xc
+                    d = np.sqrt(f(dx * dx + dy * dy))
+                    if d != 0 and d <= tSO:
+                        total += 1
+    return total / (M * M)
 
 
 class ClockSampler:
@@ -162,26 +190,38 @@ def max_over_ranks(world, x):
     return float(t.item())
 
 
-def cpu_reference_sample(stack, M, fwhm, S, n_frames=1):
-    """Reference kernels (oracle/_ref, all host cores) on `n_frames` frames of one block, the
-    Fourier interpolation of those frames by numpy's FFT, both timed."""
+def cpu_reference_sample(stack, M, fwhm, S, n_frames=1, bic=False):
+    """Reference kernels (oracle/_ref, all host cores) on `n_frames` frames of one block: for the
+    FHT path after the Fourier interpolation of those frames by numpy's FFT, both timed; for the
+    bicubic path on the raw frames with MP correction."""
     from oracle import oracle as O
 
     kind = "reference" if O.ref_available() else "port"
     raw = np.ascontiguousarray(stack[:n_frames], np.float32)
     t0 = time.perf_counter()
-    interp = O.fht_interpolate_fft(raw, M)
-    if kind == "reference":
-        O.ref_fht_block(interp, M, fwhm, S)
+    if bic:
+        if kind == "reference":
+            O.ref_bic_block(raw, M, fwhm, S, mp_correction=True)
+        else:
+            O.bic_block(raw, M, fwhm, S, mp_correction=True)
     else:
-        O.fht_block(interp, M, fwhm, S)
+        interp = O.fht_interpolate_fft(raw, M)
+        if kind == "reference":
+            O.ref_fht_block(interp, M, fwhm, S)
+        else:
+            O.fht_block(interp, M, fwhm, S)
     dt = time.perf_counter() - t0
     mpxf = raw.shape[0] * raw.shape[1] * raw.shape[2] / 1e6
     cores = os.cpu_count() or 1
+    what = "bicubic path with MP correction" if bic else "numpy-FFT interpolation"
     return {"value": mpxf / dt, "unit": "Mpx*frames/s", "cores": cores, "kind": kind,
-            "sample": f"{n_frames} frame(s) of {raw.shape[2]}x{raw.shape[1]}, M{M}: numpy-FFT "
-                      f"interpolation + {'reference kernels compiled for the host' if kind == 'reference' else 'C restatement'}"
+            "sample": f"{n_frames} frame(s) of {raw.shape[2]}x{raw.shape[1]}, M{M}: {what} + "
+                      f"{'reference kernels compiled for the host' if kind == 'reference' else 'C restatement'}"
                       f", OpenMP over {cores} threads; {dt:.2f} s"}
+
+
+def path_label(workload):
+    return "2-D bicubic path" if workload == "bic512" else "2-D FHT path"
 
 
 def run_reference(args, world, rank):
@@ -205,22 +245,25 @@ def run_reference(args, world, rank):
             "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "frames/s"},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
-    stack = synth.make_stack(name, frames=max(2, args.steps + args.warmup))
+    bic = args.workload == "bic512"
+    per = 2 if bic else 1  # frames per sample (the bicubic path's TAC2 divides by n - 1)
+    stack = synth.make_stack(name, frames=max(2, per * (args.steps + args.warmup)))
     M, fwhm, S = wl.magnification, wl.fwhm, wl.sensitivity
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_sample(stack[i:i + 1], M, fwhm, S, 1)
+        r = cpu_reference_sample(stack[per * i:per * (i + 1)], M, fwhm, S, per, bic=bic)
         if i >= args.warmup:
             vals.append(r)
     v = statistics.median([r["value"] for r in vals])
-    dt = sum(1.0 / r["value"] for r in vals) * (wl.width * wl.height / 1e6)
+    dt = sum(1.0 / r["value"] for r in vals) * (per * wl.width * wl.height / 1e6)
     line = {
-        "impl": "reference", "metric": "input Mpx*frames/s (eSRRF 2-D FHT path)", "value": v,
+        "impl": "reference", "metric": f"input Mpx*frames/s (eSRRF {path_label(args.workload)})", "value": v,
         "unit": "Mpx*frames/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * dt / max(1, len(vals)), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.workload}: 512x512x500 uint16, M4, radius 1.5, S2, "
-                               "AVG+VAR+TAC2, blocks of 100 (bounded sample: 1 frame per step)"},
+                               f"{'bicubic interpolation, MP correction, ' if bic else ''}"
+                               f"AVG+VAR+TAC2, blocks of 100 (bounded sample: {per} frame(s) per step)"},
         "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "Mpx*frames/s"},
         "e2e": {"value": v, "unit": "Mpx*frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -265,9 +308,11 @@ def run_ours(args, world, rank, local):
     n_blocks = n // nf
     L = esrrf.lib()
 
+    bic = args.workload == "bic512"
     eng = esrrf.LiveSRRF_CL()
     eng.initialise(w, h, M, fwhm, S, nf, nf, chosenDevice=local, kernel=args.kernel,
-                   framesPerLaunch=args.frames_per_launch)
+                   framesPerLaunch=args.frames_per_launch, doFHTinterpolation=not bic,
+                   doMPmapCorrection=bic)
     H = eng.handle
     fpl = ctypes.c_int()
     esrrf._lib.check(H, L.esrrf_frames_per_launch(H, ctypes.byref(fpl)))
@@ -356,7 +401,7 @@ def run_ours(args, world, rank, local):
     # roofline of the dominant kernel (fused RGC), per launch
     launches_rgc = args.steps * n_blocks * ((nf + F - 1) // F)
     avg_launch_s = (rgc_total_ms / 1000.0) / max(1, launches_rgc)
-    taps = taps_per_pixel(M, fwhm)
+    taps = bic_taps_per_pixel(M, fwhm) if bic else taps_per_pixel(M, fwhm)
     peaks, peak_src = load_peaks()
     # compulsory HBM bytes of the path per input pixel-frame: raw uint16 in, plus the four
     # float outputs of each block amortised over its frames
@@ -365,7 +410,8 @@ def run_ours(args, world, rank, local):
     achieved_gbs = alg_bytes_launch / avg_launch_s / 1e9
     ops_launch = F * WM * HM * taps * OPS_PER_TAP
     achieved_tflops = ops_launch / avg_launch_s / 1e12
-    cpu = cpu_reference_sample(stack, M, fwhm, S, 1) if not args.no_cpu_baseline and world == 1 else None
+    cpu = (cpu_reference_sample(stack, M, fwhm, S, 2 if bic else 1, bic=bic)
+           if not args.no_cpu_baseline and world == 1 else None)
     traffic = read_traffic_summary(f"rgc_{args.kernel}_{args.workload}")
     # the kernel's real limit is instruction issue: warp instructions per launch (ncu count per
     # frame x frames) over the live launch time, against one warp instruction per cycle per
@@ -381,12 +427,14 @@ def run_ours(args, world, rank, local):
                           "frac": got / peak_issue, "instructions_per_frame": ipf,
                           "source": "instructions per frame from the committed ncu summary, launch time live"}
     line = {
-        "metric": "input Mpx*frames/s (eSRRF 2-D FHT path)",
+        "metric": f"input Mpx*frames/s (eSRRF {path_label(args.workload)})",
         "value": value, "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1000.0, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.workload}: {w}x{h}x{n} uint16, M{M}, radius {fwhm}, S{S}, "
-                               f"AVG+VAR+TAC2+INT, blocks of {nf}", "kernel": args.kernel,
+                               f"{'bicubic interpolation, MP correction, ' if bic else ''}"
+                               f"AVG+VAR+TAC2+INT, blocks of {nf}",
+                   "kernel": "bicubic" if bic else args.kernel,
                    "frames_per_launch": F, "l2": "inputs (262 MB) larger than L2",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "Mpx*frames/s", "h2d_bytes_per_step": int(stack.nbytes),
@@ -395,7 +443,8 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved_gbs / peaks["hbm_gbs"],
                      "traffic": traffic, "peak_source": peak_src,
-                     "kernel": f"fht_rgc_{args.kernel}", "avg_launch_ms": avg_launch_s * 1e3,
+                     "kernel": "bic_rgc" if bic else f"fht_rgc_{args.kernel}",
+                     "avg_launch_ms": avg_launch_s * 1e3,
                      "alg_bytes_per_launch": alg_bytes_launch},
         "roofline_fp32": {"achieved": achieved_tflops, "peak": FP32_PEAK_NOMINAL_TFLOPS,
                           "unit": "TFLOP/s", "frac": achieved_tflops / FP32_PEAK_NOMINAL_TFLOPS,

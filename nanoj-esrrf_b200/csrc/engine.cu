@@ -214,6 +214,12 @@ esrrf_status esrrf_handle::init_bic3d() {
         CK(rgc3d_tables_build(bgeo, M, ws, hs, P, t3d, stream));
         CK(cudaMalloc(&d_u3, sizeof(float4) * rgc3d_field_float4s(t3d, F)));
         CK(cudaMemsetAsync(d_u3, 0, sizeof(float4) * rgc3d_field_float4s(t3d, F), stream));  // zero halo
+    } else {
+        CK(bic_tables_build(bgeo, M, ws, hs, tbic, tbic_built, stream));
+        if (tbic_built) {
+            CK(cudaMalloc(&d_u2, sizeof(float2) * bic_field_float2s(tbic, F)));
+            CK(cudaMemsetAsync(d_u2, 0, sizeof(float2) * bic_field_float2s(tbic, F), stream));  // zero halo
+        }
     }
     CK(cudaMalloc(&d_mpmap, sizeof(float) * 3 * M * M * M));
     return alloc_common(sizeof(float) * (size_t)W * H, (long)WM * HM * PM);
@@ -276,6 +282,8 @@ void esrrf_handle::release() {
     d_out2 = nullptr;
     rgc3d_tables_free(t3d);
     cudaFree(d_u3);
+    bic_tables_free(tbic);
+    cudaFree(d_u2);
     for (float* b : {d_fraw, d_planes, d_gz, d_gxi, d_gyi, d_gzi, d_mpmap, mfm.coeff, mfm.cos_t,
                      mfm.sin_t, mfm.shx, mfm.shy})
         cudaFree(b);
@@ -394,7 +402,26 @@ esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int
         launches += 6;
     }
     if (timing) CK(cudaEventRecord(e1, stream));
-    if (mode == Mode::kBIC) {
+    // tabulated taps unless a frame of this launch has drift or the plain kernel was asked for
+    bool no_drift = p.kernel == 0;
+    for (int i = 0; i < 2 * F_now; ++i) no_drift = no_drift && sh[i] == 0.f;
+    if (mode == Mode::kBIC && no_drift && tbic_built) {
+        CK(unit_grad2d(d_gxi, d_gyi, ws, hs, F_now, tbic, d_u2, stream));
+        BicTabArgs ta{};
+        ta.U = d_u2;
+        ta.fraw = d_fraw;
+        ta.w = ws;
+        ta.h = hs;
+        ta.M = p.magnification;
+        ta.F = F_now;
+        ta.t0 = frame_in_block;
+        ta.sens = bgeo.sensitivity;
+        ta.int_weighting = p.int_weighting;
+        ta.tab = tbic;
+        ta.st = st;
+        CK(bic_rgc_tab(ta, stream));
+        launches += 1;
+    } else if (mode == Mode::kBIC) {
         BicRgcArgs a{};
         a.fraw = d_fraw;
         a.gxi = d_gxi;
@@ -413,9 +440,6 @@ esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int
         a.st = st;
         CK(bic_rgc(a, stream));
     } else {
-        // tabulated taps unless a frame of this launch has drift or the plain kernel was asked for
-        bool no_drift = p.kernel == 0;
-        for (int i = 0; i < 2 * F_now; ++i) no_drift = no_drift && sh[i] == 0.f;
         if (no_drift) {
             CK(unit_grad3d(d_gxi, d_gyi, d_gzi, ws, hs, P, F_now, t3d, d_u3, stream));
             Rgc3dTabArgs ta{};

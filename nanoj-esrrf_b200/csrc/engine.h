@@ -45,6 +45,9 @@ struct esrrf_handle {
     float* d_mpmap = nullptr;   // [3][M^2 or M^3]
     esrrf::Rgc3dTables t3d;     // 3-D tap tables per sub-pixel phase (launches without drift)
     float4* d_u3 = nullptr;     // [F][P][2hs][2ws] unit gradient field
+    esrrf::BicTables tbic;      // 2-D bicubic tap tables per sub-pixel phase (launches without drift)
+    bool tbic_built = false;
+    float2* d_u2 = nullptr;     // [F][2hs][2ws] padded unit gradient field (2-D bicubic)
 
     // input staging (double-buffered)
     size_t raw_frame_bytes = 0;

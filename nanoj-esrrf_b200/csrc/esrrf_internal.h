@@ -172,6 +172,47 @@ cudaError_t bic_prepare(const void* raw, int is_u16, int w, int h, int F, float*
                         float* gy, float* gxi, float* gyi, cudaStream_t stream);
 cudaError_t grad2x(const float* g, int w, int h, int planes, float* gi, cudaStream_t stream);
 cudaError_t bic_rgc(const BicRgcArgs& a, cudaStream_t stream);
+
+// Tabulated 2-D bicubic-path RGC for launches without drift.  With zero shift the tap geometry
+// of an output pixel depends only on its sub-pixel phase (xM % M, yM % M), so each phase's taps
+// inside the disc (reference loop order j, i) are listed once; a CTA of 32 x 8 input cells of one
+// phase stages its slab of the unit-gradient field in shared memory per frame.
+struct BicTables {
+    float4* tab = nullptr;   // [taps] (offset in a CTA's slab as int bits, dx, dy, w / d)
+    float* tw = nullptr;     // [taps] w
+    int2* node = nullptr;    // [taps] 2x-grid node offset (sx, sy) from (2 qx, 2 qy)
+    int* start = nullptr;    // [M^2 + 1] first tap of each phase
+    float* wsum = nullptr;   // [h M][w M] sum of w over each pixel's in-range taps
+    int max_taps = 0;
+    // zero halo of the field (2x-grid columns, even, and rows); padded width and height
+    int padx = 0, pady = 0, W2p = 0, H2p = 0;
+    // slab of a CTA: rows 2 qy + sy - sl_symin, per parity columns qx + (sx >> 1) - sl_fxmin,
+    // both parities side by side in a row of 2 sl_nx float2s
+    int sl_symin = 0, sl_fxmin = 0, sl_rows = 0, sl_nx = 0;
+    size_t smem = 0;         // dynamic shared memory of one CTA
+};
+// Tables for frames of w x h pixels; false in `built` when a CTA's shared memory would not fit
+// (the per-pixel kernel runs instead).  The per-pixel sums of weights are computed on `stream`
+// (synchronised before returning).
+cudaError_t bic_tables_build(const BicGeometry& g, int M, int w, int h, BicTables& t, bool& built,
+                             cudaStream_t stream);
+void bic_tables_free(BicTables& t);
+size_t bic_field_float2s(const BicTables& t, int F);
+struct BicTabArgs {
+    const float2* U;     // [F][H2p][W2p] padded unit gradient, columns split by parity
+    const float* fraw;   // [F][h][w] raw frames as float (intensity source)
+    int w, h, M, F, t0;
+    float sens;
+    int int_weighting;
+    BicTables tab;
+    BlockState st;
+};
+// unit gradient (Gx read at x + 1, Gy at y + 1 of the 2x grid) into the interior of the padded
+// field; zero at the last column and row, which no tap reads.  The halo is zeroed once, when the
+// field is allocated.
+cudaError_t unit_grad2d(const float* gxi, const float* gyi, int w, int h, int F, const BicTables& t,
+                        float2* U, cudaStream_t stream);
+cudaError_t bic_rgc_tab(const BicTabArgs& a, cudaStream_t stream);
 // MP map of AVG/VAR/TAC2 and division (then NaN->0) on a finalized output [4][PM][HM][WM].
 cudaError_t mp_correct(float* out, int w, int h, int P, int M, int is3d, float* map,
                        cudaStream_t stream);

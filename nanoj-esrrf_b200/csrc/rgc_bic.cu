@@ -8,6 +8,10 @@
 // registers; the reference instead relaunches per frame and read-modify-writes global memory.
 #include <math.h>
 
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
 #include "device_common.cuh"
 #include "esrrf_internal.h"
 
@@ -157,7 +161,278 @@ __global__ void mp_correct_kernel(float* __restrict__ out, int w, int h, int P, 
     out[idx] = isnan(v) ? 0.f : v;
 }
 
+// Unit gradient on the 2x grid into the padded field, columns split by parity (column ax of
+// parity ax & 1 at ax >> 1), so 32 consecutive cells of one phase read 32 consecutive entries.
+// The reference reads Gx at (ay, ax + 1) and Gy at (ay + 1, ax) for a tap at ax = 2 (vx - 0.5)
+// and takes the tap only if 0 < vx < w, i.e. 0 <= ax <= 2w - 2 (liveSRRF.cl:271-290): the last
+// column and row hold a zero gradient, never inward, so out-of-range taps add nothing.
+__global__ void unit_grad2d_kernel(const float* __restrict__ gxi, const float* __restrict__ gyi,
+                                   int w, int h, int padx, int pady, int W2p, int H2p,
+                                   float2* __restrict__ U) {
+    const int ax = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ay = blockIdx.y;
+    const long f = blockIdx.z;
+    const int w2 = 2 * w, h2 = 2 * h;
+    if (ax >= w2) return;
+    float2 u = make_float2(0.f, 0.f);
+    if (ax < w2 - 1 && ay < h2 - 1) {
+        const long pl = f * w2 * h2;
+        const float Gx = __ldg(gxi + pl + (long)ay * w2 + ax + 1);
+        const float Gy = __ldg(gyi + pl + (long)(ay + 1) * w2 + ax);
+        const float n2 = Gx * Gx + Gy * Gy;
+        if (n2 > 0.f) {
+            const float inv = rsqrtf(n2);
+            u = make_float2(Gx * inv, Gy * inv);
+        }
+    }
+    const int xp = ax + padx;  // padx is even: same parity as ax
+    U[(f * H2p + ay + pady) * W2p + (xp & 1) * (W2p / 2) + (xp >> 1)] = u;
+}
+
+// Sum of weights over each output pixel's in-range taps (the reference's sum of w, in its tap
+// order), once per handle: it depends on the pixel's phase and on how close it is to the edges.
+__global__ void wsum2d_kernel(BicTables t, int w, int h, int M, float* __restrict__ out) {
+    const int WM = w * M, HM = h * M;
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long)WM * HM) return;
+    const int yM = (int)(idx / WM), xM = (int)(idx - (long)yM * WM);
+    const int qx = xM / M, qy = yM / M;
+    const int phase = (yM % M) * M + xM % M;
+    float ws = 0.f;
+    for (int k = t.start[phase]; k < t.start[phase + 1]; ++k) {
+        const int2 s = t.node[k];
+        const int ax = 2 * qx + s.x, ay = 2 * qy + s.y;
+        if (ax < 0 || ax > 2 * w - 2 || ay < 0 || ay > 2 * h - 2) continue;
+        ws += t.tw[k];
+    }
+    out[idx] = ws;
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    // 8-byte asynchronous copy; valid = false writes zeros and reads nothing
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(valid ? 8 : 0)
+                 : "memory");
+}
+
+// One thread per output pixel; a CTA is 32 x 8 input cells of one sub-pixel phase, so the whole
+// CTA walks the same tap list (broadcast from shared memory).  Per frame the CTA's slab of the
+// unit-gradient field (its 8 cell rows' 2x-grid rows plus the tap reach, both parity halves of
+// its 32 cell columns plus the reach) is copied with cp.async into one of two buffers while the
+// taps of the previous frame run.  Per tap: inward test g . d < 0, then Dk w = w - (w / d) |g x d|
+// (liveSRRF.cl:293-339 with the gradient normalised once per node; a zero gradient is never
+// inward, where the reference's NaN guard gives Dk = 0).  Sum of weights from the per-pixel
+// table; intensity, cumulants and the (n - 1) bookkeeping as bic_rgc_kernel.  A launch's frames
+// are summed in FP32 and folded into the block's FP64 accumulators once.
+__global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
+    extern __shared__ float4 smb[];
+    const int M = a.M;
+    const int lp = blockIdx.z, px = lp % M, py = lp / M;
+    const int t0 = a.tab.start[lp], n = a.tab.start[lp + 1] - t0;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int row2 = 2 * a.tab.sl_nx;        // float2s per slab row
+    const int slab = a.tab.sl_rows * row2;   // float2s per slab
+    float4* stab = smb;                                                   // [max_taps]
+    float* sw = reinterpret_cast<float*>(smb + a.tab.max_taps);          // [max_taps]
+    float2* sbuf = reinterpret_cast<float2*>(smb + a.tab.max_taps + (a.tab.max_taps + 3) / 4);  // [2][slab]
+    for (int i = tid; i < n; i += 256) {
+        stab[i] = a.tab.tab[t0 + i];
+        sw[i] = a.tab.tw[t0 + i];
+    }
+    const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
+    const bool valid = qx_raw < a.w && qy_raw < a.h;
+    const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
+    const int xM = qx * M + px, yM = qy * M + py;
+    const int WM = a.w * M;
+    const long pix = (long)yM * WM + xM;
+    const long whM = (long)WM * a.h * M;
+    const long fstride = (long)a.tab.H2p * a.tab.W2p;
+    const long pl = (long)a.w * a.h;
+    const int half = a.tab.W2p / 2;
+    const int row0 = 16 * blockIdx.y + a.tab.pady + a.tab.sl_symin;
+    const int cin0 = a.tab.padx / 2 + 32 * blockIdx.x + a.tab.sl_fxmin;
+    const int tbase = 2 * threadIdx.y * row2 + threadIdx.x;  // this thread's cell in the slab
+    const float xs = (float)xM / (float)M - 0.5f, ys = (float)yM / (float)M - 0.5f;
+    const float wsum = a.tab.wsum[pix];
+    float prev = valid ? a.st.prev[pix] : 0.f;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    const int st_ly = tid / row2, st_rem = tid - st_ly * row2;
+    const int st_dly = 256 / row2, st_drem = 256 - st_dly * row2;
+    // slab of frame f into buffer f & 1; element i = tid + 256 k at (row ly, position rem)
+    // advanced without divisions
+    auto stage = [&](int f) {
+        const float2* Uf = a.U + f * fstride;
+        float2* dst = sbuf + (f & 1) * slab;
+        int ly = st_ly, rem = st_rem;
+        for (int i = tid; i < slab; i += 256) {
+            const int par = rem >= a.tab.sl_nx ? 1 : 0, lx = rem - par * a.tab.sl_nx;
+            const int row = row0 + ly, cin = cin0 + lx;
+            const bool in = row < a.tab.H2p && cin < half;
+            cp_async8(dst + i, in ? (const void*)(Uf + (long)row * a.tab.W2p + par * half + cin) : (const void*)a.U, in);
+            ly += st_dly;
+            rem += st_drem;
+            if (rem >= row2) {
+                rem -= row2;
+                ++ly;
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (a.F > 0) stage(0);
+    for (int f = 0; f < a.F; ++f) {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // slab f landed everywhere; buffer (f + 1) & 1 is no longer read
+        if (f + 1 < a.F) stage(f + 1);
+        const float2* sl = sbuf + (f & 1) * slab + tbase;
+        float cg = 0.f;
+        for (int t = 0; t < n; ++t) {
+            const float4 e = stab[t];
+            const float2 u = sl[__float_as_int(e.x)];
+            const float dot = fmaf(u.x, e.y, u.y * e.z);
+            if (dot < 0.f) {
+                const float cr = fmaf(u.y, e.y, -u.x * e.z);  // gy dx - gx dy
+                cg += fmaf(-fabsf(cr), e.w, sw[t]);
+            }
+        }
+        const float c = cglh_power(cg / wsum, a.sens);
+        const float v = sample2d(a.fraw + f * pl, a.w, a.h, xs, ys);
+        const float x = a.int_weighting ? v * c : c;
+        s0 += x;
+        s1 = fmaf(x, x, s1);
+        if (a.t0 + f > 0) s2 = fmaf(x, prev, s2);
+        s3 += v;
+        prev = x;
+    }
+    if (!valid) return;
+    a.st.acc[pix] += (double)s0;
+    a.st.acc[whM + pix] += (double)s1;
+    a.st.acc[2 * whM + pix] += (double)s2;
+    a.st.acc[3 * whM + pix] += (double)s3;
+    a.st.prev[pix] = prev;
+}
+
 }  // namespace
+
+cudaError_t bic_tables_build(const BicGeometry& g, int M, int w, int h, BicTables& t, bool& built,
+                             cudaStream_t stream) {
+    // Tap geometry of bic_rgc_kernel with zero shift, for the pixel of each phase in the first
+    // input cell (Java float arithmetic as the reference: xc = (float)((xM + 0.5) / M)); the
+    // offsets from (kx, ky) and the distances repeat in every cell (exactly so for M a power of
+    // two, whose phase centres are exact in FP32).
+    built = false;
+    const int r0 = -(int)(2.0f * g.radius), r1 = (int)(2.0f * g.radius + 1);
+    struct Tap {
+        int sx, sy;
+        float dx, dy, d, wt;
+    };
+    std::vector<Tap> taps;
+    std::vector<int> start(M * M + 1, 0);
+    int sxmin = 0, sxmax = 0, symin = 0, symax = 0, maxn = 0;
+    for (int py = 0; py < M; ++py)
+        for (int px = 0; px < M; ++px) {
+            const int phase = py * M + px;
+            start[phase] = (int)taps.size();
+            const float xc = (float)(((double)px + 0.5) / M);
+            const float yc = (float)(((double)py + 0.5) / M);
+            const int kx = (int)(2.0f * xc), ky = (int)(2.0f * yc);
+            for (int j = r0; j <= r1; ++j) {
+                const float vy = ((float)ky + (float)j) / 2.0f;
+                for (int i = r0; i <= r1; ++i) {
+                    const float vx = ((float)kx + (float)i) / 2.0f;
+                    const float dx = vx - xc, dy = vy - yc;
+                    const float d = sqrtf(dx * dx + dy * dy);
+                    if (!(d != 0.f && d <= g.tSO)) continue;
+                    float wt = d * expf(-(d * d) / g.tSS);
+                    wt = wt * wt * wt * wt;
+                    const Tap tp{kx + i - 1, ky + j - 1, dx, dy, d, wt};
+                    sxmin = std::min(sxmin, tp.sx);
+                    sxmax = std::max(sxmax, tp.sx);
+                    symin = std::min(symin, tp.sy);
+                    symax = std::max(symax, tp.sy);
+                    taps.push_back(tp);
+                }
+            }
+            maxn = std::max(maxn, (int)taps.size() - start[phase]);
+        }
+    start[M * M] = (int)taps.size();
+    if (taps.empty()) return cudaSuccess;
+    // zero halo: node column ax = 2 qx + sx in [sxmin, 2w - 2 + sxmax], rows likewise
+    t.padx = std::max(-sxmin, std::max(sxmax - 1, 0));
+    t.padx += t.padx & 1;
+    t.pady = std::max(-symin, std::max(symax - 1, 0));
+    t.W2p = 2 * w + 2 * t.padx;
+    t.H2p = 2 * h + 2 * t.pady;
+    const int fxmin = sxmin >> 1, fxmax = sxmax >> 1;
+    t.sl_symin = symin;
+    t.sl_fxmin = fxmin;
+    t.sl_rows = 2 * 7 + symax - symin + 1;
+    t.sl_nx = 31 + fxmax - fxmin + 1;
+    t.max_taps = maxn;
+    t.smem = sizeof(float4) * ((size_t)maxn + (maxn + 3) / 4) + sizeof(float2) * 2 * (size_t)t.sl_rows * 2 * t.sl_nx;
+    if (t.smem > 200 * 1024) return cudaSuccess;
+    std::vector<float4> A;
+    std::vector<float> Wt;
+    std::vector<int2> node;
+    for (const Tap& tp : taps) {
+        const int off = (tp.sy - symin) * 2 * t.sl_nx + (tp.sx & 1) * t.sl_nx + ((tp.sx >> 1) - fxmin);
+        float offf;
+        std::memcpy(&offf, &off, 4);
+        A.push_back(make_float4(offf, tp.dx, tp.dy, tp.wt / tp.d));
+        Wt.push_back(tp.wt);
+        node.push_back(make_int2(tp.sx, tp.sy));
+    }
+    auto up = [](auto** d, const auto& v) -> cudaError_t {
+        cudaError_t e = cudaMalloc((void**)d, sizeof(v[0]) * v.size());
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*d, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice);
+    };
+    cudaError_t e;
+    if ((e = up(&t.tab, A)) != cudaSuccess || (e = up(&t.tw, Wt)) != cudaSuccess ||
+        (e = up(&t.node, node)) != cudaSuccess || (e = up(&t.start, start)) != cudaSuccess)
+        return e;
+    const long total = (long)w * M * h * M;
+    if ((e = cudaMalloc((void**)&t.wsum, sizeof(float) * total)) != cudaSuccess) return e;
+    wsum2d_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(t, w, h, M, t.wsum);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    built = true;
+    return cudaSuccess;
+}
+
+void bic_tables_free(BicTables& t) {
+    cudaFree(t.tab);
+    cudaFree(t.tw);
+    cudaFree(t.node);
+    cudaFree(t.start);
+    cudaFree(t.wsum);
+    t = BicTables();
+}
+
+size_t bic_field_float2s(const BicTables& t, int F) { return (size_t)F * t.H2p * t.W2p; }
+
+cudaError_t unit_grad2d(const float* gxi, const float* gyi, int w, int h, int F, const BicTables& t,
+                        float2* U, cudaStream_t stream) {
+    unit_grad2d_kernel<<<dim3((2 * w + 127) / 128, 2 * h, F), 128, 0, stream>>>(
+        gxi, gyi, w, h, t.padx, t.pady, t.W2p, t.H2p, U);
+    return cudaGetLastError();
+}
+
+cudaError_t bic_rgc_tab(const BicTabArgs& a, cudaStream_t stream) {
+    if (!a.tab.tab || a.tab.smem > 200 * 1024) return cudaErrorInvalidValue;
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && !(configured & (1ull << dev))) {
+        if ((e = cudaFuncSetAttribute(bic_tab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024)) != cudaSuccess)
+            return e;
+        configured |= 1ull << dev;
+    }
+    const dim3 grid((a.w + 31) / 32, (a.h + 7) / 8, a.M * a.M);
+    bic_tab_kernel<<<grid, dim3(32, 8), a.tab.smem, stream>>>(a);
+    return cudaGetLastError();
+}
 
 cudaError_t bic_prepare(const void* raw, int is_u16, int w, int h, int F, float* fraw, float* gx,
                         float* gy, float* gxi, float* gyi, cudaStream_t stream) {

@@ -11,12 +11,12 @@ TOL = 1e-4
 
 
 def run(esrrf, frames, M, fwhm, S, intw=True, mp=True, fht=False, calib=None, drift=None,
-        frames_per_launch=0, chunks=None):
+        frames_per_launch=0, chunks=None, kernel="fused"):
     eng = esrrf.LiveSRRF_CL()
     n = frames.shape[0]
     eng.initialise(frames.shape[-1], frames.shape[-2], M, fwhm, S, n, n, intWeighting=intw,
                    doMPmapCorrection=mp, doFHTinterpolation=fht, calibTable3DSRRF=calib,
-                   framesPerLaunch=frames_per_launch)
+                   framesPerLaunch=frames_per_launch, kernel=kernel)
     try:
         eng.resetFramePosition()
         if drift is not None:
@@ -74,6 +74,36 @@ def test_bic_chunked_u16(esrrf_mod, oracle_mod):
     ref = oracle_mod.bic_block(raw.astype(np.float32), 3, 1.5, 2)
     got, _ = run(esrrf_mod, raw, 3, 1.5, 2, chunks=[4, 4, 3], frames_per_launch=3)
     assert_close(got, ref, "bic chunked")
+
+
+@pytest.mark.parametrize("M,fwhm,S", [(2, 1.0, 1), (3, 2.5, 2), (4, 1.5, 2), (5, 2.0, 1),
+                                      (8, 1.5, 1), (4, 4.0, 1)])
+def test_bic_tabulated_taps_radii(esrrf_mod, oracle_mod, M, fwhm, S):
+    """The tabulated bicubic kernel (launches without drift: per-phase tap lists, per-pixel sums
+    of weights at the edges, slab staging, CTAs that overhang a 37 x 29 frame) across
+    magnifications -- odd M, whose phase centres are not exact in FP32, included -- and radii,
+    against the oracle and against the per-pixel kernel (kernel="plain")."""
+    from esrrf import synth
+    raw = synth.small_stack(60 + M, 6, 29, 37)
+    ref = oracle_mod.bic_block(raw.astype(np.float32), M, fwhm, S)
+    got, _ = run(esrrf_mod, raw, M, fwhm, S)
+    assert_close(got, ref, f"bic tabulated M{M} r{fwhm}")
+    plain, _ = run(esrrf_mod, raw, M, fwhm, S, kernel="plain")
+    assert_close(got, plain, f"bic tabulated vs per-pixel M{M} r{fwhm}")
+
+
+def test_bic_drift_uses_per_pixel_kernel(esrrf_mod, oracle_mod):
+    """A launch with drift takes the per-pixel kernel (the tap geometry then moves per frame);
+    the launch without drift after it the tabulated one; both against the oracle."""
+    from esrrf import synth
+    raw = synth.small_stack(77, 8, 32, 40).astype(np.float32)
+    dx = np.zeros(8, np.float32)
+    dy = np.zeros(8, np.float32)
+    dx[:4] = np.linspace(0.0, 0.3, 4)
+    dy[:4] = np.linspace(0.1, -0.2, 4)
+    ref = oracle_mod.bic_block(raw, 4, 1.5, 2, drift_x=dx, drift_y=dy)
+    got, _ = run(esrrf_mod, raw, 4, 1.5, 2, drift=(dx, dy), frames_per_launch=4)
+    assert_close(got, ref, "bic drift then none")
 
 
 @pytest.mark.parametrize("name", golden_names("3d"))
