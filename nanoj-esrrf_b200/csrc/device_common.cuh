@@ -61,6 +61,61 @@ __device__ __forceinline__ float sample2d(const float* __restrict__ a, int w, in
     return lower + yf * (upper - lower);
 }
 
+// sample2d split into the part that depends only on the position (support, interior test,
+// Catmull-Rom weights) and the part that reads the image, for a position sampled in many frames;
+// same arithmetic and accumulation order as sample2d.
+struct Sample2dAt {
+    bool interior;
+    int o;               // interior: offset of (u0 - 1, v0 - 1); else of (xb, yb)
+    float cx[4], cy[4];  // interior: weights of columns u0 - 1 .. u0 + 2 and rows; else cx[0] = xf, cy[0] = yf
+};
+
+__device__ __forceinline__ Sample2dAt sample2d_at(int w, int h, float x, float y) {
+    Sample2dAt s;
+    const int u0 = (int)floorf(x);
+    const int v0 = (int)floorf(y);
+    s.interior = u0 > 0 && u0 < w - 2 && v0 > 0 && v0 < h - 2;
+    if (s.interior) {
+        // the clamps of sample2d are no-ops inside the interior support
+        s.o = (v0 - 1) * w + (u0 - 1);
+#pragma unroll
+        for (int i = 0; i <= 3; i++) {
+            s.cx[i] = cubic(x - (float)(u0 - 1 + i));
+            s.cy[i] = cubic(y - (float)(v0 - 1 + i));
+        }
+    } else {
+        const int xb = (int)fminf((float)w - 2, fmaxf(x, 0.0f));
+        const int yb = (int)fminf((float)h - 2, fmaxf(y, 0.0f));
+        s.o = yb * w + xb;
+        s.cx[0] = x - (float)xb;
+        s.cy[0] = y - (float)yb;
+#pragma unroll
+        for (int i = 1; i <= 3; i++) s.cx[i] = s.cy[i] = 0.0f;
+    }
+    return s;
+}
+
+__device__ __forceinline__ float sample2d_apply(const float* __restrict__ a, int w, const Sample2dAt& s) {
+    const float* r = a + s.o;
+    if (s.interior) {
+        float q = 0.0f;
+#pragma unroll
+        for (int j = 0; j <= 3; j++) {
+            float p = 0.0f;
+#pragma unroll
+            for (int i = 0; i <= 3; i++) p = p + __ldg(r + (long)j * w + i) * s.cx[i];
+            q = q + p * s.cy[j];
+        }
+        return q;
+    }
+    const float xf = s.cx[0], yf = s.cy[0];
+    const float ll = __ldg(r), lr = __ldg(r + 1);
+    const float ur = __ldg(r + w + 1), ul = __ldg(r + w);
+    const float upper = ul + xf * (ur - ul);
+    const float lower = ll + xf * (lr - ll);
+    return lower + yf * (upper - lower);
+}
+
 // sample2d at one position (x, y) of four planes a + plane[k] * pl: the support, the branch and the
 // 4 x 4 cubic weights are shared, each plane keeps sample2d's own accumulation order.
 __device__ __forceinline__ void sample2d_x4(const float* __restrict__ a, long pl, const int (&plane)[4],

@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
     const int row0 = 16 * blockIdx.y + a.tab.pady + a.tab.sl_symin;
     const int cin0 = a.tab.padx / 2 + 32 * blockIdx.x + a.tab.sl_fxmin;
     const int tbase = 2 * threadIdx.y * row2 + threadIdx.x;  // this thread's cell in the slab
-    const float xs = (float)xM / (float)M - 0.5f, ys = (float)yM / (float)M - 0.5f;
+    // the intensity is sampled at the same position in every frame
+    const dev::Sample2dAt sp = dev::sample2d_at(a.w, a.h, (float)xM / (float)M - 0.5f, (float)yM / (float)M - 0.5f);
     const float wsum = a.tab.wsum[pix];
     float prev = valid ? a.st.prev[pix] : 0.f;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
@@ -289,13 +290,13 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
             const float4 e = stab[t];
             const float2 u = sl[__float_as_int(e.x)];
             const float dot = fmaf(u.x, e.y, u.y * e.z);
-            if (dot < 0.f) {
-                const float cr = fmaf(u.y, e.y, -u.x * e.z);  // gy dx - gx dy
-                cg += fmaf(-fabsf(cr), e.w, sw[t]);
-            }
+            // the term is computed for every tap so that only the add depends on the inward test
+            const float cr = fmaf(u.y, e.y, -u.x * e.z);  // gy dx - gx dy
+            const float term = fmaf(-fabsf(cr), e.w, sw[t]);
+            if (dot < 0.f) cg += term;
         }
         const float c = cglh_power(cg / wsum, a.sens);
-        const float v = sample2d(a.fraw + f * pl, a.w, a.h, xs, ys);
+        const float v = dev::sample2d_apply(a.fraw + f * pl, a.w, sp);
         const float x = a.int_weighting ? v * c : c;
         s0 += x;
         s1 = fmaf(x, x, s1);
