@@ -270,7 +270,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md"}
+TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md", "rgc_fused_bic512": "rgc_bic_bic512.md"}
 
 
 def read_traffic_summary(kernel, key="traffic_bytes_per_launch"):

@@ -75,7 +75,8 @@ typedef struct {
     int fht_scale;        /* esrrf_fht_scale */
     int kernel;           /* 0: fused tile kernel where applicable, 1: plain per-pixel kernel */
     int frames_per_launch;/* frames per interpolation + RGC launch; 0: the block in equal launches of
-                             at most 50 frames (FHT path, within ~4 GB of frame buffers), else 8 */
+                             at most 50 frames (FHT path, within ~4 GB of frame buffers) or 32
+                             (2-D bicubic path, within ~2 GB), 8 timepoints in 3-D */
     /* 3-D calibration, all arrays of length n_planes (NULL in 2-D). */
     int n_planes;
     const float* roi;

@@ -128,6 +128,15 @@ esrrf_status esrrf_handle::init(const esrrf_params& params) {
         const int nb = std::max(1, p.n_frame_for_srrf);
         const int launches = (nb + fmax - 1) / fmax;
         F = (nb + launches - 1) / launches;
+    } else if (p.frames_per_launch == 0 && mode == Mode::kBIC) {
+        // 2-D bicubic path: likewise at most 32 frames (100-frame blocks of 512 x 512 at M4: 4 %
+        // faster than 8), within ~2 GB of per-frame buffers (raw frame and its gradients, the 2x
+        // gradients and the padded unit-gradient field: ~19 input planes)
+        const double per_frame = 19.0 * sizeof(float) * (double)p.width * p.height;
+        const int fmax = (int)std::max(1.0, std::min(32.0, 2e9 / per_frame));
+        const int nb = std::max(1, p.n_frame_for_srrf);
+        const int launches = (nb + fmax - 1) / fmax;
+        F = (nb + launches - 1) / launches;
     }
 
     if (mode == Mode::kFHT) return init_fht();

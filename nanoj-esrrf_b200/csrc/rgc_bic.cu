@@ -227,7 +227,9 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid
 __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
     extern __shared__ float4 smb[];
     const int M = a.M;
-    const int lp = blockIdx.z, px = lp % M, py = lp / M;
+    // phase fastest: the M^2 CTAs that stage the same slab run together and share it through L2
+    const int lp = blockIdx.x, px = lp % M, py = lp / M;
+    const int bx = blockIdx.y, by = blockIdx.z;
     const int t0 = a.tab.start[lp], n = a.tab.start[lp + 1] - t0;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int row2 = 2 * a.tab.sl_nx;        // float2s per slab row
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
         stab[i] = a.tab.tab[t0 + i];
         sw[i] = a.tab.tw[t0 + i];
     }
-    const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
+    const int qx_raw = bx * 32 + threadIdx.x, qy_raw = by * 8 + threadIdx.y;
     const bool valid = qx_raw < a.w && qy_raw < a.h;
     const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
     const int xM = qx * M + px, yM = qy * M + py;
@@ -249,8 +251,8 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
     const long fstride = (long)a.tab.H2p * a.tab.W2p;
     const long pl = (long)a.w * a.h;
     const int half = a.tab.W2p / 2;
-    const int row0 = 16 * blockIdx.y + a.tab.pady + a.tab.sl_symin;
-    const int cin0 = a.tab.padx / 2 + 32 * blockIdx.x + a.tab.sl_fxmin;
+    const int row0 = 16 * by + a.tab.pady + a.tab.sl_symin;
+    const int cin0 = a.tab.padx / 2 + 32 * bx + a.tab.sl_fxmin;
     const int tbase = 2 * threadIdx.y * row2 + threadIdx.x;  // this thread's cell in the slab
     // the intensity is sampled at the same position in every frame
     const dev::Sample2dAt sp = dev::sample2d_at(a.w, a.h, (float)xM / (float)M - 0.5f, (float)yM / (float)M - 0.5f);
@@ -430,7 +432,8 @@ cudaError_t bic_rgc_tab(const BicTabArgs& a, cudaStream_t stream) {
             return e;
         configured |= 1ull << dev;
     }
-    const dim3 grid((a.w + 31) / 32, (a.h + 7) / 8, a.M * a.M);
+    if ((a.w + 31) / 32 > 65535 || (a.h + 7) / 8 > 65535) return cudaErrorInvalidValue;
+    const dim3 grid(a.M * a.M, (a.w + 31) / 32, (a.h + 7) / 8);
     bic_tab_kernel<<<grid, dim3(32, 8), a.tab.smem, stream>>>(a);
     return cudaGetLastError();
 }
