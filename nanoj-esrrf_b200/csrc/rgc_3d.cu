@@ -468,7 +468,10 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
     extern __shared__ float4 sm4[];
     constexpr int M = MZ, M2 = MZ * MZ;
     const int es = a.tab.zes, nz = a.tab.znz;
-    const int qz = blockIdx.z / M2, lp = blockIdx.z % M2;
+    // phase fastest: the M^2 CTAs of a cell tile and plane, which stage the same slabs, run together
+    const int lp = blockIdx.x, bx = blockIdx.y;
+    const int nby = (a.h + 7) / 8;
+    const int qz = blockIdx.z / nby, by = blockIdx.z - qz * nby;
     const int px = lp % M, py = lp / M;
     const int t0 = a.tab.zstart[lp], n = a.tab.zstart[lp + 1] - t0;
     const int tid = threadIdx.y * 32 + threadIdx.x;
@@ -484,7 +487,7 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
     }
     for (int i = tid; i <= nz; i += 256) sseg[i] = a.tab.zseg[lp * (nz + 1) + i];
     const float* sf = reinterpret_cast<const float*>(stab);
-    const int qx_raw = blockIdx.x * 32 + threadIdx.x, qy_raw = blockIdx.y * 8 + threadIdx.y;
+    const int qx_raw = bx * 32 + threadIdx.x, qy_raw = by * 8 + threadIdx.y;
     const bool valid = qx_raw < a.w && qy_raw < a.h;
     const int qx = min(qx_raw, a.w - 1), qy = min(qy_raw, a.h - 1);
     const int xM = qx * M + px, yM = qy * M + py;
@@ -493,8 +496,8 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
     const long pl = (long)a.w * a.h;
     const long fstride = (long)a.tab.Pp * a.tab.H2p * a.tab.W2p;
     const int half = a.tab.W2p / 2;
-    const int row0 = 2 * blockIdx.y * 8 + a.tab.pady + a.tab.sl_symin;
-    const int cin0 = a.tab.padx / 2 + blockIdx.x * 32 + a.tab.sl_fxmin;
+    const int row0 = 2 * by * 8 + a.tab.pady + a.tab.sl_symin;
+    const int cin0 = a.tab.padx / 2 + bx * 32 + a.tab.sl_fxmin;
     const int tbase = 2 * threadIdx.y * row2 + threadIdx.x;  // this thread's cell in the slab
     const float pxf = (float)xM / (float)M - 0.5f;
     const float pyf = (float)yM / (float)M - 0.5f;
@@ -633,7 +636,8 @@ cudaError_t launch_zs(const Rgc3dTabArgs& a, cudaStream_t stream) {
             return e;
         configured |= 1ull << dev;
     }
-    const dim3 grid((a.w + 31) / 32, (a.h + 7) / 8, MZ * MZ * a.P);
+    if ((a.w + 31) / 32 > 65535 || (long)((a.h + 7) / 8) * a.P > 65535) return cudaErrorInvalidValue;
+    const dim3 grid(MZ * MZ, (a.w + 31) / 32, ((a.h + 7) / 8) * a.P);
     rgc3d_zs_kernel<MZ><<<grid, dim3(32, 8), smem, stream>>>(a);
     return cudaGetLastError();
 }
