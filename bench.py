@@ -220,6 +220,27 @@ def cpu_reference_sample(stack, M, fwhm, S, n_frames=1, bic=False):
                       f", OpenMP over {cores} threads; {dt:.2f} s"}
 
 
+def cpu_3d_sample(planes, M, fwhm, S, theta, shx, shy, n_tp=2):
+    """Reference 3-D kernels (oracle/_ref, all host cores) on the first `n_tp` timepoints' planes,
+    with MP correction."""
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    pl = np.ascontiguousarray(planes[:n_tp], np.float32)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        O.ref_3d_block(pl, M, fwhm, S, theta, shx, shy, mp_correction=True)
+    else:
+        O.block3d(pl, M, fwhm, S, theta, shx, shy, mp_correction=True)
+    dt = time.perf_counter() - t0
+    n, P, h, w = pl.shape
+    cores = os.cpu_count() or 1
+    return {"value": n * P * h * w / 1e6 / dt, "unit": "Mpx*frames/s", "cores": cores, "kind": kind,
+            "sample": f"{n} timepoint(s) of {P} planes of {w}x{h}, M{M}: "
+                      f"{'reference 3-D kernels compiled for the host' if kind == 'reference' else 'C restatement'}"
+                      f", OpenMP over {cores} threads; {dt:.2f} s"}
+
+
 def path_label(workload):
     return "2-D bicubic path" if workload == "bic512" else "2-D FHT path"
 
@@ -244,6 +265,26 @@ def run_reference(args, world, rank):
                                    "(bounded sample: 20 frames per step)"},
             "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "frames/s"},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    if args.workload == "mfm3d":
+        planes = synth.make_stack("mfm3d", frames=2 * (args.steps + args.warmup))
+        P = planes.shape[1]
+        th = np.linspace(-0.5, 0.5, P).astype(np.float32)
+        shx = np.linspace(-0.2, 0.2, P).astype(np.float32)
+        shy = np.linspace(0.1, -0.1, P).astype(np.float32)
+        vals = [cpu_3d_sample(planes[2 * i:2 * i + 2], 3, 1.5, 1, th, shx, shy, 2)
+                for i in range(args.warmup + args.steps)][args.warmup:]
+        v = statistics.median([r["value"] for r in vals])
+        print(json.dumps({
+            "impl": "reference", "metric": "input Mpx*frames/s (eSRRF 3-D MFM path)", "value": v,
+            "unit": "Mpx*frames/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * 2 * P * planes.shape[2] * planes.shape[3] / 1e6 / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"mfm3d: {P} planes of 128x128 x 200 timepoints, M3, radius 1.5, S1, "
+                                   "MP correction (bounded sample: 2 timepoints per step)"},
+            "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "Mpx*frames/s"},
+            "e2e": {"value": v, "unit": "Mpx*frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     bic = args.workload == "bic512"
     per = 2 if bic else 1  # frames per sample (the bicubic path's TAC2 divides by n - 1)
@@ -716,12 +757,18 @@ def run_3d(args, world, rank, local):
     launches[0] = 0
     barrier(world)
     torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
+        # the engine's calls return only after their own stream drained, so events on the current
+        # stream bracket all of the device work
+        ev0.record(stream)
         for _ in range(args.steps):
             step()
+        ev1.record(stream)
         torch.cuda.synchronize()
-        t_step = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
+    barrier(world)
+    t_step = max_over_ranks(world, ev0.elapsed_time(ev1) / 1000.0 / args.steps)
     h_cam = torch.from_numpy(cam.view(np.int16)).pin_memory()
     h_out = torch.empty((4 * P * M, h * M, w * M), dtype=torch.float32).pin_memory()
     t0 = time.perf_counter()
@@ -733,6 +780,11 @@ def run_3d(args, world, rank, local):
     if rank != 0:
         return
     mpxf = n * P * h * w / 1e6
+    th = np.asarray(calib["Theta (degrees)"], np.float32)
+    shx = np.asarray(calib["X-shift (pixels)"], np.float32)
+    shy = np.asarray(calib["Y-shift (pixels)"], np.float32)
+    cpu = (cpu_3d_sample(planes, M, fwhm, S, th, shx, shy, 2)
+           if not args.no_cpu_baseline and world == 1 else None)
     print(json.dumps({
         "metric": "input Mpx*frames/s (eSRRF 3-D MFM path)", "value": world * mpxf / t_step,
         "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -747,7 +799,7 @@ def run_3d(args, world, rank, local):
                   "plain_1_timepoint_per_launch_mpx_frames_s": mpxf / (plain_ms / 1e3) if plain_ms else None},
         "e2e": {"value": mpxf / e2e, "unit": "Mpx*frames/s", "h2d_bytes_per_step": int(cam.nbytes),
                 "d2h_bytes_per_step": int(h_out.numel() * 4)},
-        "gpu_launches": launches[0] // max(1, args.steps), "clocks": clk.summary()}))
+        "gpu_launches": launches[0], "clocks": clk.summary(), "cpu_baseline": cpu}))
 
 
 def drift_cpu_sample(stack, n):
