@@ -241,6 +241,42 @@ def cpu_3d_sample(planes, M, fwhm, S, theta, shx, shy, n_tp=2):
                       f", OpenMP over {cores} threads; {dt:.2f} s"}
 
 
+def cpu_sweep_sample(stack):
+    """Reference kernels (oracle/_ref, all host cores) of the sweep: per magnification, the Fourier
+    interpolation of one frame (numpy FFT) and the RGC block of that frame at the largest radius,
+    each timed; the RGC time is scaled to every radius by its tap count and every combination costs
+    its blocks' frame evaluations (ParametersSweep_ runs each combination through the engine)."""
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    raw = np.ascontiguousarray(stack[:1], np.float32)
+    evals = sum(length for _, length in SWEEP_BLOCKS)  # (start, length) pairs
+    rmax = max(SWEEP_RADII)
+    total = 0.0
+    spent = 0.0
+    for M in SWEEP_MAGS:
+        t0 = time.perf_counter()
+        interp = O.fht_interpolate_fft(raw, M)
+        t1 = time.perf_counter()
+        if kind == "reference":
+            O.ref_fht_block(interp, M, rmax, 1)
+        else:
+            O.fht_block(interp, M, rmax, 1)
+        t2 = time.perf_counter()
+        spent += t2 - t0
+        per_tap = (t2 - t1) / taps_per_pixel(M, rmax)
+        for r in SWEEP_RADII:
+            total += len(SWEEP_SENS) * evals * ((t1 - t0) + per_tap * taps_per_pixel(M, r))
+    combos = len(SWEEP_MAGS) * len(SWEEP_RADII) * len(SWEEP_SENS)
+    cores = os.cpu_count() or 1
+    return {"value": combos / total, "unit": "combos/s", "cores": cores, "kind": kind,
+            "sample": f"1 frame of {raw.shape[2]}x{raw.shape[1]} per magnification {list(SWEEP_MAGS)} at radius "
+                      f"{rmax}: numpy-FFT interpolation + "
+                      f"{'reference kernels compiled for the host' if kind == 'reference' else 'C restatement'}"
+                      f", OpenMP over {cores} threads ({spent:.2f} s), scaled by tap count to the "
+                      f"{combos} combinations x {evals} frame evaluations"}
+
+
 def path_label(workload):
     return "2-D bicubic path" if workload == "bic512" else "2-D FHT path"
 
@@ -265,6 +301,26 @@ def run_reference(args, world, rank):
                                    "(bounded sample: 20 frames per step)"},
             "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "frames/s"},
             "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    if args.workload == "adjoint256":
+        print(json.dumps({"impl": "reference", "unavailable": "the fidelity loss and its adjoint are a new "
+                          "objective with no reference implementation (the reference scores sweeps with "
+                          "ErrorMapLiveSRRF on the CPU, not a differentiable loss)"}))
+        return
+    if args.workload == "sweep256":
+        stack = synth.make_stack("sweep256", frames=2)
+        vals = [cpu_sweep_sample(stack) for _ in range(args.warmup + args.steps)][args.warmup:]
+        v = statistics.median([r["value"] for r in vals])
+        print(json.dumps({
+            "impl": "reference", "metric": "sweep combos/s (batched, one CUDA graph)", "value": v,
+            "unit": "combos/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * len(SWEEP_MAGS) * len(SWEEP_RADII) * len(SWEEP_SENS) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "sweep256: 256x256x200, 88 combinations, blocks [0,37) [37,101) "
+                                   "[101,200) [0,100) (bounded sample, tap-count scaled)"},
+            "cpu_baseline": {k: vals[-1][k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "combos/s"},
+            "e2e": {"value": v, "unit": "combos/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     if args.workload == "mfm3d":
         planes = synth.make_stack("mfm3d", frames=2 * (args.steps + args.warmup))
