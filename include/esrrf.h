@@ -199,10 +199,13 @@ esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* r
  * Replaces the per-combination loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519:
  * initialise + resetFramePosition + calculateSRRF + readSRRFbuffer for every radius x
  * sensitivity) and the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:
- * 276-389), on the 2-D FHT path with zero drift.  All frames are interpolated once per
- * magnification and the RGC tap loop runs once per (magnification, radius) for all
- * sensitivities and blocks; the whole sweep is one captured CUDA graph replayed per run.
- * Blocks are arbitrary [start, start + length) frame ranges (uneven and overlapping allowed). */
+ * 276-389), on the 2-D FHT path or the 2-D bicubic path (the sweep's "Use FHT interpolation"
+ * option, gui/ParametersSweep_.java:879), with zero drift.  All frames are interpolated (FHT) or
+ * their gradients resampled (bicubic) once, and the RGC tap loop runs once per (magnification,
+ * radius) for all sensitivities and blocks; the whole sweep is one captured CUDA graph replayed
+ * per run.  Blocks are arbitrary [start, start + length) frame ranges (uneven and overlapping
+ * allowed).  The bicubic sweep applies the MP correction to every output, as the reference's
+ * sweep initialises the engine with it on (gui/ParametersSweep_.java:410). */
 typedef struct {
     int width, height, n_frames;
     int n_mag;
@@ -216,6 +219,7 @@ typedef struct {
     const int* block_length;
     int int_weighting;
     int device;                /* CUDA ordinal; -1 = device 0 */
+    int interp;                /* esrrf_interp: ESRRF_INTERP_FHT or ESRRF_INTERP_BIC */
 } esrrf_sweep_params;
 
 typedef struct esrrf_sweep esrrf_sweep;

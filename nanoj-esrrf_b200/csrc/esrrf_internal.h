@@ -206,6 +206,10 @@ struct BicTabArgs {
     int int_weighting;
     BicTables tab;
     BlockState st;
+    // per-frame mode (the sweep): CGLH / sum of weights and the intensity of every frame,
+    // [F][hM][wM] each, instead of the block's cumulants
+    float* cg_out;
+    float* v_out;
 };
 // unit gradient (Gx read at x + 1, Gy at y + 1 of the 2x grid) into the interior of the padded
 // field; zero at the last column and row, which no tap reads.  The halo is zeroed once, when the

@@ -257,7 +257,8 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
     // the intensity is sampled at the same position in every frame
     const dev::Sample2dAt sp = dev::sample2d_at(a.w, a.h, (float)xM / (float)M - 0.5f, (float)yM / (float)M - 0.5f);
     const float wsum = a.tab.wsum[pix];
-    float prev = valid ? a.st.prev[pix] : 0.f;
+    const bool emit = a.cg_out != nullptr;
+    float prev = valid && !emit ? a.st.prev[pix] : 0.f;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
     const int st_ly = tid / row2, st_rem = tid - st_ly * row2;
     const int st_dly = 256 / row2, st_drem = 256 - st_dly * row2;
@@ -297,8 +298,15 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
             const float term = fmaf(-fabsf(cr), e.w, sw[t]);
             if (dot < 0.f) cg += term;
         }
-        const float c = cglh_power(cg / wsum, a.sens);
         const float v = dev::sample2d_apply(a.fraw + f * pl, a.w, sp);
+        if (emit) {
+            if (valid) {
+                a.cg_out[(long)f * whM + pix] = cg / wsum;
+                a.v_out[(long)f * whM + pix] = v;
+            }
+            continue;
+        }
+        const float c = cglh_power(cg / wsum, a.sens);
         const float x = a.int_weighting ? v * c : c;
         s0 += x;
         s1 = fmaf(x, x, s1);
@@ -306,7 +314,7 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
         s3 += v;
         prev = x;
     }
-    if (!valid) return;
+    if (!valid || emit) return;
     a.st.acc[pix] += (double)s0;
     a.st.acc[whM + pix] += (double)s1;
     a.st.acc[2 * whM + pix] += (double)s2;

@@ -10,6 +10,11 @@
 //   per (sensitivity group, block group): one memory-bound launch that raises CGLH to the
 //     sensitivity, weights it by the interpolated intensity and reduces AVG/VAR/TAC2/INT over each
 //     block, FP64 accumulators in registers.
+// The bicubic sweep (the reference sweep with "Use FHT interpolation" off) computes the 2-point
+// gradients, their 2x resampling and the unit-gradient field of every frame once (none depends on
+// the magnification or radius); per (magnification, radius) the tabulated bicubic RGC writes
+// CGLH / sum of weights and the bicubic intensity of every frame; the cumulant launches apply the
+// path's double (n - 1) division of TAC2, and every output gets the MP correction.
 // Output: for each magnification, radius, sensitivity and block, the four [HM][WM] slices of
 // readSRRFbuffer (AVG, VAR, TAC2, INT; NaN -> 0).
 #include <string.h>
@@ -38,6 +43,7 @@ struct CumArgs {
     float sens[kSG];
     int ns;
     int int_weighting;
+    int tac_div2;      // bicubic path: TAC2 divided by (n - 1) twice (liveSRRF.cl:374,377)
     float* out;        // base of this (magnification, radius): [nS][nB][4][P]
     int s0, b0, nB;    // global indices of the first sensitivity and block of the launch
 };
@@ -88,7 +94,8 @@ __global__ void __launch_bounds__(256) sweep_cumulants_kernel(CumArgs a) {
             if (b >= a.nb) break;
             const int n = a.len[b];
             const double avg = acc[s][b][0] / n, av2 = avg * avg;
-            const double tac = n > 1 ? acc[s][b][2] / (n - 1) : 0.0;
+            double tac = n > 1 ? acc[s][b][2] / (n - 1) : 0.0;
+            if (a.tac_div2 && n > 1) tac /= (n - 1);
             float o[4] = {(float)avg, (float)(acc[s][b][1] / n - av2), (float)(tac - av2),
                           (float)(acc[s][b][3] / n)};
             float* dst = a.out + (((long)(a.s0 + s) * a.nB + (a.b0 + b)) * 4) * a.P + pix;
@@ -103,6 +110,8 @@ struct MagPlan {
     InterpPlan plan;
     std::vector<FhtGeometry> geo;       // per radius
     std::vector<FhtFusedTables> tables; // per radius
+    std::vector<BicGeometry> bgeo;      // bicubic sweep: per radius
+    std::vector<BicTables> btab;        // bicubic sweep: per radius (common field padding)
 };
 
 }  // namespace
@@ -119,6 +128,15 @@ struct esrrf_sweep {
     float* d_cg = nullptr;
     void* d_in = nullptr;       // host-input staging on the device
     float* d_outbuf = nullptr;  // host-output staging on the device
+    // bicubic sweep: frames as float, 2-point gradients, 2x gradients, unit-gradient field
+    bool bic = false;
+    float* d_fraw = nullptr;
+    float* d_gx = nullptr;
+    float* d_gy = nullptr;
+    float* d_gxi = nullptr;
+    float* d_gyi = nullptr;
+    float2* d_u2 = nullptr;
+    float* d_mpmap = nullptr;
     std::vector<size_t> offsets;
     size_t total = 0;
     cudaGraph_t graph = nullptr;
@@ -139,6 +157,7 @@ struct esrrf_sweep {
                     std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
     }
     esrrf_status enqueue(const void* frames, int is_u16, float* out);
+    esrrf_status enqueue_bic(const void* frames, int is_u16, float* out);
     void release();
 };
 
@@ -153,6 +172,7 @@ esrrf_status esrrf_sweep::enqueue(const void* frames, int is_u16, float* out) {
     const int T = p.n_frames;
     const size_t fb = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)p.width * p.height;
     int launches = 0;
+    if (bic) return enqueue_bic(frames, is_u16, out);
     for (size_t mi = 0; mi < mp.size(); ++mi) {
         const MagPlan& m = mp[mi];
         const long P = (long)m.plan.WM * m.plan.HM;
@@ -202,6 +222,68 @@ esrrf_status esrrf_sweep::enqueue(const void* frames, int is_u16, float* out) {
     return ESRRF_OK;
 }
 
+esrrf_status esrrf_sweep::enqueue_bic(const void* frames, int is_u16, float* out) {
+    esrrf_sweep* s = this;
+    const int T = p.n_frames, w = p.width, h = p.height;
+    int launches = 0;
+    SK(bic_prepare(frames, is_u16, w, h, T, d_fraw, d_gx, d_gy, d_gxi, d_gyi, stream), "gradients");
+    launches += 3;
+    SK(unit_grad2d(d_gxi, d_gyi, w, h, T, mp[0].btab[0], d_u2, stream), "unit gradient");
+    ++launches;
+    for (size_t mi = 0; mi < mp.size(); ++mi) {
+        const MagPlan& m = mp[mi];
+        const long P = (long)w * m.M * h * m.M;
+        for (size_t ri = 0; ri < radii.size(); ++ri) {
+            BicTabArgs a{};
+            a.U = d_u2;
+            a.fraw = d_fraw;
+            a.w = w;
+            a.h = h;
+            a.M = m.M;
+            a.F = T;
+            a.t0 = 0;
+            a.sens = 1.f;
+            a.int_weighting = p.int_weighting;
+            a.tab = m.btab[ri];
+            a.cg_out = d_cg;
+            a.v_out = d_interp;
+            SK(bic_rgc_tab(a, stream), "RGC");
+            ++launches;
+            float* base = out + offsets[mi * radii.size() + ri];
+            for (int s0 = 0; s0 < (int)sens.size(); s0 += kSG)
+                for (int b0 = 0; b0 < (int)bstart.size(); b0 += kBG) {
+                    CumArgs c{};
+                    c.cg = d_cg;
+                    c.v = d_interp;
+                    c.P = P;
+                    c.nb = std::min(kBG, (int)bstart.size() - b0);
+                    for (int b = 0; b < c.nb; ++b) {
+                        c.start[b] = bstart[b0 + b];
+                        c.len[b] = blen[b0 + b];
+                    }
+                    c.ns = std::min(kSG, (int)sens.size() - s0);
+                    for (int q = 0; q < c.ns; ++q) c.sens[q] = (float)sens[s0 + q];
+                    c.int_weighting = p.int_weighting;
+                    c.tac_div2 = 1;
+                    c.out = base;
+                    c.s0 = s0;
+                    c.b0 = b0;
+                    c.nB = (int)bstart.size();
+                    sweep_cumulants_kernel<<<(unsigned)((P + 255) / 256), 256, 0, stream>>>(c);
+                    SK(cudaGetLastError(), "cumulants");
+                    ++launches;
+                }
+            // MP correction of AVG, VAR and TAC2 of every (sensitivity, block) output
+            for (size_t q = 0; q < sens.size() * bstart.size(); ++q) {
+                SK(mp_correct(base + q * 4 * P, w, h, 1, m.M, 0, d_mpmap, stream), "MP correction");
+                launches += 2;
+            }
+        }
+    }
+    launches_per_run = launches;
+    return ESRRF_OK;
+}
+
 void esrrf_sweep::release() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
@@ -212,7 +294,12 @@ void esrrf_sweep::release() {
     for (auto& m : mp) {
         interp_plan_destroy(m.plan);
         for (auto& t : m.tables) fht_fused_tables_free(t);
+        for (auto& t : m.btab) bic_tables_free(t);
     }
+    for (float* b : {d_fraw, d_gx, d_gy, d_gxi, d_gyi, d_mpmap}) cudaFree(b);
+    cudaFree(d_u2);
+    d_fraw = d_gx = d_gy = d_gxi = d_gyi = d_mpmap = nullptr;
+    d_u2 = nullptr;
     mp.clear();
     cudaFree(scratch.rowT);
     cudaFree(scratch.xs);
@@ -230,6 +317,68 @@ namespace {
 std::mutex g_sweep_mu;
 std::string g_sweep_create_error;
 }  // namespace
+
+// Bicubic sweep set-up: per (magnification, radius) tap tables, all on one unit-gradient field
+// whose zero halo is the widest any table needs; per-frame buffers for the whole stack.
+static esrrf_status sweep_create_bic(esrrf_sweep* s) {
+    const int w = s->p.width, h = s->p.height, T = s->p.n_frames;
+    cudaError_t e;
+    long maxP = 0;
+    int padx = 0, pady = 0;
+    s->total = 0;
+    for (int M : s->mags) {
+        s->mp.emplace_back();
+        MagPlan& m = s->mp.back();
+        m.M = M;
+        const long P = (long)w * M * h * M;
+        maxP = std::max(maxP, P);
+        for (float r : s->radii) {
+            const BicGeometry g = bic_geometry(r, 1);
+            BicTables t;
+            bool built = false;
+            if ((e = bic_tables_build(g, M, w, h, t, built, s->stream)) != cudaSuccess) {
+                bic_tables_free(t);
+                return s->fail_cuda(e, "RGC tables");
+            }
+            if (!built) {
+                bic_tables_free(t);
+                return s->fail(ESRRF_ERR_INVALID, "radius " + std::to_string(r) + " at magnification " +
+                                                      std::to_string(M) + " needs more than 200 KB of shared memory per CTA");
+            }
+            padx = std::max(padx, t.padx);
+            pady = std::max(pady, t.pady);
+            m.bgeo.push_back(g);
+            m.btab.push_back(t);
+            s->offsets.push_back(s->total);
+            s->total += (size_t)s->sens.size() * s->bstart.size() * 4 * P;
+        }
+    }
+    for (auto& m : s->mp)
+        for (auto& t : m.btab) {
+            t.padx = padx;  // even: every table's padx is
+            t.pady = pady;
+            t.W2p = 2 * w + 2 * padx;
+            t.H2p = 2 * h + 2 * pady;
+        }
+    const size_t plane = (size_t)w * h;
+    const size_t field = bic_field_float2s(s->mp[0].btab[0], T);
+    int maxM = 1;
+    for (int M : s->mags) maxM = std::max(maxM, M);
+    if ((e = cudaMalloc(&s->d_fraw, sizeof(float) * T * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_gx, sizeof(float) * T * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_gy, sizeof(float) * T * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_gxi, sizeof(float) * T * 4 * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_gyi, sizeof(float) * T * 4 * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_u2, sizeof(float2) * field)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_mpmap, sizeof(float) * 3 * maxM * maxM)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||
+        (e = cudaMalloc(&s->d_cg, sizeof(float) * (size_t)T * maxP)) != cudaSuccess)
+        return s->fail_cuda(e, "sweep buffers");
+    if ((e = cudaMemsetAsync(s->d_u2, 0, sizeof(float2) * field, s->stream)) != cudaSuccess)  // zero halo
+        return s->fail_cuda(e, "sweep buffers");
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return s->fail_cuda(e, "sync");
+    return ESRRF_OK;
+}
 
 extern "C" {
 
@@ -255,6 +404,7 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
         if (!(sp->radii[i] > 0.f) || sp->radii[i] > 20.f) return reject("radius out of range");
     for (int i = 0; i < sp->n_sens; ++i)
         if (sp->sensitivities[i] < 0 || sp->sensitivities[i] > 64) return reject("sensitivity out of range");
+    if (sp->interp != ESRRF_INTERP_FHT && sp->interp != ESRRF_INTERP_BIC) return reject("unknown interpolation");
 
     esrrf_sweep* s = new esrrf_sweep();
     s->p = *sp;
@@ -287,6 +437,13 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
     if ((e = cudaSetDevice(s->device)) != cudaSuccess) return bail(s->fail_cuda(e, "cudaSetDevice"));
     if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(s->fail_cuda(e, "stream"));
+    if (sp->interp == ESRRF_INTERP_BIC) {
+        s->bic = true;
+        esrrf_status r = sweep_create_bic(s);
+        if (r != ESRRF_OK) return bail(r);
+        *out = s;
+        return ESRRF_OK;
+    }
     long maxP = 0;
     int maxN = 0, maxWM = 0;
     s->total = 0;
@@ -348,6 +505,7 @@ esrrf_status esrrf_sweep_output_layout(const esrrf_sweep* s, size_t* total_float
 
 // Reads every plan's tensor-core failure flag after the stream has drained.
 static esrrf_status sweep_tc_check(esrrf_sweep* s) {
+    if (s->bic) return ESRRF_OK;
     for (auto& m : s->mp) {
         bool failed = false;
         SK(interp_tc_check(m.plan, s->stream, &failed), "interpolation status");

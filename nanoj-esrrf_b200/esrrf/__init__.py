@@ -283,10 +283,12 @@ class Sweep:
     """Batched parameter sweep / rolling analysis (esrrf_sweep_*): every (magnification, radius,
     sensitivity, block) reconstruction of a stack in one captured CUDA graph.  Replaces the
     per-combination engine loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519) and
-    the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:276-389)."""
+    the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:276-389).
+    ``interpolation``: "fht" or "bicubic" (the sweep's "Use FHT interpolation" option; the
+    bicubic sweep applies the MP correction, as the reference's sweep does)."""
 
     def __init__(self, width, height, n_frames, magnifications, radii, sensitivities, blocks,
-                 int_weighting=True, device=-1):
+                 int_weighting=True, device=-1, interpolation="fht"):
         from ._lib import EsrrfSweepParams
 
         self.width, self.height, self.n_frames = int(width), int(height), int(n_frames)
@@ -302,7 +304,8 @@ class Sweep:
                              self.mags.ctypes.data_as(ip), len(self.radii), self.radii.ctypes.data_as(fp),
                              len(self.sens), self.sens.ctypes.data_as(ip), len(self.bstart),
                              self.bstart.ctypes.data_as(ip), self.blen.ctypes.data_as(ip),
-                             int(bool(int_weighting)), int(device))
+                             int(bool(int_weighting)), int(device),
+                             {"fht": 0, "bicubic": 1}[interpolation])
         h = ctypes.c_void_p()
         _lib.check(None, lib().esrrf_sweep_create(ctypes.byref(p), ctypes.byref(h)), sweep=True)
         self._h = h

@@ -92,7 +92,7 @@ class EsrrfSweepParams(ctypes.Structure):
         ("n_sens", ctypes.c_int), ("sensitivities", ctypes.POINTER(ctypes.c_int)),
         ("n_blocks", ctypes.c_int), ("block_start", ctypes.POINTER(ctypes.c_int)),
         ("block_length", ctypes.POINTER(ctypes.c_int)),
-        ("int_weighting", ctypes.c_int), ("device", ctypes.c_int),
+        ("int_weighting", ctypes.c_int), ("device", ctypes.c_int), ("interp", ctypes.c_int),
     ]
 
 

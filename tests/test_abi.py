@@ -29,13 +29,18 @@ def test_library_exports_every_declared_symbol(esrrf_mod):
         assert n in _lib.SIGNATURES, f"{n} has no ctypes signature"
 
 
-def test_params_layout_matches_c():
-    from esrrf import EsrrfParams
+@pytest.mark.parametrize("py_name,c_name", [("EsrrfParams", "esrrf_params"),
+                                             ("EsrrfSweepParams", "esrrf_sweep_params"),
+                                             ("EsrrfSquirrelParams", "esrrf_squirrel_params"),
+                                             ("EsrrfFrcParams", "esrrf_frc_params")])
+def test_params_layout_matches_c(py_name, c_name):
+    from esrrf import _lib
+    EsrrfParams = getattr(_lib, py_name)
     fields = [f for f, _ in EsrrfParams._fields_]
     prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"esrrf.h\"\nint main(){"
-    prog += 'printf("%zu\\n", sizeof(esrrf_params));'
+    prog += f'printf("%zu\\n", sizeof({c_name}));'
     for f in fields:
-        prog += f'printf("%zu\\n", offsetof(esrrf_params, {f}));'
+        prog += f'printf("%zu\\n", offsetof({c_name}, {f}));'
     prog += "return 0;}"
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
