@@ -578,16 +578,24 @@ def run_sweep(args, world, rank, local):
         esrrf._lib.check(sw.handle, L.esrrf_sweep_run_device(sw.handle, ctypes.c_void_p(d_stack.data_ptr()),
                                                             1, ctypes.c_void_p(d_out.data_ptr())), sweep=True)
 
+    def timed(fn, n):
+        # each sweep call returns after its stream drained: events on the current stream bracket it
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(n):
+            fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / 1000.0 / n
+
     for _ in range(args.warmup):
         step()
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            step()
-        torch.cuda.synchronize()
-        t_step = max_over_ranks(world, (time.perf_counter() - t0) / args.steps)
+        t_local = timed(step, args.steps)
+    barrier(world)
+    t_step = max_over_ranks(world, t_local)
     launches = sw.launch_count()
     # e2e: host stack in, host results out
     h_stack = torch.from_numpy(stack.view(np.int16)).pin_memory()
@@ -685,6 +693,22 @@ def run_sweep(args, world, rank, local):
         frc_cpu_per_pair = (time.perf_counter() - t0) / len(SWEEP_MAGS)
     sw.release()
 
+    # the same sweep on the bicubic path (the sweep's "Use FHT interpolation" option off: bicubic
+    # RGC with MP correction), into the same output buffer (same layout)
+    swb = esrrf.Sweep(w, h, n, SWEEP_MAGS, SWEEP_RADII, SWEEP_SENS, SWEEP_BLOCKS, device=local,
+                      interpolation="bicubic")
+    assert swb.total == sw.total
+
+    def step_b():
+        esrrf._lib.check(swb.handle, L.esrrf_sweep_run_device(swb.handle, ctypes.c_void_p(d_stack.data_ptr()),
+                                                             1, ctypes.c_void_p(d_out.data_ptr())), sweep=True)
+
+    for _ in range(max(1, args.warmup)):
+        step_b()
+    t_bic = timed(step_b, args.steps)
+    bic_launches = swb.launch_count()
+    swb.release()
+
     def single_combo_loop(kernel, subset=None):
         """One engine per combination, every block pushed and read back (device frames)."""
         fb = h * w * 2
@@ -727,7 +751,11 @@ def run_sweep(args, world, rank, local):
                          "every 8th combination, fused loop on every 4th, scaled to 88",
         "e2e": {"value": combos / e2e, "unit": "combos/s", "h2d_bytes_per_step": int(stack.nbytes),
                 "d2h_bytes_per_step": int(h_out.numel() * 4)},
-        "gpu_launches": launches, "clocks": clk.summary(),
+        "gpu_launches": launches * args.steps, "clocks": clk.summary(),
+        "bicubic": {"combos_per_s": combos / t_bic, "ms_per_run": t_bic * 1e3,
+                    "launches_per_run": bic_launches,
+                    "what": "the same 88 combinations and 4 blocks on the bicubic path with MP "
+                            "correction, one CUDA graph"},
         "squirrel": {"images": sq_images, "seconds": sq_s, "images_per_s": sq_images / sq_s,
                      "what": "RSE, RSP (Brent-optimised blur sigma, alpha/beta fit) of every AVG, "
                              "VAR and TAC2 reconstruction against its block's INT slice",

@@ -380,12 +380,14 @@ class Sweep:
             pass
 
 
-def rolling(stack, magnification, fwhm, sensitivity, blocks, int_weighting=True):
-    """Rolling analysis over arbitrary (start, length) blocks, each frame interpolated and run
-    through the RGC once: {(start, length): [4][HM][WM]}."""
+def rolling(stack, magnification, fwhm, sensitivity, blocks, int_weighting=True,
+            interpolation="fht"):
+    """Rolling analysis over arbitrary (start, length) blocks, each frame interpolated (or its
+    gradients resampled, ``interpolation="bicubic"``) and run through the RGC once:
+    {(start, length): [4][HM][WM]}."""
     a = np.asarray(stack)
     sw = Sweep(a.shape[-1], a.shape[-2], a.shape[0], [magnification], [fwhm], [sensitivity],
-               blocks, int_weighting)
+               blocks, int_weighting, interpolation=interpolation)
     try:
         res = sw.run(a)
         return {k[3]: v.copy() for k, v in res.items()}

@@ -72,3 +72,23 @@ def test_bicubic_sweep_matches_per_block_oracle(esrrf_mod, oracle_mod):
             np.testing.assert_array_equal(again[key], res[key])
     finally:
         sw.release()
+
+
+def test_bicubic_rolling_matches_engine_blocks(esrrf_mod):
+    """Rolling analysis on the bicubic path equals running the engine (bicubic, MP correction)
+    block by block."""
+    from esrrf import synth
+    raw = synth.small_stack(54, 30, 24, 40)
+    blocks = [(0, 11), (11, 19), (5, 20)]
+    res = esrrf_mod.rolling(raw, 4, 1.5, 2, blocks, interpolation="bicubic")
+    for (st, ln) in blocks:
+        eng = esrrf_mod.LiveSRRF_CL()
+        eng.initialise(40, 24, 4, 1.5, 2, ln, ln, doMPmapCorrection=True, doFHTinterpolation=False)
+        try:
+            eng.resetFramePosition()
+            assert not eng.calculateSRRF(raw[st:st + ln])
+            ref = eng.readSRRFbuffer().copy()
+        finally:
+            eng.release()
+        for k in range(4):
+            assert rel_err(res[(st, ln)][k], ref[k]) < TOL, (st, ln, k)
