@@ -49,3 +49,43 @@ def test_async_reads_match_sync(esrrf_mod, pinned):
     for b in range(5):
         np.testing.assert_array_equal(outs[b], want[b])
     np.testing.assert_array_equal(again, want[0])
+
+
+def test_async_reads_bicubic_mp_correction(esrrf_mod):
+    """Queued read-backs on the bicubic path: the MP correction runs inside each queued read, so
+    five blocks read through two slots equal synchronous reads bit for bit, and the MP maps read
+    after the last queued block are that block's."""
+    import torch
+    from esrrf import synth
+    stack = synth.small_stack(5, 30, 40, 56)  # 5 blocks of 6 frames
+    M, nf = 4, 6
+
+    def engine():
+        e = esrrf_mod.LiveSRRF_CL()
+        e.initialise(56, 40, M, 1.5, 2, nf, nf, doMPmapCorrection=True, doFHTinterpolation=False)
+        return e
+
+    want, maps = [], None
+    eng = engine()
+    try:
+        for b in range(5):
+            eng.resetFramePosition()
+            assert not eng.calculateSRRF(stack[b * nf:(b + 1) * nf])
+            want.append(eng.readSRRFbuffer().copy())
+        maps = eng.readMPmaps()
+    finally:
+        eng.release()
+    outs = [torch.empty((4, 40 * M, 56 * M), dtype=torch.float32).pin_memory().numpy() for _ in range(5)]
+    eng = engine()
+    try:
+        for b in range(5):
+            eng.resetFramePosition()
+            assert not eng.calculateSRRF(stack[b * nf:(b + 1) * nf])
+            eng.readSRRFbufferAsync(outs[b])
+        eng.finishQueue()
+        got_maps = eng.readMPmaps()
+    finally:
+        eng.release()
+    for b in range(5):
+        np.testing.assert_array_equal(outs[b], want[b])
+    np.testing.assert_array_equal(got_maps, maps)
