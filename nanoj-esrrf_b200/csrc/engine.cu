@@ -252,6 +252,7 @@ esrrf_status esrrf_handle::init_fht() {
     if (plan.tc) CK(cudaMalloc(&scratch.xs, sizeof(float) * (size_t)F * interp_xs_floats(plan)));
     CK(cudaMalloc(&scratch.alt, sizeof(float) * (size_t)F * interp_alt_floats(plan.N)));
     CK(cudaMalloc(&scratch.vec, sizeof(float) * (size_t)F * interp_vec_floats(HM, WM)));
+    CK(cudaMalloc(&d_prev_out, sizeof(float) * (size_t)WM * HM));
     CK(cudaMalloc(&d_interp, sizeof(float) * (size_t)F * whM));
     CK(cudaMalloc(&d_gx, sizeof(float) * (size_t)F * whM));
     CK(cudaMalloc(&d_gy, sizeof(float) * (size_t)F * whM));
@@ -286,6 +287,7 @@ void esrrf_handle::release() {
     }
     cudaFree(st.acc);
     cudaFree(st.prev);
+    cudaFree(d_prev_out);
     cudaFree(d_out);
     cudaFree(d_out2);
     d_out2 = nullptr;
@@ -348,6 +350,7 @@ esrrf_status esrrf_handle::process_chunk(const void* src, bool is_u16, int F_now
     a.t0 = frame_in_block;
     a.int_weighting = p.int_weighting;
     a.st = st;
+    a.prev_out = d_prev_out;
     if (use_fused && !any_drift) {
         CK(fht_rgc_fused(geo, tables, a, stream));
         launches += 1;

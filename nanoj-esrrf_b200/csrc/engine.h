@@ -62,6 +62,7 @@ struct esrrf_handle {
 
     // block accumulators and output
     esrrf::BlockState st;
+    float* d_prev_out = nullptr;  // [HM][WM] lets a fused launch split its frames into groups (FHT)
     float* d_out = nullptr;
     // queued read-back (esrrf_read_srrf_async): two output slots, slot 0 = d_out; the
     // device-to-host copies run on read_stream and overlap the next block's kernels

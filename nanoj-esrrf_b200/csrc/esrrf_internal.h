@@ -119,6 +119,10 @@ struct FhtRgcArgs {
     BlockState st;
     float* cg_out = nullptr;  // fused kernel only: if set, write CGLH / sum of weights per frame
                               // [F][H][W] (before the sensitivity power) instead of accumulating
+    float* prev_out = nullptr;  // fused kernel: [H][W] scratch that lets a launch split its frames
+                                // into groups across CTAs (the last group's values land here and
+                                // are copied to st.prev after the launch, so no group overwrites a
+                                // value another group still reads); null: one group
 };
 
 cudaError_t fht_robx(const float* interp, int W, int H, int F, float* gx, float* gy,

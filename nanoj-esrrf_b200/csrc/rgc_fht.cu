@@ -327,6 +327,12 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
 
     const int xM = x0 + tx;
     const bool emit = a.cg_out != nullptr;
+    // frame group: frames [fb, fe) of the launch (one group unless the tiles alone leave SMs
+    // idle); a later group first runs frame fb - 1 only for its intensity-weighted value, the
+    // previous value of TAC2's product at fb
+    const int G = gridDim.z, grp = blockIdx.z;
+    const int fb = (int)((long long)a.F * grp / G), fe = (int)((long long)a.F * (grp + 1) / G);
+    const int fs = grp > 0 && !emit ? fb - 1 : fb;
     float wsum[kK];
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
@@ -357,10 +363,10 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    if (L::kDB && a.F > 0) prefetch_tile(0, sIb);
+    if (L::kDB && fe > fs) prefetch_tile(fs, sIb);
 
-    for (int f = 0; f < a.F; ++f) {
-        float* sI = sIb + (L::kDB ? (f & 1) * kIStride : 0);
+    for (int f = fs; f < fe; ++f) {
+        float* sI = sIb + (L::kDB ? ((f - fs) & 1) * kIStride : 0);
         __syncthreads();
         // 1. this frame's intensity tile: prefetched during the previous frame, or loaded now
         if (L::kDB) {
@@ -406,7 +412,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         }
         __syncthreads();
         // the next frame's tile goes into the other buffer while this frame's taps run
-        if (L::kDB && f + 1 < a.F) prefetch_tile(f + 1, sIb + ((f + 1) & 1) * kIStride);
+        if (L::kDB && f + 1 < fe) prefetch_tile(f + 1, sIb + ((f + 1 - fs) & 1) * kIStride);
         // 3. tap loop, one box column at a time with its weights in registers
         float acc[kK];
 #pragma unroll
@@ -447,6 +453,10 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             const float cg = cglh_power(acc[k] / wsum[k], fp.sens);
             const float v = sI[(ty * kK + k + 1 - r0) * IW + (tx + 1 - r0)];
             const float x = a.int_weighting ? v * cg : cg;
+            if (f < fb) {  // the frame before the group: previous value only
+                sst[4 * kTX * kTH + o] = x;
+                continue;
+            }
             const float pv = sst[4 * kTX * kTH + o];
             sst[0 * kTX * kTH + o] += x;
             sst[1 * kTX * kTH + o] += x * x;
@@ -463,12 +473,32 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         if (xM >= W || yM >= H) continue;
         const long pix = (long)yM * W + xM;
         const int o = (ty * kK + k) * kTX + tx;
-        a.st.acc[pix] += (double)sst[0 * kTX * kTH + o];
-        a.st.acc[wh + pix] += (double)sst[1 * kTX * kTH + o];
-        a.st.acc[2 * wh + pix] += (double)sst[2 * kTX * kTH + o];
-        a.st.acc[3 * wh + pix] += (double)sst[3 * kTX * kTH + o];
-        a.st.prev[pix] = sst[4 * kTX * kTH + o];
+        if (G == 1) {
+            a.st.acc[pix] += (double)sst[0 * kTX * kTH + o];
+            a.st.acc[wh + pix] += (double)sst[1 * kTX * kTH + o];
+            a.st.acc[2 * wh + pix] += (double)sst[2 * kTX * kTH + o];
+            a.st.acc[3 * wh + pix] += (double)sst[3 * kTX * kTH + o];
+        } else {  // several groups add into the same pixels
+#pragma unroll
+            for (int c = 0; c < 4; ++c) atomicAdd(a.st.acc + c * wh + pix, (double)sst[c * kTX * kTH + o]);
+        }
+        if (grp == G - 1) (G == 1 ? a.st.prev : a.prev_out)[pix] = sst[4 * kTX * kTH + o];
     }
+}
+
+// Multiprocessor count of a device, queried once per device.
+int sm_count(int dev) {
+    static int cache[64] = {0};
+    if (dev < 0 || dev >= 64) return 148;
+    if (cache[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = 148;
+        }
+        cache[dev] = n;
+    }
+    return cache[dev];
 }
 
 template <int S>
@@ -489,8 +519,19 @@ cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const Fh
     }
     FusedParams fp{g.r0, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
     dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
+    // frames split into groups across CTAs only where the tiles alone give fewer than two CTAs
+    // per SM (small frames); a group keeps at least 4 frames when it pays an extra frame
+    const int tiles = (int)(grid.x * grid.y), slots = 2 * sm_count(dev);
+    if (tiles < slots && a.F > 1 && (a.cg_out || a.prev_out)) {
+        const int gmax = a.cg_out ? a.F : std::max(1, a.F / 4);
+        grid.z = (unsigned)std::max(1, std::min({(slots + tiles - 1) / tiles, gmax, 65535}));
+    }
     fht_rgc_fused_kernel<S><<<grid, 256, bytes, stream>>>(a, fp);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (grid.z > 1 && !a.cg_out)
+        return cudaMemcpyAsync(a.st.prev, a.prev_out, sizeof(float) * (size_t)a.W * a.H,
+                               cudaMemcpyDeviceToDevice, stream);
+    return cudaSuccess;
 }
 
 __global__ void finalize_kernel(BlockState st, int n, int tac_div2, float* __restrict__ out) {

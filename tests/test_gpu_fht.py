@@ -155,3 +155,18 @@ def test_block_overflow_and_cancel(esrrf_mod):
         assert eng.calculateSRRF(raw[:4]) is True
     finally:
         eng.release()
+
+
+def test_small_frames_split_into_frame_groups(esrrf_mod, oracle_mod):
+    """Small frames (a 96 x 80 output is 6 CTA tiles) split each launch's frames into groups
+    across CTAs: 20-frame launches in 5 groups, each later group re-running the frame before it
+    for TAC2's previous value, sums folded atomically, the last values handed to the next launch.
+    Same block as the oracle and as 3-frame launches (one group)."""
+    from esrrf import synth
+    raw = synth.small_stack(91, 40, 40, 48).astype(np.float32)
+    ref = oracle_mod.fht_block(oracle_mod.fht_interpolate(raw, 2), 2, 1.5, 2)
+    grouped = run_engine(esrrf_mod, raw, 2, 1.5, 2, frames_per_launch=20, chunks=[20, 20])
+    single = run_engine(esrrf_mod, raw, 2, 1.5, 2, frames_per_launch=3)
+    assert_close(grouped, ref, what="grouped vs oracle")
+    assert_close(grouped, single, tol=1e-5, what="grouped vs one group")
+    assert np.abs(grouped[2]).max() > 0
