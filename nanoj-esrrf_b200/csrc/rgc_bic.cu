@@ -260,24 +260,29 @@ __global__ void __launch_bounds__(256, 4) bic_tab_kernel(BicTabArgs a) {
     const bool emit = a.cg_out != nullptr;
     float prev = valid && !emit ? a.st.prev[pix] : 0.f;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-    const int st_ly = tid / row2, st_rem = tid - st_ly * row2;
-    const int st_dly = 256 / row2, st_drem = 256 - st_dly * row2;
-    // slab of frame f into buffer f & 1; element i = tid + 256 k at (row ly, position rem)
-    // advanced without divisions
+    // slab staging: warp ty copies rows ty, ty + 8, ...; lane tx the positions tx + 32 q of each
+    // row, whose source column offsets (parity half + column; -1 beyond the field) are the same
+    // for every row and frame (row2 <= 4 x 32, checked when the tables are built)
+    int coff[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int rem = threadIdx.x + 32 * q;
+        const int par = rem >= a.tab.sl_nx ? 1 : 0, cin = cin0 + rem - par * a.tab.sl_nx;
+        coff[q] = rem < row2 && cin < half ? par * half + cin : -1;
+    }
     auto stage = [&](int f) {
         const float2* Uf = a.U + f * fstride;
         float2* dst = sbuf + (f & 1) * slab;
-        int ly = st_ly, rem = st_rem;
-        for (int i = tid; i < slab; i += 256) {
-            const int par = rem >= a.tab.sl_nx ? 1 : 0, lx = rem - par * a.tab.sl_nx;
-            const int row = row0 + ly, cin = cin0 + lx;
-            const bool in = row < a.tab.H2p && cin < half;
-            cp_async8(dst + i, in ? (const void*)(Uf + (long)row * a.tab.W2p + par * half + cin) : (const void*)a.U, in);
-            ly += st_dly;
-            rem += st_drem;
-            if (rem >= row2) {
-                rem -= row2;
-                ++ly;
+        for (int ly = threadIdx.y; ly < a.tab.sl_rows; ly += 8) {
+            const int row = row0 + ly;
+            const bool rin = row < a.tab.H2p;
+            const float2* src = Uf + (long)row * a.tab.W2p;
+            float2* d = dst + ly * row2 + threadIdx.x;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if ((int)threadIdx.x + 32 * q >= row2) break;
+                const bool in = rin && coff[q] >= 0;
+                cp_async8(d + 32 * q, in ? (const void*)(src + coff[q]) : (const void*)a.U, in);
             }
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -380,7 +385,8 @@ cudaError_t bic_tables_build(const BicGeometry& g, int M, int w, int h, BicTable
     t.sl_nx = 31 + fxmax - fxmin + 1;
     t.max_taps = maxn;
     t.smem = sizeof(float4) * ((size_t)maxn + (maxn + 3) / 4) + sizeof(float2) * 2 * (size_t)t.sl_rows * 2 * t.sl_nx;
-    if (t.smem > 200 * 1024) return cudaSuccess;
+    // the kernel stages a slab row with at most 4 x 32 lanes' positions
+    if (t.smem > 200 * 1024 || 2 * t.sl_nx > 128) return cudaSuccess;
     std::vector<float4> A;
     std::vector<float> Wt;
     std::vector<int2> node;
