@@ -524,27 +524,32 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
 #pragma unroll
     for (int k = 0; k < 4; ++k) splane[k] = min(max(zlo - 1 + k, 0), a.P - 1);
 
-    const int st_ly = tid / row2, st_rem = tid - st_ly * row2;
-    const int st_dly = 256 / row2, st_drem = 256 - st_dly * row2;
+    // slab staging: warp ty copies rows ty, ty + 8, ...; lane tx the positions tx + 32 q of each
+    // row, whose source column offsets (parity half + column; -1 beyond the field) are the same
+    // for every row, plane and frame (row2 <= 4 x 32, checked before this form is chosen)
+    int coff[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int rem = threadIdx.x + 32 * q;
+        const int par = rem >= a.tab.sl_nx ? 1 : 0, cin = cin0 + rem - par * a.tab.sl_nx;
+        coff[q] = rem < row2 && cin < half ? par * half + cin : -1;
+    }
     // slab g = (frame g / nz, plane offset zk0 + g % nz) into buffer g & 1
     auto stage = [&](int g) {
         const int f = g / nz, sidx = g - f * nz;
         const int plane = qz + a.tab.padz_lo + a.tab.zk0 + sidx;
         const float4* Uf = a.U + f * fstride + (long)plane * a.tab.H2p * a.tab.W2p;
         float4* dst = sbuf + (g & 1) * slab;
-        // element i = tid + 256 k of the slab: (row ly, position rem in the row) advanced without
-        // divisions (st_ly, st_rem: this thread's first element, 256 = st_dly rows + st_drem)
-        int ly = st_ly, rem = st_rem;
-        for (int i = tid; i < slab; i += 256) {
-            const int par = rem >= a.tab.sl_nx ? 1 : 0, lx = rem - par * a.tab.sl_nx;
-            const int row = row0 + ly, cin = cin0 + lx;
-            const bool in = row < a.tab.H2p && cin < half;
-            cp_async16(dst + i, in ? (const void*)(Uf + (long)row * a.tab.W2p + par * half + cin) : (const void*)a.U, in);
-            ly += st_dly;
-            rem += st_drem;
-            if (rem >= row2) {
-                rem -= row2;
-                ++ly;
+        for (int ly = threadIdx.y; ly < a.tab.sl_rows; ly += 8) {
+            const int row = row0 + ly;
+            const bool rin = row < a.tab.H2p;
+            const float4* src = Uf + (long)row * a.tab.W2p;
+            float4* d = dst + ly * row2 + threadIdx.x;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if ((int)threadIdx.x + 32 * q >= row2) break;
+                const bool in = rin && coff[q] >= 0;
+                cp_async16(d + 32 * q, in ? (const void*)(src + coff[q]) : (const void*)a.U, in);
             }
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -870,7 +875,8 @@ cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream) {
         // slab-staged form where two CTAs' shared memory fits an SM (ESRRF_RGC3D=zb: the form
         // that reads the field through the L1 cache)
         const char* form = std::getenv("ESRRF_RGC3D");
-        const bool slab = zs_smem_bytes(a.tab) <= 112 * 1024 && !(form && std::strcmp(form, "zb") == 0);
+        const bool slab = zs_smem_bytes(a.tab) <= 112 * 1024 && 2 * a.tab.sl_nx <= 128 &&
+                          !(form && std::strcmp(form, "zb") == 0);
         switch (a.M) {
             case 2: return slab ? launch_zs<2>(a, stream) : launch_zb<2>(a, stream);
             case 3: return slab ? launch_zs<3>(a, stream) : launch_zb<3>(a, stream);
