@@ -822,6 +822,12 @@ esrrf_status esrrf_adjoint_create(int width, int height, int n_frames, int magni
     a->w = width;
     a->h = height;
     a->T = n_frames;
+    // frames per chunk of the passes: equal chunks of at most 32 (the transposed interpolation's
+    // GEMMs have only 16 and 4 CTAs per frame at 256 x 256, M4, so fewer frames leave SMs idle)
+    {
+        const int chunks = (n_frames + 31) / 32;
+        a->Fc = (n_frames + chunks - 1) / chunks;
+    }
     a->M = magnification;
     a->device = device >= 0 ? device : 0;
     a->WM = width * magnification;
