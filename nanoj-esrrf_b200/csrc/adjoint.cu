@@ -41,11 +41,19 @@ template <int S>
 struct AdjLayout {
     static constexpr int EW = kTX + S - 1, EH = kTH + S - 1;
     static constexpr int IW = EW + 2, IH = EH + 2;
+    static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
     static constexpr size_t off_E = 0;
-    static constexpr size_t off_I = off_E + sizeof(float2) * EW * EH;
-    static constexpr size_t off_wt = (off_I + sizeof(float) * IW * IH + 15) & ~size_t(15);
+    static constexpr size_t off_I = (off_E + sizeof(float2) * EW * EH + 15) & ~size_t(15);  // 2 buffers
+    static constexpr size_t off_wt = off_I + 2 * I_bytes;
     static constexpr size_t bytes = off_wt + sizeof(float4) * S * S;
 };
+
+// 4-byte asynchronous copy into shared memory; valid = false writes a zero and reads nothing
+__device__ __forceinline__ void cp_async4z(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
 
 struct AdjAArgs {
     const float* I;      // [F][H][W] interpolated frames of the chunk
@@ -148,8 +156,9 @@ __global__ void __launch_bounds__(256, 2) adj_a_kernel(AdjAArgs g) {
     constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
     extern __shared__ __align__(16) unsigned char smem[];
     float2* sE = reinterpret_cast<float2*>(smem + L::off_E);
-    float* sI = reinterpret_cast<float*>(smem + L::off_I);
+    float* sIb = reinterpret_cast<float*>(smem + L::off_I);
     float4* stab = reinterpret_cast<float4*>(smem + L::off_wt);
+    constexpr int kIS = (int)(L::I_bytes / sizeof(float));
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTH, r0 = g.r0;
     const int W = g.W, H = g.H;
@@ -159,14 +168,22 @@ __global__ void __launch_bounds__(256, 2) adj_a_kernel(AdjAArgs g) {
     const int gX0 = x0 + r0 - 1, gY0 = y0 + r0 - 1;
     const float fr0 = (float)r0;
     double dS = 0.0, dT = 0.0;
-    for (int f = 0; f < g.F; ++f) {
+    // intensity tile of frame f (clamped reads) copied asynchronously into dst: the next frame's
+    // tile lands in the other buffer while this frame's taps run
+    auto prefetch = [&](int f, float* dst) {
         const float* fr = g.I + (long)f * wh;
-        __syncthreads();
         for (int ly = ty; ly < IH; ly += kTYT) {
             const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
-            for (int lx = tx; lx < IW; lx += kTX) sI[ly * IW + lx] = __ldg(fr + grow + min(max(gX0 + lx, 0), W - 1));
+            for (int lx = tx; lx < IW; lx += kTX) cp_async4z(dst + ly * IW + lx, fr + grow + min(max(gX0 + lx, 0), W - 1), true);
         }
-        __syncthreads();
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (g.F > 0) prefetch(0, sIb);
+    for (int f = 0; f < g.F; ++f) {
+        float* sI = sIb + (f & 1) * kIS;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // frame f's tile landed; every thread is done with frame f - 1's buffer
+        if (f + 1 < g.F) prefetch(f + 1, sIb + ((f + 1) & 1) * kIS);
         for (int ey = ty; ey < EH; ey += kTYT) {
             const int Y = y0 + r0 + ey;
             const bool yin = Y >= 0 && Y < H;
@@ -262,9 +279,11 @@ template <int S>
 struct AdjBLayout {
     static constexpr int BW = kTX + S - 1, BH = kTH + S - 1;  // dL/dN tile, origin (x0-r1, y0-r1)
     static constexpr int IW = kTX + 2, IH = kTH + 2;          // intensity around the sources
-    static constexpr size_t off_B = 0;
-    static constexpr size_t off_I = off_B + sizeof(float) * BW * BH;
-    static constexpr size_t off_wd = (off_I + sizeof(float) * IW * IH + 15) & ~size_t(15);
+    static constexpr size_t B_bytes = (sizeof(float) * BW * BH + 15) & ~size_t(15);
+    static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
+    static constexpr size_t off_B = 0;                  // 2 buffers
+    static constexpr size_t off_I = off_B + 2 * B_bytes;  // 2 buffers
+    static constexpr size_t off_wd = off_I + 2 * I_bytes;
     static constexpr size_t bytes = off_wd + sizeof(float) * S * S;
 };
 
@@ -329,9 +348,10 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
     using L = AdjBLayout<S>;
     constexpr int BW = L::BW, BH = L::BH, IW = L::IW, IH = L::IH;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* sB = reinterpret_cast<float*>(smem + L::off_B);
-    float* sI = reinterpret_cast<float*>(smem + L::off_I);
+    float* sBb = reinterpret_cast<float*>(smem + L::off_B);
+    float* sIb = reinterpret_cast<float*>(smem + L::off_I);
     float* swd = reinterpret_cast<float*>(smem + L::off_wd);
+    constexpr int kBS = (int)(L::B_bytes / sizeof(float)), kIS = (int)(L::I_bytes / sizeof(float));
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTH, r1 = g.r1;
     const int W = g.W, H = g.H;
@@ -339,22 +359,34 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
     for (int i = tid; i < S * S; i += blockDim.x) swd[i] = g.wdB[i];
     const int X = x0 + tx;
     const float fr1 = (float)r1;
-    for (int f = 0; f < g.F; ++f) {
+    // dL/dN tile (zero outside the image) and intensity tile (clamped reads) of frame f copied
+    // asynchronously into buffer f & 1 while the previous frame's taps run
+    auto prefetch = [&](int f) {
         const float* fr = g.I + (long)f * wh;
         const float* bf = g.b + (long)f * wh;
-        __syncthreads();
+        float* dB = sBb + (f & 1) * kBS;
+        float* dI = sIb + (f & 1) * kIS;
         for (int ly = ty; ly < BH; ly += kTYT) {
             const int q_y = y0 - r1 + ly;
             for (int lx = tx; lx < BW; lx += kTX) {
                 const int q_x = x0 - r1 + lx;
-                sB[ly * BW + lx] = (q_x >= 0 && q_x < W && q_y >= 0 && q_y < H) ? __ldg(bf + (long)q_y * W + q_x) : 0.f;
+                const bool in = q_x >= 0 && q_x < W && q_y >= 0 && q_y < H;
+                cp_async4z(dB + ly * BW + lx, in ? bf + (long)q_y * W + q_x : bf, in);
             }
         }
         for (int ly = ty; ly < IH; ly += kTYT) {
             const long grow = (long)min(max(y0 - 1 + ly, 0), H - 1) * W;
-            for (int lx = tx; lx < IW; lx += kTX) sI[ly * IW + lx] = __ldg(fr + grow + min(max(x0 - 1 + lx, 0), W - 1));
+            for (int lx = tx; lx < IW; lx += kTX) cp_async4z(dI + ly * IW + lx, fr + grow + min(max(x0 - 1 + lx, 0), W - 1), true);
         }
-        __syncthreads();
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (g.F > 0) prefetch(0);
+    for (int f = 0; f < g.F; ++f) {
+        const float* sB = sBb + (f & 1) * kBS;
+        const float* sI = sIb + (f & 1) * kIS;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // frame f's tiles landed; every thread is done with frame f - 1's buffers
+        if (f + 1 < g.F) prefetch(f + 1);
         // unit gradient at this thread's 8 sources
         float gx[kK], gy[kK], inv[kK];
 #pragma unroll
