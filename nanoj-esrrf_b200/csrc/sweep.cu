@@ -343,7 +343,8 @@ static esrrf_status sweep_create_bic(esrrf_sweep* s) {
             if (!built) {
                 bic_tables_free(t);
                 return s->fail(ESRRF_ERR_INVALID, "radius " + std::to_string(r) + " at magnification " +
-                                                      std::to_string(M) + " needs more than 200 KB of shared memory per CTA");
+                                                      std::to_string(M) + " reaches too far for the tabulated "
+                                                      "bicubic kernel (shared memory or slab row width)");
             }
             padx = std::max(padx, t.padx);
             pady = std::max(pady, t.pady);
