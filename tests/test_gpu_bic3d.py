@@ -92,6 +92,16 @@ def test_bic_tabulated_taps_radii(esrrf_mod, oracle_mod, M, fwhm, S):
     assert_close(got, plain, f"bic tabulated vs per-pixel M{M} r{fwhm}")
 
 
+def test_bic_radius_beyond_the_tables_uses_per_pixel_kernel(esrrf_mod, oracle_mod):
+    """A radius whose slab rows exceed the tabulated kernel's reach (fwhm 20: 138 positions per
+    row) builds no tables: every launch takes the per-pixel kernel, against the oracle."""
+    from esrrf import synth
+    raw = synth.small_stack(88, 4, 40, 44).astype(np.float32)
+    ref = oracle_mod.bic_block(raw, 2, 20.0, 1)
+    got, _ = run(esrrf_mod, raw, 2, 20.0, 1)
+    assert_close(got, ref, "bic fwhm 20")
+
+
 def test_bic_drift_uses_per_pixel_kernel(esrrf_mod, oracle_mod):
     """A launch with drift takes the per-pixel kernel (the tap geometry then moves per frame);
     the launch without drift after it the tabulated one; both against the oracle."""
