@@ -51,6 +51,14 @@ struct CumArgs {
 __global__ void __launch_bounds__(256) sweep_cumulants_kernel(CumArgs a) {
     const long pix = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= a.P) return;
+    // block bounds in registers; unused block slots get an empty range, unused sensitivity slots
+    // are skipped by guards (no early exits, so every index below is a compile-time constant)
+    int bs[kBG], be[kBG];
+#pragma unroll
+    for (int b = 0; b < kBG; ++b) {
+        bs[b] = b < a.nb ? a.start[b] : 0;
+        be[b] = b < a.nb ? a.start[b] + a.len[b] : 0;
+    }
     double acc[kSG][kBG][4];
     float prev[kSG];
 #pragma unroll
@@ -61,37 +69,42 @@ __global__ void __launch_bounds__(256) sweep_cumulants_kernel(CumArgs a) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[s][b][c] = 0.0;
     }
-    int t_lo = a.start[0], t_hi = a.start[0] + a.len[0];
-    for (int b = 1; b < a.nb; ++b) {
-        t_lo = min(t_lo, a.start[b]);
-        t_hi = max(t_hi, a.start[b] + a.len[b]);
-    }
+    int t_lo = bs[0], t_hi = be[0];
+#pragma unroll
+    for (int b = 1; b < kBG; ++b)
+        if (b < a.nb) {
+            t_lo = min(t_lo, bs[b]);
+            t_hi = max(t_hi, be[b]);
+        }
     for (int t = t_lo; t < t_hi; ++t) {
         const float c = __ldg(a.cg + (long)t * a.P + pix);
         const float v = __ldg(a.v + (long)t * a.P + pix);
+        const double vd = (double)v;
 #pragma unroll
         for (int s = 0; s < kSG; ++s) {
-            if (s >= a.ns) break;
-            const float cg = dev::cglh_power(c, a.sens[s]);
-            const float x = a.int_weighting ? v * cg : cg;
+            if (s < a.ns) {
+                const float cg = dev::cglh_power(c, a.sens[s]);
+                const float x = a.int_weighting ? v * cg : cg;
+                const double xd = (double)x;
 #pragma unroll
-            for (int b = 0; b < kBG; ++b) {
-                if (b >= a.nb) break;
-                if (t < a.start[b] || t >= a.start[b] + a.len[b]) continue;
-                acc[s][b][0] += x;
-                acc[s][b][1] += (double)x * x;
-                if (t > a.start[b]) acc[s][b][2] += (double)x * prev[s];
-                acc[s][b][3] += v;
+                for (int b = 0; b < kBG; ++b) {
+                    if (t >= bs[b] && t < be[b]) {
+                        acc[s][b][0] += xd;
+                        acc[s][b][1] = fma(xd, xd, acc[s][b][1]);
+                        if (t > bs[b]) acc[s][b][2] = fma(xd, (double)prev[s], acc[s][b][2]);
+                        acc[s][b][3] += vd;
+                    }
+                }
+                prev[s] = x;
             }
-            prev[s] = x;
         }
     }
 #pragma unroll
     for (int s = 0; s < kSG; ++s) {
-        if (s >= a.ns) break;
+        if (s >= a.ns) continue;
 #pragma unroll
         for (int b = 0; b < kBG; ++b) {
-            if (b >= a.nb) break;
+            if (b >= a.nb) continue;
             const int n = a.len[b];
             const double avg = acc[s][b][0] / n, av2 = avg * avg;
             double tac = n > 1 ? acc[s][b][2] / (n - 1) : 0.0;
