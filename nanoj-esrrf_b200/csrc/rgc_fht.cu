@@ -301,7 +301,9 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
                  : "memory");
 }
 
-template <int S>
+// GROUPED: the launch may split its frames into groups (gridDim.z); the one-group instantiation
+// compiles the frame loop and the fold without the group bookkeeping.
+template <int S, bool GROUPED>
 __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, FusedParams fp) {
     using L = FusedLayout<S>;
     constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
     // frame group: frames [fb, fe) of the launch (one group unless the tiles alone leave SMs
     // idle); a later group first runs frame fb - 1 only for its intensity-weighted value, the
     // previous value of TAC2's product at fb
-    const int G = gridDim.z, grp = blockIdx.z;
+    const int G = GROUPED ? (int)gridDim.z : 1, grp = GROUPED ? (int)blockIdx.z : 0;
     const int fb = (int)((long long)a.F * grp / G), fe = (int)((long long)a.F * (grp + 1) / G);
     const int fs = grp > 0 && !emit ? fb - 1 : fb;
     float wsum[kK];
@@ -512,9 +514,11 @@ cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const Fh
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 64 || !(configured & (1ull << dev))) {
-        e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)bytes);
-        if (e != cudaSuccess) return e;
+        if ((e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bytes)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bytes)) != cudaSuccess)
+            return e;
         if (dev < 64) configured |= 1ull << dev;
     }
     FusedParams fp{g.r0, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
@@ -526,7 +530,10 @@ cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const Fh
         const int gmax = a.cg_out ? a.F : std::max(1, a.F / 4);
         grid.z = (unsigned)std::max(1, std::min({(slots + tiles - 1) / tiles, gmax, 65535}));
     }
-    fht_rgc_fused_kernel<S><<<grid, 256, bytes, stream>>>(a, fp);
+    if (grid.z > 1)
+        fht_rgc_fused_kernel<S, true><<<grid, 256, bytes, stream>>>(a, fp);
+    else
+        fht_rgc_fused_kernel<S, false><<<grid, 256, bytes, stream>>>(a, fp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (grid.z > 1 && !a.cg_out)
         return cudaMemcpyAsync(a.st.prev, a.prev_out, sizeof(float) * (size_t)a.W * a.H,
