@@ -276,6 +276,20 @@ esrrf_status fail(const std::string& m, esrrf_status s = ESRRF_ERR_INVALID) {
     return s;
 }
 
+// Scratch of esrrf_squirrel, kept per device between calls (grow-only): allocating and freeing
+// the up-to-1 GB blur buffer on every call made the call's time vary by a factor of two.  A call
+// holds its device's lock throughout, so concurrent calls on one device run one after the other.
+struct SquirrelScratch {
+    std::mutex mu;
+    float* tmp = nullptr;
+    size_t tmp_floats = 0;
+    void* img = nullptr;  // Img[batch]
+    double* sums = nullptr;
+    float* ab = nullptr;
+    int batch = 0;
+};
+SquirrelScratch g_sq[64];
+
 }  // namespace
 
 extern "C" {
@@ -307,28 +321,43 @@ esrrf_status esrrf_squirrel(const esrrf_squirrel_params* p, int n, const float* 
     if ((e = cudaFuncSetAttribute(col_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)colsmem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(row_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rowsmem)) != cudaSuccess)
         return fail(cudaGetErrorString(e), ESRRF_ERR_CUDA);
-    float* tmp = nullptr;
-    Img* d_img = nullptr;
-    double* d_sums = nullptr;
-    float* d_ab = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(tmp);
-        cudaFree(d_img);
-        cudaFree(d_sums);
-        cudaFree(d_ab);
-    };
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return fail(cudaGetErrorString(e), ESRRF_ERR_CUDA);
+    if (dev < 0 || dev >= 64) return fail("device ordinal out of range");
+    SquirrelScratch& sc = g_sq[dev];
+    std::lock_guard<std::mutex> lk(sc.mu);
 #define SQ(call)                                                     \
     do {                                                             \
         cudaError_t _e = (call);                                     \
-        if (_e != cudaSuccess) {                                     \
-            cleanup();                                               \
-            return fail(cudaGetErrorString(_e), ESRRF_ERR_CUDA);     \
-        }                                                            \
+        if (_e != cudaSuccess) return fail(cudaGetErrorString(_e), ESRRF_ERR_CUDA); \
     } while (0)
-    SQ(cudaMalloc(&tmp, sizeof(float) * (size_t)batch * Wc * Hc));
-    SQ(cudaMalloc(&d_img, sizeof(Img) * batch));
-    SQ(cudaMalloc(&d_sums, sizeof(double) * 3 * batch));
-    SQ(cudaMalloc(&d_ab, sizeof(float) * 2 * batch));
+    const size_t need = (size_t)batch * Wc * Hc;
+    if (sc.tmp_floats < need) {
+        SQ(cudaStreamSynchronize(st));
+        cudaFree(sc.tmp);
+        sc.tmp = nullptr;
+        sc.tmp_floats = 0;
+        SQ(cudaMalloc(&sc.tmp, sizeof(float) * need));
+        sc.tmp_floats = need;
+    }
+    if (sc.batch < batch) {
+        SQ(cudaStreamSynchronize(st));
+        cudaFree(sc.img);
+        cudaFree(sc.sums);
+        cudaFree(sc.ab);
+        sc.img = nullptr;
+        sc.sums = nullptr;
+        sc.ab = nullptr;
+        sc.batch = 0;
+        SQ(cudaMalloc(&sc.img, sizeof(Img) * batch));
+        SQ(cudaMalloc(&sc.sums, sizeof(double) * 3 * batch));
+        SQ(cudaMalloc(&sc.ab, sizeof(float) * 2 * batch));
+        sc.batch = batch;
+    }
+    float* tmp = sc.tmp;
+    Img* d_img = static_cast<Img*>(sc.img);
+    double* d_sums = sc.sums;
+    float* d_ab = sc.ab;
     const double npx = (double)Wc * Hc;
     std::vector<Img> hi(batch);
     std::vector<double> hs(3 * batch);
@@ -412,7 +441,6 @@ esrrf_status esrrf_squirrel(const esrrf_squirrel_params* p, int n, const float* 
         }
     }
 #undef SQ
-    cleanup();
     return ESRRF_OK;
 }
 
