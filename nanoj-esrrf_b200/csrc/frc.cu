@@ -191,6 +191,32 @@ __global__ void fire_kernel(const double* __restrict__ part, int chunks, int N, 
     fire[pair] = res;
 }
 
+// Buffers of esrrf_frc, kept per device between calls (grow-only), as the SQUIRREL scratch: a
+// call holds its device's lock throughout, so concurrent calls on one device run one after the
+// other.
+struct FrcScratch {
+    std::mutex mu;
+    void* buf[7] = {};
+    size_t cap[7] = {};
+};
+FrcScratch g_frc[64];
+
+// buffer i of the device's scratch with at least `bytes` (reallocated, after the stream drained,
+// when it is smaller)
+cudaError_t frc_buffer(FrcScratch& sc, int i, size_t bytes, cudaStream_t st, void** out) {
+    if (sc.cap[i] < bytes) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        cudaFree(sc.buf[i]);
+        sc.buf[i] = nullptr;
+        sc.cap[i] = 0;
+        if ((e = cudaMalloc(&sc.buf[i], bytes)) != cudaSuccess) return e;
+        sc.cap[i] = bytes;
+    }
+    *out = sc.buf[i];
+    return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -226,34 +252,31 @@ esrrf_status esrrf_frc(const esrrf_frc_params* p, int n, const float* d_base, co
         1, std::min<size_t>({(size_t)n, (1ull << 30) / (4 * plane), (size_t)16384}));
     const int rows_per_chunk = std::max(1, std::min(N, (1 << 16) / N));
     const int chunks = (N + rows_per_chunk - 1) / rows_per_chunk;
-    float2 *F = nullptr, *G = nullptr;
-    double *mean = nullptr, *part = nullptr;
-    size_t* d_offs = nullptr;
-    float *d_fire = nullptr, *d_curves = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(F);
-        cudaFree(G);
-        cudaFree(mean);
-        cudaFree(part);
-        cudaFree(d_offs);
-        cudaFree(d_fire);
-        cudaFree(d_curves);
-    };
-#define FK(call)                                                 \
-    do {                                                         \
-        cudaError_t _e = (call);                                 \
-        if (_e != cudaSuccess) {                                 \
-            cleanup();                                           \
-            return fail(cudaGetErrorString(_e), ESRRF_ERR_CUDA); \
-        }                                                        \
+#define FK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t _e = (call);                                                   \
+        if (_e != cudaSuccess) return fail(cudaGetErrorString(_e), ESRRF_ERR_CUDA); \
     } while (0)
-    FK(cudaMalloc(&F, 2 * plane * batch));
-    FK(cudaMalloc(&G, 2 * plane * batch));
-    FK(cudaMalloc(&mean, sizeof(double) * 2 * batch));
-    FK(cudaMalloc(&part, sizeof(double) * 3 * R * (size_t)chunks * batch));
-    FK(cudaMalloc(&d_offs, sizeof(size_t) * 2 * batch));
-    FK(cudaMalloc(&d_fire, sizeof(float) * batch));
-    if (curves) FK(cudaMalloc(&d_curves, sizeof(float) * R * (size_t)batch));
+    int dev = 0;
+    FK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail("device ordinal out of range");
+    FrcScratch& sc = g_frc[dev];
+    std::lock_guard<std::mutex> lk(sc.mu);
+    void* bp[7] = {};
+    FK(frc_buffer(sc, 0, 2 * plane * batch, st, &bp[0]));
+    FK(frc_buffer(sc, 1, 2 * plane * batch, st, &bp[1]));
+    FK(frc_buffer(sc, 2, sizeof(double) * 2 * batch, st, &bp[2]));
+    FK(frc_buffer(sc, 3, sizeof(double) * 3 * R * (size_t)chunks * batch, st, &bp[3]));
+    FK(frc_buffer(sc, 4, sizeof(size_t) * 2 * batch, st, &bp[4]));
+    FK(frc_buffer(sc, 5, sizeof(float) * batch, st, &bp[5]));
+    if (curves) FK(frc_buffer(sc, 6, sizeof(float) * R * (size_t)batch, st, &bp[6]));
+    float2* F = static_cast<float2*>(bp[0]);
+    float2* G = static_cast<float2*>(bp[1]);
+    double* mean = static_cast<double*>(bp[2]);
+    double* part = static_cast<double*>(bp[3]);
+    size_t* d_offs = static_cast<size_t*>(bp[4]);
+    float* d_fire = static_cast<float*>(bp[5]);
+    float* d_curves = static_cast<float*>(bp[6]);
     const size_t fft_smem = sizeof(float2) * (N + N / 2);
     FK(cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem));
     const size_t ring_smem = sizeof(double) * 3 * R;
@@ -281,7 +304,6 @@ esrrf_status esrrf_frc(const esrrf_frc_params* p, int n, const float* d_base, co
         FK(cudaStreamSynchronize(st));
     }
 #undef FK
-    cleanup();
     return ESRRF_OK;
 }
 
