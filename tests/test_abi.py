@@ -104,3 +104,32 @@ def test_drift_window_matches_oracle(esrrf_mod):
         assert esrrf_mod.drift_window(w, h, ms) == D.window(w, h, ms)
     with pytest.raises(esrrf_mod.EsrrfError):
         esrrf_mod.drift_window(2, 64)
+
+
+def test_sweep_rejects_bad_parameters_before_any_device_work(esrrf_mod):
+    """esrrf_sweep_create validates its parameters first (no GPU needed): an unknown
+    interpolation, a block outside the stack, an empty radius list."""
+    from esrrf import _lib
+    ip = ctypes.POINTER(ctypes.c_int)
+    fp = ctypes.POINTER(ctypes.c_float)
+    mags = (ctypes.c_int * 1)(2)
+    radii = (ctypes.c_float * 1)(1.5)
+    sens = (ctypes.c_int * 1)(1)
+    bs = (ctypes.c_int * 1)(0)
+
+    def create(interp=0, blen=10, n_radius=1):
+        bl = (ctypes.c_int * 1)(blen)
+        p = _lib.EsrrfSweepParams(32, 32, 10, 1, ctypes.cast(mags, ip), n_radius, ctypes.cast(radii, fp),
+                                  1, ctypes.cast(sens, ip), 1, ctypes.cast(bs, ip), ctypes.cast(bl, ip),
+                                  1, -1, interp)
+        h = ctypes.c_void_p()
+        rc = esrrf_mod.lib().esrrf_sweep_create(ctypes.byref(p), ctypes.byref(h))
+        return rc, esrrf_mod.lib().esrrf_sweep_last_error(None).decode()
+
+    invalid = -1  # ESRRF_ERR_INVALID
+    rc, msg = create(interp=7)
+    assert rc == invalid and "interpolation" in msg
+    rc, msg = create(blen=11)
+    assert rc == invalid and "outside the stack" in msg
+    rc, msg = create(n_radius=0)
+    assert rc == invalid and "non-empty" in msg
