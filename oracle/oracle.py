@@ -29,10 +29,14 @@ _ref = None
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compile the restatement, and the reference-kernel replay when the reference exists."""
+    """Compile the restatement, and the reference-kernel replay when the reference exists.
+
+    The reference tree is ``reference_root`` or the ``ESRRF_REFERENCE_DIR`` environment
+    variable; with neither, or without the tree there, only the restatement is built.
+    """
     subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
-    ref = reference_root or "/root/reference"
-    if os.path.isfile(os.path.join(ref, "resources", "liveSRRF_noInterpolation.cl")):
+    ref = reference_root or os.environ.get("ESRRF_REFERENCE_DIR", "")
+    if ref and os.path.isfile(os.path.join(ref, "resources", "liveSRRF_noInterpolation.cl")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 

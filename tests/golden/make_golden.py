@@ -76,7 +76,7 @@ def main():
     if not O.ref_available():
         O.build()
     if not O.ref_available():
-        raise SystemExit("reference kernels not built: the reference tree is needed")
+        raise SystemExit("reference kernels not built: set ESRRF_REFERENCE_DIR to the reference tree")
     for c in CASES:
         make_case(*c)
         print("wrote", c[0])
