@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define ESRRF_VERSION_MAJOR 0
-#define ESRRF_VERSION_MINOR 1
+#define ESRRF_VERSION_MINOR 2
 
 typedef enum {
     ESRRF_OK = 0,
@@ -197,15 +197,24 @@ esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* r
 
 /* ---- Batched parameter sweep and rolling analysis over uneven blocks -----------------------
  * Replaces the per-combination loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519:
- * initialise + resetFramePosition + calculateSRRF + readSRRFbuffer for every radius x
- * sensitivity) and the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:
- * 276-389), on the 2-D FHT path or the 2-D bicubic path (the sweep's "Use FHT interpolation"
- * option, gui/ParametersSweep_.java:879), with zero drift.  All frames are interpolated (FHT) or
- * their gradients resampled (bicubic) once, and the RGC tap loop runs once per (magnification,
- * radius) for all sensitivities and blocks; the whole sweep is one captured CUDA graph replayed
- * per run.  Blocks are arbitrary [start, start + length) frame ranges (uneven and overlapping
- * allowed).  The bicubic sweep applies the MP correction to every output, as the reference's
- * sweep initialises the engine with it on (gui/ParametersSweep_.java:410). */
+ * initialise + resetFramePosition + loadDriftXYGPUbuffer + calculateSRRF + readSRRFbuffer for
+ * every radius x sensitivity) and the block loop of LiveSRRF_optimised_.run
+ * (gui/LiveSRRF_optimised_.java:276-389), on the 2-D FHT path or the 2-D bicubic path (the
+ * sweep's "Use FHT interpolation" option, gui/ParametersSweep_.java:879).  All frames are
+ * interpolated (FHT) or their gradients resampled (bicubic) once, and the RGC tap loop runs once
+ * per (magnification, radius) for all sensitivities and blocks; the whole sweep is one captured
+ * CUDA graph per device replayed per run.  Blocks are arbitrary [start, start + length) frame
+ * ranges (uneven and overlapping allowed).  The bicubic sweep applies the MP correction to every
+ * output, as the reference's sweep initialises the engine with it on
+ * (gui/ParametersSweep_.java:410).
+ * Drift (FHT sweep): one shift per frame of the stack in raw pixels, the array the sweep computes
+ * once and loads into every combination's engine (gui/ParametersSweep_.java:282-290, 452-454);
+ * NULL = zero drift.  A rolling analysis whose blocks each have their own shift array (relative to
+ * the block's first frame, gui/LiveSRRF_optimised_.java:283-305) passes non-overlapping blocks
+ * with the arrays laid end to end.
+ * Devices: n_devices > 1 splits the sweep across those CUDA ordinals (esrrf_sweep_plan says how);
+ * each device keeps its own copy of the frames it needs, nothing is exchanged between devices, and
+ * esrrf_sweep_run gathers every output into the host buffer.  n_devices = 0 uses `device`. */
 typedef struct {
     int width, height, n_frames;
     int n_mag;
@@ -220,20 +229,37 @@ typedef struct {
     int int_weighting;
     int device;                /* CUDA ordinal; -1 = device 0 */
     int interp;                /* esrrf_interp: ESRRF_INTERP_FHT or ESRRF_INTERP_BIC */
+    const float* drift_x;      /* [n_frames] per-frame shift in raw pixels, or NULL (FHT only) */
+    const float* drift_y;
+    int n_devices;             /* 0: one device (`device`); > 1: shard across `devices` */
+    const int* devices;
 } esrrf_sweep_params;
 
 typedef struct esrrf_sweep esrrf_sweep;
 
 esrrf_status esrrf_sweep_create(const esrrf_sweep_params* params, esrrf_sweep** out);
+/* How esrrf_sweep_create splits a sweep across its devices (host arithmetic, no device work; the
+ * reference runs one device).  Units are the (magnification, radius) pairs, costed by tap count x
+ * output pixels x frame span, assigned longest first to the least-loaded device, or -- when that
+ * leaves devices idle or unbalanced -- the blocks, cut by start into contiguous runs of balanced
+ * frame span, every pair on every device; the split with the smaller largest cost is used.
+ * pair_device[m * n_radius + r] / block_device[b]: the device ordinal, -1 = every device of the
+ * split, -2 = none.  device_cost[d] (per entry of the device list): the relative cost.  Each may
+ * be NULL. */
+esrrf_status esrrf_sweep_plan(const esrrf_sweep_params* params, int* pair_device, int* block_device,
+                              double* device_cost);
 /* Output layout: for magnification m, radius r the floats from offsets[m * n_radius + r] hold
  * [n_sens][n_blocks][4][HM_m][WM_m] (AVG, VAR, TAC2, INT; NaN -> 0), HM_m = height * M_m. */
 esrrf_status esrrf_sweep_output_layout(const esrrf_sweep* s, size_t* total_floats, size_t* offsets);
-/* frames: [n_frames][height][width] uint16 (is_u16 = 1) or float; device pointers here, host
- * pointers in esrrf_sweep_run.  The first run with given pointers captures the graph. */
+/* frames: [n_frames][height][width] uint16 (is_u16 = 1) or float; device pointers here (a sweep on
+ * one device only), host pointers in esrrf_sweep_run.  The first run with given pointers captures
+ * the graph. */
 esrrf_status esrrf_sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out);
 esrrf_status esrrf_sweep_run(esrrf_sweep* s, const void* frames, int is_u16, float* out);
-/* Kernels in one run (the graph's node count). */
+/* Kernels in one run (the graphs' node count over all devices). */
 esrrf_status esrrf_sweep_launch_count(const esrrf_sweep* s, int* launches);
+/* Devices the sweep runs on (1 unless it was split). */
+esrrf_status esrrf_sweep_shard_count(const esrrf_sweep* s, int* shards);
 const char* esrrf_sweep_last_error(const esrrf_sweep* s);
 esrrf_status esrrf_sweep_destroy(esrrf_sweep* s);
 

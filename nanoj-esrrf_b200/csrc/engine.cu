@@ -22,7 +22,7 @@ namespace {
 std::mutex g_err_mu;
 std::string g_create_error;
 
-const char* kVersion = "0.1";
+const char* kVersion = "0.2";
 }  // namespace
 
 #define CK(call)                                                                     \
@@ -266,6 +266,13 @@ void esrrf_handle::release() {
     if (read_stream) cudaStreamSynchronize(read_stream);
     interp_plan_destroy(plan);
     fht_fused_tables_free(tables);
+    fht_drift_tables_free(dtab);
+    cudaFree(d_drift);
+    d_drift = nullptr;
+    if (h_drift_pin) cudaFreeHost(h_drift_pin);
+    h_drift_pin = nullptr;
+    if (ev_drift) cudaEventDestroy(ev_drift);
+    ev_drift = nullptr;
     cudaFree(scratch.rowT);
     cudaFree(scratch.xs);
     cudaFree(scratch.alt);
@@ -311,6 +318,38 @@ void esrrf_handle::release() {
     stream = copy_stream = read_stream = nullptr;
 }
 
+// loadDriftXYGPUbuffer (LiveSRRF_CL.java:583-595): the block's shifts, stored x M.  On the fused
+// FHT path they also go to the device (stream-ordered after the kernels already queued, so a
+// later block's shifts never reach an earlier block's launches); the pinned copy is rewritten only
+// once its previous upload has been read.
+esrrf_status esrrf_handle::set_drift(const float* dx, const float* dy) {
+    esrrf_handle* h = this;
+    const int n = p.n_frame_for_srrf;
+    bool any = false;
+    for (int i = 0; i < n; ++i) {
+        drift_x[i] = dx ? dx[i] : 0.f;
+        drift_y[i] = dy ? dy[i] : 0.f;
+        any |= drift_x[i] != 0.f || drift_y[i] != 0.f;
+    }
+    if (mode != Mode::kFHT || !use_fused || (!any && !d_drift)) return ESRRF_OK;
+    CK(cudaSetDevice(device));
+    if (!d_drift) {
+        CK(cudaMalloc(&d_drift, sizeof(float) * 2 * (size_t)n));
+        CK(cudaMallocHost(&h_drift_pin, sizeof(float) * 2 * (size_t)n));
+        CK(cudaEventCreateWithFlags(&ev_drift, cudaEventDisableTiming));
+    } else {
+        CK(cudaEventSynchronize(ev_drift));
+    }
+    const int M = p.magnification;
+    for (int i = 0; i < n; ++i) {
+        h_drift_pin[i] = M * drift_x[i];
+        h_drift_pin[n + i] = M * drift_y[i];
+    }
+    CK(cudaMemcpyAsync(d_drift, h_drift_pin, sizeof(float) * 2 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(ev_drift, stream));
+    return ESRRF_OK;
+}
+
 esrrf_status esrrf_handle::reset_block() {
     esrrf_handle* h = this;
     CK(cudaSetDevice(device));
@@ -354,6 +393,14 @@ esrrf_status esrrf_handle::process_chunk(const void* src, bool is_u16, int F_now
     if (use_fused && !any_drift) {
         CK(fht_rgc_fused(geo, tables, a, stream));
         launches += 1;
+    } else if (use_fused && d_drift) {
+        // frames with drift: per-frame tap tables and shifted intensities, then the fused kernel
+        if (!dtab.fr) CK(fht_drift_tables_alloc(geo.S, F, (long)WM * HM, dtab));
+        const int n = p.n_frame_for_srrf;
+        CK(fht_drift_build(geo, d_drift + frame_in_block, d_drift + n + frame_in_block, F_now, d_interp,
+                           WM, HM, dtab, stream));
+        CK(fht_rgc_fused_drift(geo, dtab, a, stream));
+        launches += 3;
     } else {
         CK(cudaMemcpyAsync(d_shift, sh.data(), sizeof(float) * 2 * F_now, cudaMemcpyHostToDevice, stream));
         CK(fht_robx(d_interp, WM, HM, F_now, d_gx, d_gy, stream));
@@ -712,11 +759,7 @@ esrrf_status esrrf_set_drift(esrrf_handle* h, const float* dx, const float* dy, 
     if (!h) return ESRRF_ERR_INVALID;
     if (n != h->p.n_frame_for_srrf && !(n == 0 && !dx && !dy))
         return h->fail(ESRRF_ERR_INVALID, "drift arrays must hold n_frame_for_srrf values");
-    for (int i = 0; i < h->p.n_frame_for_srrf; ++i) {
-        h->drift_x[i] = dx ? dx[i] : 0.f;
-        h->drift_y[i] = dy ? dy[i] : 0.f;
-    }
-    return ESRRF_OK;
+    return h->set_drift(dx, dy);
 }
 
 esrrf_status esrrf_reset_frame_position(esrrf_handle* h) {

@@ -31,6 +31,12 @@ struct esrrf_handle {
     float* d_gx = nullptr;
     float* d_gy = nullptr;
     float* d_shift = nullptr;
+    // drift on the fused kernel: the block's shifts x M on the device ([2][n_frame_for_srrf],
+    // uploaded by esrrf_set_drift from a pinned copy on the compute stream), per-launch tables
+    float* d_drift = nullptr;
+    float* h_drift_pin = nullptr;
+    cudaEvent_t ev_drift = nullptr;   // the last upload of h_drift_pin has been read
+    esrrf::FhtDriftTables dtab;
 
     // 2-D bicubic and 3-D paths
     esrrf::BicGeometry bgeo;
@@ -95,6 +101,7 @@ struct esrrf_handle {
     esrrf_status alloc_common(size_t raw_frame_bytes, long out_pixels);
     void release();
     esrrf_status reset_block();
+    esrrf_status set_drift(const float* dx, const float* dy);
     esrrf_status calculate(const void* frames, bool is_u16, int n, bool on_device);
     esrrf_status process_chunk(const void* src, bool is_u16, int F_now);
     esrrf_status process_chunk_bic3d(const void* src, bool is_u16, int F_now,

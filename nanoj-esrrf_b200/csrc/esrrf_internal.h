@@ -141,6 +141,47 @@ void fht_fused_tables_free(FhtFusedTables& t);
 cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                           cudaStream_t stream);
 bool fht_fused_supported(const FhtGeometry& g);
+// Multiprocessor count of a device (cached per device).
+int sm_count(int dev);
+
+// Frames with drift on the fused kernel.  A frame's shift (sx, sy) in magnified pixels is
+// uniform over the frame, so the tap geometry of every output pixel is the same: source offsets
+// (floor(sx) + i, floor(sy) + j) and centre offsets (i - frac(sx), j - frac(sy)), i, j in
+// [r0, r1].  Per frame of a launch: the integer shift, the offsets of tap (0, 0), the sum of the
+// weights over the whole disc in the reference's (j, i) order, the weight tables, each column's
+// disc chord and 2-D prefix sums of the weights (for output pixels whose tap box leaves the
+// image).
+struct FhtDriftFrame {
+    int ix, iy;         // floor of the shift
+    float fi0, fj0;     // r0 - frac(sx), r0 - frac(sy)
+    float wsum_int;     // sum of w over the disc, (j, i) order
+    float fx, fy;       // frac(sx), frac(sy)
+    int zero;           // 1: sx == sy == 0 (the interpolated pixel is the intensity)
+};
+struct FhtDriftTables {
+    int capacity = 0, S = 0;
+    FhtDriftFrame* fr = nullptr;  // [F]
+    float2* wt = nullptr;         // [F][S][S] (w, w/d), [ii][jj]
+    int* jr = nullptr;            // [F][2S] per column: first and last tap row of the disc
+    double* pre = nullptr;        // [F][S+1][S+1] prefix sums: pre[jj][ii] = sum over rows < jj, cols < ii
+    float* v = nullptr;           // [F][H][W] intensity at the shifted position
+};
+// Buffers for F frames of tap boxes up to S wide and `pixels` output pixels per frame (0: no
+// intensity planes).
+cudaError_t fht_drift_tables_alloc(int S, int F, long pixels, FhtDriftTables& t);
+cudaError_t fht_drift_tables_build(const FhtGeometry& g, const float* sx, const float* sy, int F,
+                                   FhtDriftTables& t, cudaStream_t stream);
+cudaError_t fht_shift_sample(const float* interp, int W, int H, int F, const float* sx, const float* sy,
+                             float* v, cudaStream_t stream);
+void fht_drift_tables_free(FhtDriftTables& t);
+// Tables of F frames with shifts sx[f], sy[f] (device, magnified pixels) and the intensity of
+// each frame at the shifted position: getInterpolatedValue(xM + sx, yM + sy) (bicubic, bilinear
+// near the border; the pixel itself for a frame with sx == sy == 0).
+cudaError_t fht_drift_build(const FhtGeometry& g, const float* sx, const float* sy, int F,
+                            const float* interp, int W, int H, FhtDriftTables& t, cudaStream_t stream);
+// The fused kernel on a launch whose frames have the tables of `t` (built for this launch).
+cudaError_t fht_rgc_fused_drift(const FhtGeometry& g, const FhtDriftTables& t, const FhtRgcArgs& a,
+                                cudaStream_t stream);
 // Per-pixel sum of a [S][S] tap table over the in-image taps, (j, i) order.
 cudaError_t tap_table_sum(const float* tab, int r0, int S, int W, int H, float* out,
                           cudaStream_t stream);

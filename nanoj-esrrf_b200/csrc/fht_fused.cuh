@@ -1,0 +1,483 @@
+// fht_fused.cuh -- the fused tile kernel of the FHT-path RGC (liveSRRF_noInterpolation.cl:245-393),
+// shared by rgc_fht.cu (frames without drift) and rgc_fht_drift.cu (launches with drift).
+//
+// 32x64-pixel output tiles; per frame the kernel stages the interpolated tile plus the RGC halo
+// in shared memory, forms the unit gradient field there, and runs the tap loop with each thread
+// owning 8 vertically adjacent outputs so that one shared-memory load feeds up to 8 taps.
+//
+// Tap geometry.  The reference places output pixel xM's centre at xc = xM + 0.5 + sx and takes
+// taps at vx = (int)(xc - 0.5) + i + 0.5, i in [-R, R + 1], so a tap's source column is
+// X = xM + floor(sx) + i and its offset from the centre dx = i - frac(sx) (up to the rounding of
+// xc); the same holds in y.  A frame's shift is uniform over the frame, so the distance weights
+// w and w/d of every tap (i, j) are one table per frame, the source tile moves by
+// (floor(sx), floor(sy)), and the contribution of an inward tap is w - (w/d) |g x (dx, dy)| on
+// the unit gradient g.  Without drift dx = i exactly and the tables are built once.
+//  * DRIFT = false: one table (FusedParams), intensity = the interpolated pixel.
+//  * DRIFT = true: per-frame tables (DriftParams), the source tile at the frame's integer shift,
+//    per-pixel sums of weights from a per-frame 2-D prefix table where the tap box leaves the
+//    image, intensity from a plane sampled at the shifted position (getInterpolatedValue).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "device_common.cuh"
+#include "esrrf_internal.h"
+
+namespace esrrf {
+namespace fused {
+
+constexpr int kTX = 32;          // output columns per CTA (one warp wide)
+constexpr int kTYT = 8;          // thread rows per CTA
+constexpr int kK = 8;            // outputs per thread (vertical)
+constexpr int kTH = kTYT * kK;   // output rows per CTA
+
+// Shared-memory layout for a tap box of side S (S = r1 - r0 + 1, always even).
+template <int S>
+struct FusedLayout {
+    static constexpr int EW = kTX + S - 1, EH = kTH + S - 1;  // unit-gradient tile
+    static constexpr int IW = EW + 2, IH = EH + 2;            // intensity tile (+1 px margin)
+    static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
+    static constexpr size_t off_E = 0;
+    static constexpr size_t off_I = off_E + ((sizeof(float2) * EW * EH + 15) & ~size_t(15));
+    static constexpr size_t tail = ((sizeof(float2) * S * S + sizeof(int) * 2 * S + 15) & ~size_t(15)) +
+                                   sizeof(float) * 5 * kTX * kTH;
+    // A second intensity buffer (the next frame's tile prefetched during this frame's taps) is
+    // used where two CTAs of 256 threads still fit in an SM's 228 KB of shared memory.
+    static constexpr bool kDB = 2 * (off_I + 2 * I_bytes + tail + 1024) <= 228 * 1024;
+    static constexpr int nI = kDB ? 2 : 1;
+    static constexpr size_t off_wt = off_I + nI * I_bytes;
+    static constexpr size_t off_jr = off_wt + sizeof(float2) * S * S;
+    static constexpr size_t off_st = (off_jr + sizeof(int) * 2 * S + 15) & ~size_t(15);
+    static constexpr size_t bytes = off_st + sizeof(float) * 5 * kTX * kTH;
+};
+
+struct FusedParams {
+    int r0;
+    float sens;
+    const float* wtab;
+    const float* wdtab;
+    const int* jrange;
+    const float* wsum;
+};
+
+// Per-frame tables of a launch with drift (frame index local to the launch).
+struct DriftParams {
+    const FhtDriftFrame* fr;  // [F]
+    const float2* wt;         // [F][S][S] (w, w/d), [ii][jj]
+    const int* jr;            // [F][2S] disc chord per column
+    const double* pre;        // [F][S+1][S+1] 2-D prefix sums of w
+    const float* v;           // [F][H][W] intensity at the shifted position
+};
+
+// One column offset i of the tap box for a thread's 8 outputs: source rows rr = 0 .. S+6 of the
+// unit-gradient tile column; row rr feeds output k with tap row jj = rr - k, whose offset from
+// the centre is dy = fr0 + jj (fr0 = r0 without drift, r0 - frac(sy) with), and dx = fi.  CHECK
+// skips rows outside [lo, hi] (columns whose disc chord is not one of the instantiated ranges).
+//
+// The inward test g . (dx, dy) < 0 with dy = fr - k is, for gy > 0, k > fr + dx gx / gy, and the
+// reverse for gy < 0, so one threshold per source row and one compare per output replace the
+// per-output dot product.  gy = +0 gives an infinite threshold of the right sign (the tile stores
+// +0, never -0), a zero gradient a NaN threshold (never inward); 1 / gy is the approximate
+// reciprocal, whose error only moves the threshold within rounding.  The two tests can disagree only
+// where g . (dx, dy) is within rounding of 0, where |g x (dx, dy)| = d and the contribution
+// w - (w / d) |g x (dx, dy)| vanishes quadratically.
+template <int S, bool CHECK>
+__device__ __forceinline__ void tap_column(const float2* __restrict__ col, float fi, float fr0, int lo,
+                                           int hi, const float (&w)[S], const float (&wd)[S],
+                                           float (&acc)[kK]) {
+    constexpr int EW = FusedLayout<S>::EW;
+#pragma unroll
+    for (int rr = 0; rr < S + kK - 1; ++rr) {
+        if (CHECK && (rr < lo || rr > hi)) continue;
+        const float2 e = col[rr * EW];
+        const float fr = fr0 + (float)rr;       // tap row offset of output k = 0
+        float rgy;  // 1 / gy, +-inf for gy = +-0 (subnormals flush to a zero of their sign)
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
+        const float thr = fmaf(e.x * rgy, fi, fr);
+        const bool neg = e.y < 0.f;
+        const float cr0 = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;
+            if (jj >= 0 && jj < S) {
+                // cross = cr0 + k g_x (independent of k - 1)
+                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
+                if (((float)k > thr) != neg) acc[k] += t;
+            }
+        }
+    }
+}
+
+// A column whose disc chord is the compile-time tap-row range [LO, HI]: only the chord's taps
+// are evaluated (rows LO .. HI + 7, and per row only the outputs whose tap row is in the chord).
+template <int S, int LO, int HI>
+__device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float fi, float fr0,
+                                          const float (&w)[S], const float (&wd)[S], float (&acc)[kK]) {
+    constexpr int EW = FusedLayout<S>::EW;
+#pragma unroll
+    for (int rr = LO; rr <= HI + kK - 1; ++rr) {
+        const float2 e = col[rr * EW];
+        const float fr = fr0 + (float)rr;
+        float rgy;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
+        const float thr = fmaf(e.x * rgy, fi, fr);
+        const bool neg = e.y < 0.f;
+        const float cr0 = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int jj = rr - k;
+            if (jj >= LO && jj <= HI) {
+                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
+                if (((float)k > thr) != neg) acc[k] += t;
+            }
+        }
+    }
+}
+
+// Without drift the disc is symmetric in j, so a column's chord inside the box [-R, R+1] is
+// either the whole box or the rows -J .. J, i.e. tap rows [LO, S - 2 - LO]: one instantiation per
+// LO.  With drift the disc's centre sits at frac(sy) in [0, 1) of the box's row 0, so a chord
+// [lo, hi] that does not fill the box has lo + hi in {S - 2, S - 1, S} (D = 0, 1, 2 below).  Any
+// other range takes the generic row-checked loop.
+template <int S, int LO, int D>
+__device__ __forceinline__ void tap_dispatch(const float2* __restrict__ col, float fi, float fr0, int lo,
+                                             int hi, const float (&w)[S], const float (&wd)[S],
+                                             float (&acc)[kK]) {
+    constexpr int HI = S - 2 - LO + D;
+    if constexpr (LO <= HI && HI <= S - 1) {
+        if (lo == LO && hi == HI) {
+            tap_chord<S, LO, HI>(col, fi, fr0, w, wd, acc);
+            return;
+        }
+    }
+    if constexpr (D > 0) {
+        tap_dispatch<S, LO, D - 1>(col, fi, fr0, lo, hi, w, wd, acc);
+    } else if constexpr (LO < S / 2) {
+        tap_dispatch<S, LO + 1, 2>(col, fi, fr0, lo, hi, w, wd, acc);
+    } else {
+        tap_column<S, true>(col, fi, fr0, lo, hi + kK - 1, w, wd, acc);
+    }
+}
+
+template <int S, int LO>
+__device__ __forceinline__ void tap_dispatch_sym(const float2* __restrict__ col, float fi, float fr0, int lo,
+                                                 int hi, const float (&w)[S], const float (&wd)[S],
+                                                 float (&acc)[kK]) {
+    if constexpr (LO <= (S - 2) / 2) {
+        if (lo == LO && hi == S - 2 - LO) {
+            tap_chord<S, LO, S - 2 - LO>(col, fi, fr0, w, wd, acc);
+            return;
+        }
+        tap_dispatch_sym<S, LO + 1>(col, fi, fr0, lo, hi, w, wd, acc);
+    } else {
+        tap_column<S, true>(col, fi, fr0, lo, hi + kK - 1, w, wd, acc);
+    }
+}
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
+// Sum of the tap weights of output (xM, yM) over its in-image taps for a frame with drift: the
+// whole table's sum (in the reference's (j, i) order) where the tap box lies inside the image,
+// else the in-image rectangle of the box from the frame's 2-D prefix table.
+template <int S>
+__device__ __forceinline__ float drift_wsum(const FhtDriftFrame& d, const double* __restrict__ pre, int xM,
+                                            int yM, int r0, int W, int H) {
+    const int bx = xM + d.ix + r0, by = yM + d.iy + r0;  // source of tap (ii, jj) = (0, 0)
+    const int i0 = max(0, -bx), i1 = min(S - 1, W - 1 - bx);
+    const int j0 = max(0, -by), j1 = min(S - 1, H - 1 - by);
+    if (i0 == 0 && i1 == S - 1 && j0 == 0 && j1 == S - 1) return d.wsum_int;
+    if (i0 > i1 || j0 > j1) return 0.f;
+    constexpr int P = S + 1;
+    return (float)(pre[(j1 + 1) * P + i1 + 1] - pre[j0 * P + i1 + 1] - pre[(j1 + 1) * P + i0] +
+                   pre[j0 * P + i0]);
+}
+
+// GROUPED: the launch may split its frames into groups (gridDim.z); the one-group instantiation
+// compiles the frame loop and the fold without the group bookkeeping.
+template <int S, bool GROUPED, bool DRIFT>
+__global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, FusedParams fp, DriftParams dp) {
+    using L = FusedLayout<S>;
+    constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
+    constexpr int r0c = -(S - 2) / 2;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* sE = reinterpret_cast<float2*>(smem + L::off_E);
+    float* sIb = reinterpret_cast<float*>(smem + L::off_I);  // nI buffers of L::I_bytes
+    float2* swt = reinterpret_cast<float2*>(smem + L::off_wt);  // [ii][jj] = (w, w/d)
+    int* sjr = reinterpret_cast<int*>(smem + L::off_jr);
+    float* sst = reinterpret_cast<float*>(smem + L::off_st);    // [5][kTH][kTX]
+
+    const int tid = threadIdx.x;
+    const int tx = tid & 31, ty = tid >> 5;
+    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTH;
+    const int W = a.W, H = a.H;
+    const long wh = (long)W * H;
+
+    if constexpr (!DRIFT) {
+        for (int idx = tid; idx < S * S; idx += blockDim.x) {
+            const int ii = idx / S, jj = idx - ii * S;
+            swt[idx] = make_float2(fp.wtab[jj * S + ii], fp.wdtab[jj * S + ii]);
+        }
+        for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = fp.jrange[i];
+    }
+
+    const int xM = x0 + tx;
+    const bool emit = a.cg_out != nullptr;
+    // frame group: frames [fb, fe) of the launch (one group unless the tiles alone leave SMs
+    // idle); a later group first runs frame fb - 1 only for its intensity-weighted value, the
+    // previous value of TAC2's product at fb
+    const int G = GROUPED ? (int)gridDim.z : 1, grp = GROUPED ? (int)blockIdx.z : 0;
+    const int fb = (int)((long long)a.F * grp / G), fe = (int)((long long)a.F * (grp + 1) / G);
+    const int fs = grp > 0 && !emit ? fb - 1 : fb;
+    float wsum[kK];
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const int yM = y0 + ty * kK + k;
+        const bool in = xM < W && yM < H;
+        const long pix = (long)yM * W + xM;
+        wsum[k] = DRIFT ? 1.f : (in ? fp.wsum[pix] : 1.f);
+        if (emit) continue;
+        const int o = (ty * kK + k) * kTX + tx;
+        sst[0 * kTX * kTH + o] = 0.f;
+        sst[1 * kTX * kTH + o] = 0.f;
+        sst[2 * kTX * kTH + o] = 0.f;
+        sst[3 * kTX * kTH + o] = 0.f;
+        sst[4 * kTX * kTH + o] = in ? a.st.prev[pix] : 0.f;
+    }
+
+    constexpr int kIStride = (int)(L::I_bytes / sizeof(float));
+    // global origin of frame f's intensity tile: the tap box's first source column and row (at
+    // the frame's integer shift) minus the one-pixel margin
+    auto origin = [&](int f, int& gx0, int& gy0) {
+        int ox = 0, oy = 0;
+        if constexpr (DRIFT) {
+            ox = dp.fr[f].ix;
+            oy = dp.fr[f].iy;
+        }
+        gx0 = x0 + ox + r0c - 1;
+        gy0 = y0 + oy + r0c - 1;
+    };
+    // interpolated tile of frame f with a one-pixel margin beyond the gradient halo (clamped
+    // reads), copied asynchronously into dst
+    auto prefetch_tile = [&](int f, float* dst) {
+        int gX0, gY0;
+        origin(f, gX0, gY0);
+        const float* fr = a.interp + (long)f * wh;
+        for (int ly = ty; ly < IH; ly += kTYT) {
+            const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
+            for (int lx = tx; lx < IW; lx += kTX)
+                cp_async4(dst + ly * IW + lx, fr + grow + min(max(gX0 + lx, 0), W - 1));
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (L::kDB && fe > fs) prefetch_tile(fs, sIb);
+
+    for (int f = fs; f < fe; ++f) {
+        float* sI = sIb + (L::kDB ? ((f - fs) & 1) * kIStride : 0);
+        __syncthreads();
+        // 0. this frame's tap tables (drift)
+        FhtDriftFrame df{};
+        float fi0 = (float)r0c, fj0 = (float)r0c;
+        if constexpr (DRIFT) {
+            df = dp.fr[f];
+            fi0 = df.fi0;
+            fj0 = df.fj0;
+            const float2* wt = dp.wt + (long)f * S * S;
+            for (int idx = tid; idx < S * S; idx += blockDim.x) swt[idx] = wt[idx];
+            for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = dp.jr[(long)f * 2 * S + i];
+        }
+        int gX0, gY0;
+        origin(f, gX0, gY0);
+        // 1. this frame's intensity tile: prefetched during the previous frame, or loaded now
+        if (L::kDB) {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        } else {
+            const float* fr = a.interp + (long)f * wh;
+            for (int ly = ty; ly < IH; ly += kTYT) {
+                const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
+                for (int lx = tx; lx < IW; lx += kTX)
+                    sI[ly * IW + lx] = __ldg(fr + grow + min(max(gX0 + lx, 0), W - 1));
+            }
+        }
+        __syncthreads();
+        // 2. unit gradient at each tap source: Gx read at min(X+1, W-1), Gy at min(Y+1, H-1),
+        //    Roberts cross with max(.-1, 0) clamps (liveSRRF_noInterpolation.cl:144-155, 291-292)
+        for (int ey = ty; ey < EH; ey += kTYT) {
+            const int Y = gY0 + 1 + ey;
+            const bool yin = Y >= 0 && Y < H;
+            const int ya0 = max(Y - 1, 0), yb = min(Y + 1, H - 1), yb0 = max(yb - 1, 0);
+            for (int ex = tx; ex < EW; ex += kTX) {
+                const int X = gX0 + 1 + ex;
+                float2 e = make_float2(0.f, 0.f);
+                if (yin && X >= 0 && X < W) {
+                    const int xa = min(X + 1, W - 1), xa0 = max(xa - 1, 0), xb0 = max(X - 1, 0);
+                    const float ga = sI[(ya0 - gY0) * IW + (xa - gX0)];
+                    const float gb = sI[(Y - gY0) * IW + (xa0 - gX0)];
+                    const float gc = sI[(Y - gY0) * IW + (xa - gX0)];
+                    const float gd = sI[(ya0 - gY0) * IW + (xa0 - gX0)];
+                    const float Gx = ga - gb + gc - gd;
+                    const float ha = sI[(yb0 - gY0) * IW + (X - gX0)];
+                    const float hb = sI[(yb - gY0) * IW + (xb0 - gX0)];
+                    const float hc = sI[(yb - gY0) * IW + (X - gX0)];
+                    const float hd = sI[(yb0 - gY0) * IW + (xb0 - gX0)];
+                    const float Gy = -ha + hb + hc - hd;
+                    const float n2 = Gx * Gx + Gy * Gy;
+                    if (n2 > 0.f) {
+                        const float inv = rsqrtf(n2);
+                        e = make_float2(Gx * inv, Gy * inv + 0.f);  // + 0: -0 becomes +0
+                    }
+                }
+                sE[ey * EW + ex] = e;
+            }
+        }
+        __syncthreads();
+        // the next frame's tile goes into the other buffer while this frame's taps run
+        if (L::kDB && f + 1 < fe) prefetch_tile(f + 1, sIb + ((f + 1 - fs) & 1) * kIStride);
+        // 3. tap loop, one box column at a time with its weights in registers
+        float acc[kK];
+#pragma unroll
+        for (int k = 0; k < kK; ++k) acc[k] = 0.f;
+        for (int ii = 0; ii < S; ++ii) {
+            const int lo = sjr[2 * ii], hi = sjr[2 * ii + 1];
+            if (lo > hi) continue;  // no tap of the disc in this column
+            const float fi = fi0 + (float)ii;
+            float w[S], wd[S];
+            const float4* wc = reinterpret_cast<const float4*>(swt + ii * S);
+#pragma unroll
+            for (int q = 0; q < S / 2; ++q) {
+                const float4 v = wc[q];
+                w[2 * q] = v.x;
+                wd[2 * q] = v.y;
+                w[2 * q + 1] = v.z;
+                wd[2 * q + 1] = v.w;
+            }
+            const float2* col = sE + (ty * kK) * EW + tx + ii;
+            if (lo == 0 && hi == S - 1)
+                tap_chord<S, 0, S - 1>(col, fi, fj0, w, wd, acc);
+            else if constexpr (DRIFT)
+                tap_dispatch<S, 0, 2>(col, fi, fj0, lo, hi, w, wd, acc);
+            else
+                tap_dispatch_sym<S, 0>(col, fi, fj0, lo, hi, w, wd, acc);
+        }
+        if constexpr (DRIFT) {
+            const double* pre = dp.pre + (long)f * (S + 1) * (S + 1);
+#pragma unroll
+            for (int k = 0; k < kK; ++k) wsum[k] = drift_wsum<S>(df, pre, xM, y0 + ty * kK + k, r0c, W, H);
+        }
+        // 4. normalisation, sensitivity, intensity weighting and cumulants
+        if (emit) {
+#pragma unroll
+            for (int k = 0; k < kK; ++k) {
+                const int yM = y0 + ty * kK + k;
+                if (xM < W && yM < H) a.cg_out[(long)f * wh + (long)yM * W + xM] = acc[k] / wsum[k];
+            }
+            continue;
+        }
+        const int tglob = a.t0 + f;
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            const int o = (ty * kK + k) * kTX + tx;
+            const float cg = dev::cglh_power(acc[k] / wsum[k], fp.sens);
+            float v;
+            if constexpr (DRIFT) {
+                const int yM = y0 + ty * kK + k;
+                v = xM < W && yM < H ? __ldg(dp.v + (long)f * wh + (long)yM * W + xM) : 0.f;
+            } else {
+                v = sI[(ty * kK + k + 1 - r0c) * IW + (tx + 1 - r0c)];
+            }
+            const float x = a.int_weighting ? v * cg : cg;
+            if (f < fb) {  // the frame before the group: previous value only
+                sst[4 * kTX * kTH + o] = x;
+                continue;
+            }
+            const float pv = sst[4 * kTX * kTH + o];
+            sst[0 * kTX * kTH + o] += x;
+            sst[1 * kTX * kTH + o] += x * x;
+            if (tglob > 0) sst[2 * kTX * kTH + o] += x * pv;
+            sst[3 * kTX * kTH + o] += v;
+            sst[4 * kTX * kTH + o] = x;
+        }
+    }
+    // 5. fold this launch's FP32 partial sums into the block's FP64 accumulators
+    if (emit) return;
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+        const int yM = y0 + ty * kK + k;
+        if (xM >= W || yM >= H) continue;
+        const long pix = (long)yM * W + xM;
+        const int o = (ty * kK + k) * kTX + tx;
+        if (G == 1) {
+            a.st.acc[pix] += (double)sst[0 * kTX * kTH + o];
+            a.st.acc[wh + pix] += (double)sst[1 * kTX * kTH + o];
+            a.st.acc[2 * wh + pix] += (double)sst[2 * kTX * kTH + o];
+            a.st.acc[3 * wh + pix] += (double)sst[3 * kTX * kTH + o];
+        } else {  // several groups add into the same pixels
+#pragma unroll
+            for (int c = 0; c < 4; ++c) atomicAdd(a.st.acc + c * wh + pix, (double)sst[c * kTX * kTH + o]);
+        }
+        if (grp == G - 1) (G == 1 ? a.st.prev : a.prev_out)[pix] = sst[4 * kTX * kTH + o];
+    }
+}
+
+// Launch of one tap-box size: the grid, the frame groups for small frames and the copy of the
+// last group's previous values.
+template <int S, bool DRIFT>
+cudaError_t launch_fused(int r0, float sens, const FusedParams& fp_in, const DriftParams& dp,
+                         const FhtRgcArgs& a, cudaStream_t stream) {
+    constexpr size_t bytes = FusedLayout<S>::bytes;
+    // The opt-in shared-memory size is a per-device function attribute: set it once per device
+    // (also keeps the call out of CUDA-graph captures after the first, uncaptured launch).
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 64 || !(configured & (1ull << dev))) {
+        if ((e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S, false, DRIFT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S, true, DRIFT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)) != cudaSuccess)
+            return e;
+        if (dev < 64) configured |= 1ull << dev;
+    }
+    FusedParams fp = fp_in;
+    fp.r0 = r0;
+    fp.sens = sens;
+    dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
+    // frames split into groups across CTAs only where the tiles alone give fewer than two CTAs
+    // per SM (small frames); a group keeps at least 4 frames when it pays an extra frame
+    const int tiles = (int)(grid.x * grid.y), slots = 2 * sm_count(dev);
+    if (tiles < slots && a.F > 1 && (a.cg_out || a.prev_out)) {
+        const int gmax = a.cg_out ? a.F : std::max(1, a.F / 4);
+        grid.z = (unsigned)std::max(1, std::min({(slots + tiles - 1) / tiles, gmax, 65535}));
+    }
+    if (grid.z > 1)
+        fht_rgc_fused_kernel<S, true, DRIFT><<<grid, 256, bytes, stream>>>(a, fp, dp);
+    else
+        fht_rgc_fused_kernel<S, false, DRIFT><<<grid, 256, bytes, stream>>>(a, fp, dp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (grid.z > 1 && !a.cg_out)
+        return cudaMemcpyAsync(a.st.prev, a.prev_out, sizeof(float) * (size_t)a.W * a.H,
+                               cudaMemcpyDeviceToDevice, stream);
+    return cudaSuccess;
+}
+
+// The tap box side S = 2 * loop radius + 2 is even; one instantiation per size keeps the weight
+// offsets and the tile geometry compile-time constants.  Sizes SLO .. SHI (even) are dispatched
+// here; others return cudaErrorInvalidValue (the caller uses the plain kernel).
+template <bool DRIFT, int SLO, int SHI>
+cudaError_t launch_fused_in(int S, int r0, float sens, const FusedParams& fp, const DriftParams& dp,
+                            const FhtRgcArgs& a, cudaStream_t stream) {
+    if (S == SLO) return launch_fused<SLO, DRIFT>(r0, sens, fp, dp, a, stream);
+    if constexpr (SLO + 2 <= SHI) return launch_fused_in<DRIFT, SLO + 2, SHI>(S, r0, sens, fp, dp, a, stream);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace fused
+}  // namespace esrrf

@@ -19,6 +19,7 @@
 
 #include "device_common.cuh"
 #include "esrrf_internal.h"
+#include "fht_fused.cuh"
 
 namespace esrrf {
 
@@ -171,322 +172,7 @@ __global__ void wsum_kernel(const float* __restrict__ wtab, int r0, int S, int W
     wsum[pix] = s;
 }
 
-// ---------------------------------------------------------------------------------------------
-// Fused tile kernel.
-// ---------------------------------------------------------------------------------------------
-constexpr int kTX = 32;          // output columns per CTA (one warp wide)
-constexpr int kTYT = 8;          // thread rows per CTA
-constexpr int kK = 8;            // outputs per thread (vertical)
-constexpr int kTH = kTYT * kK;   // output rows per CTA
-
-// Shared-memory layout for a tap box of side S (S = r1 - r0 + 1, always even).
-template <int S>
-struct FusedLayout {
-    static constexpr int EW = kTX + S - 1, EH = kTH + S - 1;  // unit-gradient tile
-    static constexpr int IW = EW + 2, IH = EH + 2;            // intensity tile (+1 px margin)
-    static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
-    static constexpr size_t off_E = 0;
-    static constexpr size_t off_I = off_E + ((sizeof(float2) * EW * EH + 15) & ~size_t(15));
-    static constexpr size_t tail = ((sizeof(float2) * S * S + sizeof(int) * 2 * S + 15) & ~size_t(15)) +
-                                   sizeof(float) * 5 * kTX * kTH;
-    // A second intensity buffer (the next frame's tile prefetched during this frame's taps) is
-    // used where two CTAs of 256 threads still fit in an SM's 228 KB of shared memory.
-    static constexpr bool kDB = 2 * (off_I + 2 * I_bytes + tail + 1024) <= 228 * 1024;
-    static constexpr int nI = kDB ? 2 : 1;
-    static constexpr size_t off_wt = off_I + nI * I_bytes;
-    static constexpr size_t off_jr = off_wt + sizeof(float2) * S * S;
-    static constexpr size_t off_st = (off_jr + sizeof(int) * 2 * S + 15) & ~size_t(15);
-    static constexpr size_t bytes = off_st + sizeof(float) * 5 * kTX * kTH;
-};
-
-struct FusedParams {
-    int r0;
-    float sens;
-    const float* wtab;
-    const float* wdtab;
-    const int* jrange;
-    const float* wsum;
-};
-
-// One column offset i of the tap box for a thread's 8 outputs: source rows rr = 0 .. S+6 of the
-// unit-gradient tile column; row rr feeds output k with tap row jj = rr - k, j = r0 + jj, where
-// r0 = -(S - 2) / 2 (the box of an integer radius R is [-R, R + 1]).  CHECK skips rows outside
-// [lo, hi] (columns whose disc chord is shorter than the box).
-//
-// The inward test g . (i, j) < 0 with j = fr - k is, for gy > 0, k > fr + i gx / gy, and the
-// reverse for gy < 0, so one threshold per source row and one compare per output replace the
-// per-output dot product.  gy = +0 gives an infinite threshold of the right sign (the tile stores
-// +0, never -0), a zero gradient a NaN threshold (never inward); 1 / gy is the approximate
-// reciprocal, whose error only moves the threshold within rounding.  The two tests can disagree only
-// where g . (i, j) is within rounding of 0, where |g x (i, j)| = d and the contribution
-// w - (w / d) |g x (i, j)| vanishes quadratically.
-template <int S, bool CHECK>
-__device__ __forceinline__ void tap_column(const float2* __restrict__ col, float fi, int lo, int hi,
-                                           const float (&w)[S], const float (&wd)[S],
-                                           float (&acc)[kK]) {
-    constexpr int EW = FusedLayout<S>::EW;
-    constexpr float fr0 = -(float)((S - 2) / 2);
-#pragma unroll
-    for (int rr = 0; rr < S + kK - 1; ++rr) {
-        if (CHECK && (rr < lo || rr > hi)) continue;
-        const float2 e = col[rr * EW];
-        const float fr = fr0 + (float)rr;       // tap row j of output k = 0
-        float rgy;  // 1 / gy, +-inf for gy = +-0 (subnormals flush to a zero of their sign)
-        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
-        const float thr = fmaf(e.x * rgy, fi, fr);
-        const bool neg = e.y < 0.f;
-        const float cr0 = fmaf(-e.x, fr, e.y * fi);
-#pragma unroll
-        for (int k = 0; k < kK; ++k) {
-            const int jj = rr - k;
-            if (jj >= 0 && jj < S) {
-                // cross = cr0 + k g_x (independent of k - 1)
-                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
-                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
-                if (((float)k > thr) != neg) acc[k] += t;
-            }
-        }
-    }
-}
-
-// A column whose disc chord is the compile-time tap-row range [LO, HI]: only the chord's taps
-// are evaluated (rows LO .. HI + 7, and per row only the outputs whose tap row is in the chord).
-template <int S, int LO, int HI>
-__device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float fi, const float (&w)[S],
-                                          const float (&wd)[S], float (&acc)[kK]) {
-    constexpr int EW = FusedLayout<S>::EW;
-    constexpr float fr0 = -(float)((S - 2) / 2);
-#pragma unroll
-    for (int rr = LO; rr <= HI + kK - 1; ++rr) {
-        const float2 e = col[rr * EW];
-        const float fr = fr0 + (float)rr;
-        float rgy;
-        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
-        const float thr = fmaf(e.x * rgy, fi, fr);
-        const bool neg = e.y < 0.f;
-        const float cr0 = fmaf(-e.x, fr, e.y * fi);
-#pragma unroll
-        for (int k = 0; k < kK; ++k) {
-            const int jj = rr - k;
-            if (jj >= LO && jj <= HI) {
-                const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
-                const float t = fmaf(-fabsf(ck), wd[jj], w[jj]);
-                if (((float)k > thr) != neg) acc[k] += t;
-            }
-        }
-    }
-}
-
-// The disc is symmetric in j, so a column's chord inside the box [-R, R+1] is either the whole
-// box or the rows -J .. J, i.e. tap rows [LO, S - 2 - LO]: one instantiation per LO.  Any other
-// range takes the generic row-checked loop.
-template <int S, int LO>
-__device__ __forceinline__ void tap_dispatch(const float2* __restrict__ col, float fi, int lo, int hi,
-                                             const float (&w)[S], const float (&wd)[S],
-                                             float (&acc)[kK]) {
-    if constexpr (LO <= (S - 2) / 2) {
-        if (lo == LO && hi == S - 2 - LO) {
-            tap_chord<S, LO, S - 2 - LO>(col, fi, w, wd, acc);
-            return;
-        }
-        tap_dispatch<S, LO + 1>(col, fi, lo, hi, w, wd, acc);
-    } else {
-        tap_column<S, true>(col, fi, lo, hi + kK - 1, w, wd, acc);
-    }
-}
-
-__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
-}
-
-// GROUPED: the launch may split its frames into groups (gridDim.z); the one-group instantiation
-// compiles the frame loop and the fold without the group bookkeeping.
-template <int S, bool GROUPED>
-__global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, FusedParams fp) {
-    using L = FusedLayout<S>;
-    constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
-    extern __shared__ __align__(16) unsigned char smem[];
-    float2* sE = reinterpret_cast<float2*>(smem + L::off_E);
-    float* sIb = reinterpret_cast<float*>(smem + L::off_I);  // nI buffers of L::I_bytes
-    float2* swt = reinterpret_cast<float2*>(smem + L::off_wt);  // [ii][jj] = (w, w/d)
-    int* sjr = reinterpret_cast<int*>(smem + L::off_jr);
-    float* sst = reinterpret_cast<float*>(smem + L::off_st);    // [5][kTH][kTX]
-
-    const int tid = threadIdx.x;
-    const int tx = tid & 31, ty = tid >> 5;
-    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTH;
-    const int r0 = fp.r0;
-    const int W = a.W, H = a.H;
-    const long wh = (long)W * H;
-
-    for (int idx = tid; idx < S * S; idx += blockDim.x) {
-        const int ii = idx / S, jj = idx - ii * S;
-        swt[idx] = make_float2(fp.wtab[jj * S + ii], fp.wdtab[jj * S + ii]);
-    }
-    for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = fp.jrange[i];
-
-    const int xM = x0 + tx;
-    const bool emit = a.cg_out != nullptr;
-    // frame group: frames [fb, fe) of the launch (one group unless the tiles alone leave SMs
-    // idle); a later group first runs frame fb - 1 only for its intensity-weighted value, the
-    // previous value of TAC2's product at fb
-    const int G = GROUPED ? (int)gridDim.z : 1, grp = GROUPED ? (int)blockIdx.z : 0;
-    const int fb = (int)((long long)a.F * grp / G), fe = (int)((long long)a.F * (grp + 1) / G);
-    const int fs = grp > 0 && !emit ? fb - 1 : fb;
-    float wsum[kK];
-#pragma unroll
-    for (int k = 0; k < kK; ++k) {
-        const int yM = y0 + ty * kK + k;
-        const bool in = xM < W && yM < H;
-        const long pix = (long)yM * W + xM;
-        wsum[k] = in ? fp.wsum[pix] : 1.f;
-        if (emit) continue;
-        const int o = (ty * kK + k) * kTX + tx;
-        sst[0 * kTX * kTH + o] = 0.f;
-        sst[1 * kTX * kTH + o] = 0.f;
-        sst[2 * kTX * kTH + o] = 0.f;
-        sst[3 * kTX * kTH + o] = 0.f;
-        sst[4 * kTX * kTH + o] = in ? a.st.prev[pix] : 0.f;
-    }
-
-    const int gX0 = x0 + r0 - 1, gY0 = y0 + r0 - 1;  // global origin of the intensity tile
-    const float fr0 = (float)r0;
-    constexpr int kIStride = (int)(L::I_bytes / sizeof(float));
-    // interpolated tile of frame f with a one-pixel margin beyond the gradient halo (clamped
-    // reads), copied asynchronously into dst
-    auto prefetch_tile = [&](int f, float* dst) {
-        const float* fr = a.interp + (long)f * wh;
-        for (int ly = ty; ly < IH; ly += kTYT) {
-            const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
-            for (int lx = tx; lx < IW; lx += kTX)
-                cp_async4(dst + ly * IW + lx, fr + grow + min(max(gX0 + lx, 0), W - 1));
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-    if (L::kDB && fe > fs) prefetch_tile(fs, sIb);
-
-    for (int f = fs; f < fe; ++f) {
-        float* sI = sIb + (L::kDB ? ((f - fs) & 1) * kIStride : 0);
-        __syncthreads();
-        // 1. this frame's intensity tile: prefetched during the previous frame, or loaded now
-        if (L::kDB) {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        } else {
-            const float* fr = a.interp + (long)f * wh;
-            for (int ly = ty; ly < IH; ly += kTYT) {
-                const long grow = (long)min(max(gY0 + ly, 0), H - 1) * W;
-                for (int lx = tx; lx < IW; lx += kTX)
-                    sI[ly * IW + lx] = __ldg(fr + grow + min(max(gX0 + lx, 0), W - 1));
-            }
-        }
-        __syncthreads();
-        // 2. unit gradient at each tap source: Gx read at min(X+1, W-1), Gy at min(Y+1, H-1),
-        //    Roberts cross with max(.-1, 0) clamps (liveSRRF_noInterpolation.cl:144-155, 291-292)
-        for (int ey = ty; ey < EH; ey += kTYT) {
-            const int Y = y0 + r0 + ey;
-            const bool yin = Y >= 0 && Y < H;
-            const int ya0 = max(Y - 1, 0), yb = min(Y + 1, H - 1), yb0 = max(yb - 1, 0);
-            for (int ex = tx; ex < EW; ex += kTX) {
-                const int X = x0 + r0 + ex;
-                float2 e = make_float2(0.f, 0.f);
-                if (yin && X >= 0 && X < W) {
-                    const int xa = min(X + 1, W - 1), xa0 = max(xa - 1, 0), xb0 = max(X - 1, 0);
-                    const float ga = sI[(ya0 - gY0) * IW + (xa - gX0)];
-                    const float gb = sI[(Y - gY0) * IW + (xa0 - gX0)];
-                    const float gc = sI[(Y - gY0) * IW + (xa - gX0)];
-                    const float gd = sI[(ya0 - gY0) * IW + (xa0 - gX0)];
-                    const float Gx = ga - gb + gc - gd;
-                    const float ha = sI[(yb0 - gY0) * IW + (X - gX0)];
-                    const float hb = sI[(yb - gY0) * IW + (xb0 - gX0)];
-                    const float hc = sI[(yb - gY0) * IW + (X - gX0)];
-                    const float hd = sI[(yb0 - gY0) * IW + (xb0 - gX0)];
-                    const float Gy = -ha + hb + hc - hd;
-                    const float n2 = Gx * Gx + Gy * Gy;
-                    if (n2 > 0.f) {
-                        const float inv = rsqrtf(n2);
-                        e = make_float2(Gx * inv, Gy * inv + 0.f);  // + 0: -0 becomes +0
-                    }
-                }
-                sE[ey * EW + ex] = e;
-            }
-        }
-        __syncthreads();
-        // the next frame's tile goes into the other buffer while this frame's taps run
-        if (L::kDB && f + 1 < fe) prefetch_tile(f + 1, sIb + ((f + 1 - fs) & 1) * kIStride);
-        // 3. tap loop, one box column at a time with its weights in registers
-        float acc[kK];
-#pragma unroll
-        for (int k = 0; k < kK; ++k) acc[k] = 0.f;
-        for (int ii = 0; ii < S; ++ii) {
-            const int lo = sjr[2 * ii], hi = sjr[2 * ii + 1];
-            if (lo > hi) continue;  // no tap of the disc in this column
-            const float fi = fr0 + (float)ii;
-            float w[S], wd[S];
-            const float4* wc = reinterpret_cast<const float4*>(swt + ii * S);
-#pragma unroll
-            for (int q = 0; q < S / 2; ++q) {
-                const float4 v = wc[q];
-                w[2 * q] = v.x;
-                wd[2 * q] = v.y;
-                w[2 * q + 1] = v.z;
-                wd[2 * q + 1] = v.w;
-            }
-            const float2* col = sE + (ty * kK) * EW + tx + ii;
-            if (lo == 0 && hi == S - 1)
-                tap_chord<S, 0, S - 1>(col, fi, w, wd, acc);
-            else
-                tap_dispatch<S, 0>(col, fi, lo, hi, w, wd, acc);
-        }
-        // 4. normalisation, sensitivity, intensity weighting and cumulants
-        if (emit) {
-#pragma unroll
-            for (int k = 0; k < kK; ++k) {
-                const int yM = y0 + ty * kK + k;
-                if (xM < W && yM < H) a.cg_out[(long)f * wh + (long)yM * W + xM] = acc[k] / wsum[k];
-            }
-            continue;
-        }
-        const int tglob = a.t0 + f;
-#pragma unroll
-        for (int k = 0; k < kK; ++k) {
-            const int o = (ty * kK + k) * kTX + tx;
-            const float cg = cglh_power(acc[k] / wsum[k], fp.sens);
-            const float v = sI[(ty * kK + k + 1 - r0) * IW + (tx + 1 - r0)];
-            const float x = a.int_weighting ? v * cg : cg;
-            if (f < fb) {  // the frame before the group: previous value only
-                sst[4 * kTX * kTH + o] = x;
-                continue;
-            }
-            const float pv = sst[4 * kTX * kTH + o];
-            sst[0 * kTX * kTH + o] += x;
-            sst[1 * kTX * kTH + o] += x * x;
-            if (tglob > 0) sst[2 * kTX * kTH + o] += x * pv;
-            sst[3 * kTX * kTH + o] += v;
-            sst[4 * kTX * kTH + o] = x;
-        }
-    }
-    // 5. fold this launch's FP32 partial sums into the block's FP64 accumulators
-    if (emit) return;
-#pragma unroll
-    for (int k = 0; k < kK; ++k) {
-        const int yM = y0 + ty * kK + k;
-        if (xM >= W || yM >= H) continue;
-        const long pix = (long)yM * W + xM;
-        const int o = (ty * kK + k) * kTX + tx;
-        if (G == 1) {
-            a.st.acc[pix] += (double)sst[0 * kTX * kTH + o];
-            a.st.acc[wh + pix] += (double)sst[1 * kTX * kTH + o];
-            a.st.acc[2 * wh + pix] += (double)sst[2 * kTX * kTH + o];
-            a.st.acc[3 * wh + pix] += (double)sst[3 * kTX * kTH + o];
-        } else {  // several groups add into the same pixels
-#pragma unroll
-            for (int c = 0; c < 4; ++c) atomicAdd(a.st.acc + c * wh + pix, (double)sst[c * kTX * kTH + o]);
-        }
-        if (grp == G - 1) (G == 1 ? a.st.prev : a.prev_out)[pix] = sst[4 * kTX * kTH + o];
-    }
-}
+}  // namespace
 
 // Multiprocessor count of a device, queried once per device.
 int sm_count(int dev) {
@@ -503,43 +189,7 @@ int sm_count(int dev) {
     return cache[dev];
 }
 
-template <int S>
-cudaError_t launch_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
-                         cudaStream_t stream) {
-    constexpr size_t bytes = FusedLayout<S>::bytes;
-    // The opt-in shared-memory size is a per-device function attribute: set it once per device
-    // (also keeps the call out of CUDA-graph captures after the first, uncaptured launch).
-    static unsigned long long configured = 0;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev >= 64 || !(configured & (1ull << dev))) {
-        if ((e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)bytes)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(fht_rgc_fused_kernel<S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)bytes)) != cudaSuccess)
-            return e;
-        if (dev < 64) configured |= 1ull << dev;
-    }
-    FusedParams fp{g.r0, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
-    dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
-    // frames split into groups across CTAs only where the tiles alone give fewer than two CTAs
-    // per SM (small frames); a group keeps at least 4 frames when it pays an extra frame
-    const int tiles = (int)(grid.x * grid.y), slots = 2 * sm_count(dev);
-    if (tiles < slots && a.F > 1 && (a.cg_out || a.prev_out)) {
-        const int gmax = a.cg_out ? a.F : std::max(1, a.F / 4);
-        grid.z = (unsigned)std::max(1, std::min({(slots + tiles - 1) / tiles, gmax, 65535}));
-    }
-    if (grid.z > 1)
-        fht_rgc_fused_kernel<S, true><<<grid, 256, bytes, stream>>>(a, fp);
-    else
-        fht_rgc_fused_kernel<S, false><<<grid, 256, bytes, stream>>>(a, fp);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (grid.z > 1 && !a.cg_out)
-        return cudaMemcpyAsync(a.st.prev, a.prev_out, sizeof(float) * (size_t)a.W * a.H,
-                               cudaMemcpyDeviceToDevice, stream);
-    return cudaSuccess;
-}
+namespace {
 
 __global__ void finalize_kernel(BlockState st, int n, int tac_div2, float* __restrict__ out) {
     const long pix = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -607,26 +257,8 @@ void fht_fused_tables_free(FhtFusedTables& t) {
 
 cudaError_t fht_rgc_fused(const FhtGeometry& g, const FhtFusedTables& t, const FhtRgcArgs& a,
                           cudaStream_t stream) {
-    // The tap box side S = 2 * loop radius + 2 is even; one instantiation per size keeps the
-    // weight offsets and the tile geometry compile-time constants.
-    switch (g.S) {
-        case 4: return launch_fused<4>(g, t, a, stream);
-        case 6: return launch_fused<6>(g, t, a, stream);
-        case 8: return launch_fused<8>(g, t, a, stream);
-        case 10: return launch_fused<10>(g, t, a, stream);
-        case 12: return launch_fused<12>(g, t, a, stream);
-        case 14: return launch_fused<14>(g, t, a, stream);
-        case 16: return launch_fused<16>(g, t, a, stream);
-        case 18: return launch_fused<18>(g, t, a, stream);
-        case 20: return launch_fused<20>(g, t, a, stream);
-        case 22: return launch_fused<22>(g, t, a, stream);
-        case 24: return launch_fused<24>(g, t, a, stream);
-        case 26: return launch_fused<26>(g, t, a, stream);
-        case 28: return launch_fused<28>(g, t, a, stream);
-        case 30: return launch_fused<30>(g, t, a, stream);
-        case 32: return launch_fused<32>(g, t, a, stream);
-        default: return cudaErrorInvalidValue;  // caller uses the plain kernel
-    }
+    const fused::FusedParams fp{g.r0, g.sensitivity, t.wtab, t.wdtab, t.jrange, t.wsum};
+    return fused::launch_fused_in<false, 4, 32>(g.S, g.r0, g.sensitivity, fp, fused::DriftParams{}, a, stream);
 }
 
 // Sum of a tap table over the in-image taps of every pixel (the wsum_kernel above, exported).

@@ -1,20 +1,31 @@
-// sweep.cu -- batched parameter sweep and rolling analysis over uneven frame blocks.
+// sweep.cu -- batched parameter sweep and rolling analysis over uneven frame blocks, on one or
+// several devices.
 //
 // The reference's ParametersSweep_ (gui/ParametersSweep_.java:328-519) re-initialises the
 // engine -- context, program build, buffers, per-frame upload -- for every (radius, sensitivity)
 // combination, and its rolling analysis (gui/LiveSRRF_optimised_.java:276-389) recomputes every
-// frame once per block that contains it.  Here one captured CUDA graph does the whole sweep:
+// frame once per block that contains it.  Here one captured CUDA graph per device does the work:
 //   per magnification: Fourier-interpolate every frame once (interp.cu);
 //   per radius: one fused-RGC launch over all frames that writes CGLH / sum-of-weights per frame
 //     (the tap loop is shared by every sensitivity and every block);
 //   per (sensitivity group, block group): one memory-bound launch that raises CGLH to the
-//     sensitivity, weights it by the interpolated intensity and reduces AVG/VAR/TAC2/INT over each
-//     block, FP64 accumulators in registers.
+//     sensitivity, weights it by the intensity and reduces AVG/VAR/TAC2/INT over each block, FP64
+//     accumulators in registers.
+// With drift (the sweep's vibration correction: one shift per frame of the stack,
+// gui/ParametersSweep_.java:282-290, loaded into every combination's engine at :452-454) the RGC
+// launch takes per-frame tap tables (rgc_fht_drift.cu) and the intensity is each frame's
+// getInterpolatedValue at its shifted position, sampled once per magnification.
 // The bicubic sweep (the reference sweep with "Use FHT interpolation" off) computes the 2-point
 // gradients, their 2x resampling and the unit-gradient field of every frame once (none depends on
 // the magnification or radius); per (magnification, radius) the tabulated bicubic RGC writes
 // CGLH / sum of weights and the bicubic intensity of every frame; the cumulant launches apply the
 // path's double (n - 1) division of TAC2, and every output gets the MP correction.
+//
+// Several devices: the (magnification, radius) pairs, or the blocks, are split across the devices
+// (plan_shards below: longest-processing-time assignment of pairs by tap-count cost, or contiguous
+// runs of blocks of balanced frame span, whichever finishes first); each device holds its own copy
+// of the frames its part needs and runs its own graph; nothing crosses between devices and the
+// results are gathered into the host output.
 // Output: for each magnification, radius, sensitivity and block, the four [HM][WM] slices of
 // readSRRFbuffer (AVG, VAR, TAC2, INT; NaN -> 0).
 #include <string.h>
@@ -22,6 +33,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/esrrf.h"
@@ -118,24 +130,34 @@ __global__ void __launch_bounds__(256) sweep_cumulants_kernel(CumArgs a) {
     }
 }
 
+// One magnification of a shard and the radii it handles at that magnification.
 struct MagPlan {
-    int M = 0;
+    int M = 0, mi = 0;                  // magnification and its index in the sweep
+    std::vector<int> ri;                // radius indices (into the sweep's radii)
     InterpPlan plan;
-    std::vector<FhtGeometry> geo;       // per radius
-    std::vector<FhtFusedTables> tables; // per radius
-    std::vector<BicGeometry> bgeo;      // bicubic sweep: per radius
-    std::vector<BicTables> btab;        // bicubic sweep: per radius (common field padding)
+    std::vector<FhtGeometry> geo;       // per entry of ri
+    std::vector<FhtFusedTables> tables; // per entry of ri
+    std::vector<BicGeometry> bgeo;      // bicubic sweep: per entry of ri
+    std::vector<BicTables> btab;        // bicubic sweep: per entry of ri (common field padding)
+    float* d_shift = nullptr;           // drift x M, [2][T] (FHT sweep with drift)
 };
 
-}  // namespace
+std::string cuda_msg(cudaError_t e, const char* what) {
+    return std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+}
 
-struct esrrf_sweep {
-    esrrf_sweep_params p{};
-    std::vector<int> mags, sens, bstart, blen;
-    std::vector<float> radii;
+// One device's part of a sweep: a set of (magnification, radius) pairs over the frames
+// [f0, f0 + T) of the stack, which hold its blocks.
+struct Shard {
     int device = -1;
     cudaStream_t stream = nullptr;
+    int w = 0, h = 0, T = 0, f0 = 0;
+    int int_weighting = 1;
+    std::vector<int> sens, bstart, blen, bglob;  // blocks: local start, length, global index
     std::vector<MagPlan> mp;
+    bool drift = false;
+    std::vector<float> dx, dy;                  // [T] raw pixels (drift)
+    FhtDriftTables dtab;                        // per-frame tap tables + shifted intensities
     InterpScratch scratch;
     float* d_interp = nullptr;  // [T][HM][WM] for the largest magnification
     float* d_cg = nullptr;
@@ -150,7 +172,7 @@ struct esrrf_sweep {
     float* d_gyi = nullptr;
     float2* d_u2 = nullptr;
     float* d_mpmap = nullptr;
-    std::vector<size_t> offsets;
+    std::vector<size_t> offsets;  // local layout: per (mp entry, radius entry) in order
     size_t total = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -166,11 +188,14 @@ struct esrrf_sweep {
     }
     esrrf_status fail_cuda(cudaError_t e, const char* what) {
         cudaGetLastError();
-        return fail(e == cudaErrorMemoryAllocation ? ESRRF_ERR_NOMEM : ESRRF_ERR_CUDA,
-                    std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+        return fail(e == cudaErrorMemoryAllocation ? ESRRF_ERR_NOMEM : ESRRF_ERR_CUDA, cuda_msg(e, what));
     }
+    esrrf_status create(const std::vector<float>& radii, int interp);
+    esrrf_status create_bic(const std::vector<float>& radii);
     esrrf_status enqueue(const void* frames, int is_u16, float* out);
     esrrf_status enqueue_bic(const void* frames, int is_u16, float* out);
+    esrrf_status tc_check();
+    esrrf_status run_device(const void* d_frames, int is_u16, float* d_out);
     void release();
 };
 
@@ -179,13 +204,18 @@ struct esrrf_sweep {
         cudaError_t _e = (call);                               \
         if (_e != cudaSuccess) return s->fail_cuda(_e, what);  \
     } while (0)
+#define SKS(call, what)                                         \
+    do {                                                        \
+        cudaError_t _e = (call);                                \
+        if (_e != cudaSuccess) return sh->fail_cuda(_e, what);  \
+    } while (0)
 
-esrrf_status esrrf_sweep::enqueue(const void* frames, int is_u16, float* out) {
-    esrrf_sweep* s = this;
-    const int T = p.n_frames;
-    const size_t fb = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)p.width * p.height;
+esrrf_status Shard::enqueue(const void* frames, int is_u16, float* out) {
+    Shard* s = this;
+    const size_t fb = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)w * h;
     int launches = 0;
     if (bic) return enqueue_bic(frames, is_u16, out);
+    size_t oi = 0;
     for (size_t mi = 0; mi < mp.size(); ++mi) {
         const MagPlan& m = mp[mi];
         const long P = (long)m.plan.WM * m.plan.HM;
@@ -195,23 +225,36 @@ esrrf_status esrrf_sweep::enqueue(const void* frames, int is_u16, float* out) {
                           d_interp + (size_t)t * P, stream, &launches),
                "interpolation");
         }
-        for (size_t ri = 0; ri < radii.size(); ++ri) {
+        const float* vsrc = d_interp;
+        if (drift) {  // every frame's intensity at its shifted position, shared by the radii
+            SK(fht_shift_sample(d_interp, m.plan.WM, m.plan.HM, T, m.d_shift, m.d_shift + T, dtab.v, stream),
+               "shifted intensities");
+            ++launches;
+            vsrc = dtab.v;
+        }
+        for (size_t e = 0; e < m.ri.size(); ++e, ++oi) {
             FhtRgcArgs a{};
             a.interp = d_interp;
             a.W = m.plan.WM;
             a.H = m.plan.HM;
             a.F = T;
             a.t0 = 0;
-            a.int_weighting = p.int_weighting;
+            a.int_weighting = int_weighting;
             a.cg_out = d_cg;
-            SK(fht_rgc_fused(m.geo[ri], m.tables[ri], a, stream), "RGC");
-            ++launches;
-            float* base = out + offsets[mi * radii.size() + ri];
+            if (drift) {
+                SK(fht_drift_tables_build(m.geo[e], m.d_shift, m.d_shift + T, T, dtab, stream), "drift tables");
+                SK(fht_rgc_fused_drift(m.geo[e], dtab, a, stream), "RGC");
+                launches += 2;
+            } else {
+                SK(fht_rgc_fused(m.geo[e], m.tables[e], a, stream), "RGC");
+                ++launches;
+            }
+            float* base = out + offsets[oi];
             for (int s0 = 0; s0 < (int)sens.size(); s0 += kSG)
                 for (int b0 = 0; b0 < (int)bstart.size(); b0 += kBG) {
                     CumArgs c{};
                     c.cg = d_cg;
-                    c.v = d_interp;
+                    c.v = vsrc;
                     c.P = P;
                     c.nb = std::min(kBG, (int)bstart.size() - b0);
                     for (int b = 0; b < c.nb; ++b) {
@@ -220,7 +263,7 @@ esrrf_status esrrf_sweep::enqueue(const void* frames, int is_u16, float* out) {
                     }
                     c.ns = std::min(kSG, (int)sens.size() - s0);
                     for (int q = 0; q < c.ns; ++q) c.sens[q] = (float)sens[s0 + q];
-                    c.int_weighting = p.int_weighting;
+                    c.int_weighting = int_weighting;
                     c.out = base;
                     c.s0 = s0;
                     c.b0 = b0;
@@ -235,18 +278,18 @@ esrrf_status esrrf_sweep::enqueue(const void* frames, int is_u16, float* out) {
     return ESRRF_OK;
 }
 
-esrrf_status esrrf_sweep::enqueue_bic(const void* frames, int is_u16, float* out) {
-    esrrf_sweep* s = this;
-    const int T = p.n_frames, w = p.width, h = p.height;
+esrrf_status Shard::enqueue_bic(const void* frames, int is_u16, float* out) {
+    Shard* s = this;
     int launches = 0;
     SK(bic_prepare(frames, is_u16, w, h, T, d_fraw, d_gx, d_gy, d_gxi, d_gyi, stream), "gradients");
     launches += 3;
     SK(unit_grad2d(d_gxi, d_gyi, w, h, T, mp[0].btab[0], d_u2, stream), "unit gradient");
     ++launches;
+    size_t oi = 0;
     for (size_t mi = 0; mi < mp.size(); ++mi) {
         const MagPlan& m = mp[mi];
         const long P = (long)w * m.M * h * m.M;
-        for (size_t ri = 0; ri < radii.size(); ++ri) {
+        for (size_t e = 0; e < m.ri.size(); ++e, ++oi) {
             BicTabArgs a{};
             a.U = d_u2;
             a.fraw = d_fraw;
@@ -256,13 +299,13 @@ esrrf_status esrrf_sweep::enqueue_bic(const void* frames, int is_u16, float* out
             a.F = T;
             a.t0 = 0;
             a.sens = 1.f;
-            a.int_weighting = p.int_weighting;
-            a.tab = m.btab[ri];
+            a.int_weighting = int_weighting;
+            a.tab = m.btab[e];
             a.cg_out = d_cg;
             a.v_out = d_interp;
             SK(bic_rgc_tab(a, stream), "RGC");
             ++launches;
-            float* base = out + offsets[mi * radii.size() + ri];
+            float* base = out + offsets[oi];
             for (int s0 = 0; s0 < (int)sens.size(); s0 += kSG)
                 for (int b0 = 0; b0 < (int)bstart.size(); b0 += kBG) {
                     CumArgs c{};
@@ -276,7 +319,7 @@ esrrf_status esrrf_sweep::enqueue_bic(const void* frames, int is_u16, float* out
                     }
                     c.ns = std::min(kSG, (int)sens.size() - s0);
                     for (int q = 0; q < c.ns; ++q) c.sens[q] = (float)sens[s0 + q];
-                    c.int_weighting = p.int_weighting;
+                    c.int_weighting = int_weighting;
                     c.tac_div2 = 1;
                     c.out = base;
                     c.s0 = s0;
@@ -297,7 +340,7 @@ esrrf_status esrrf_sweep::enqueue_bic(const void* frames, int is_u16, float* out
     return ESRRF_OK;
 }
 
-void esrrf_sweep::release() {
+void Shard::release() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
     if (exec) cudaGraphExecDestroy(exec);
@@ -308,7 +351,9 @@ void esrrf_sweep::release() {
         interp_plan_destroy(m.plan);
         for (auto& t : m.tables) fht_fused_tables_free(t);
         for (auto& t : m.btab) bic_tables_free(t);
+        cudaFree(m.d_shift);
     }
+    fht_drift_tables_free(dtab);
     for (float* b : {d_fraw, d_gx, d_gy, d_gxi, d_gyi, d_mpmap}) cudaFree(b);
     cudaFree(d_u2);
     d_fraw = d_gx = d_gy = d_gxi = d_gyi = d_mpmap = nullptr;
@@ -318,56 +363,51 @@ void esrrf_sweep::release() {
     cudaFree(scratch.xs);
     cudaFree(scratch.alt);
     cudaFree(scratch.vec);
+    scratch = InterpScratch();
     cudaFree(d_interp);
     cudaFree(d_cg);
     cudaFree(d_in);
     cudaFree(d_outbuf);
+    d_interp = d_cg = d_outbuf = nullptr;
+    d_in = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
 
-namespace {
-std::mutex g_sweep_mu;
-std::string g_sweep_create_error;
-}  // namespace
-
 // Bicubic sweep set-up: per (magnification, radius) tap tables, all on one unit-gradient field
-// whose zero halo is the widest any table needs; per-frame buffers for the whole stack.
-static esrrf_status sweep_create_bic(esrrf_sweep* s) {
-    const int w = s->p.width, h = s->p.height, T = s->p.n_frames;
+// whose zero halo is the widest any table needs; per-frame buffers for the shard's frames.
+esrrf_status Shard::create_bic(const std::vector<float>& radii) {
+    Shard* s = this;
     cudaError_t e;
     long maxP = 0;
     int padx = 0, pady = 0;
-    s->total = 0;
-    for (int M : s->mags) {
-        s->mp.emplace_back();
-        MagPlan& m = s->mp.back();
-        m.M = M;
-        const long P = (long)w * M * h * M;
+    total = 0;
+    for (auto& m : mp) {
+        const long P = (long)w * m.M * h * m.M;
         maxP = std::max(maxP, P);
-        for (float r : s->radii) {
-            const BicGeometry g = bic_geometry(r, 1);
+        for (int r : m.ri) {
+            const BicGeometry g = bic_geometry(radii[r], 1);
             BicTables t;
             bool built = false;
-            if ((e = bic_tables_build(g, M, w, h, t, built, s->stream)) != cudaSuccess) {
+            if ((e = bic_tables_build(g, m.M, w, h, t, built, stream)) != cudaSuccess) {
                 bic_tables_free(t);
-                return s->fail_cuda(e, "RGC tables");
+                return fail_cuda(e, "RGC tables");
             }
             if (!built) {
                 bic_tables_free(t);
-                return s->fail(ESRRF_ERR_INVALID, "radius " + std::to_string(r) + " at magnification " +
-                                                      std::to_string(M) + " reaches too far for the tabulated "
-                                                      "bicubic kernel (shared memory or slab row width)");
+                return fail(ESRRF_ERR_INVALID, "radius " + std::to_string(radii[r]) + " at magnification " +
+                                                   std::to_string(m.M) + " reaches too far for the tabulated "
+                                                   "bicubic kernel (shared memory or slab row width)");
             }
             padx = std::max(padx, t.padx);
             pady = std::max(pady, t.pady);
             m.bgeo.push_back(g);
             m.btab.push_back(t);
-            s->offsets.push_back(s->total);
-            s->total += (size_t)s->sens.size() * s->bstart.size() * 4 * P;
+            offsets.push_back(total);
+            total += (size_t)sens.size() * bstart.size() * 4 * P;
         }
     }
-    for (auto& m : s->mp)
+    for (auto& m : mp)
         for (auto& t : m.btab) {
             t.padx = padx;  // even: every table's padx is
             t.pady = pady;
@@ -375,35 +415,276 @@ static esrrf_status sweep_create_bic(esrrf_sweep* s) {
             t.H2p = 2 * h + 2 * pady;
         }
     const size_t plane = (size_t)w * h;
-    const size_t field = bic_field_float2s(s->mp[0].btab[0], T);
+    const size_t field = bic_field_float2s(mp[0].btab[0], T);
     int maxM = 1;
-    for (int M : s->mags) maxM = std::max(maxM, M);
-    if ((e = cudaMalloc(&s->d_fraw, sizeof(float) * T * plane)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_gx, sizeof(float) * T * plane)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_gy, sizeof(float) * T * plane)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_gxi, sizeof(float) * T * 4 * plane)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_gyi, sizeof(float) * T * 4 * plane)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_u2, sizeof(float2) * field)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_mpmap, sizeof(float) * 3 * maxM * maxM)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_cg, sizeof(float) * (size_t)T * maxP)) != cudaSuccess)
-        return s->fail_cuda(e, "sweep buffers");
-    if ((e = cudaMemsetAsync(s->d_u2, 0, sizeof(float2) * field, s->stream)) != cudaSuccess)  // zero halo
-        return s->fail_cuda(e, "sweep buffers");
-    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return s->fail_cuda(e, "sync");
+    for (auto& m : mp) maxM = std::max(maxM, m.M);
+    if ((e = cudaMalloc(&d_fraw, sizeof(float) * T * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&d_gx, sizeof(float) * T * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&d_gy, sizeof(float) * T * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&d_gxi, sizeof(float) * T * 4 * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&d_gyi, sizeof(float) * T * 4 * plane)) != cudaSuccess ||
+        (e = cudaMalloc(&d_u2, sizeof(float2) * field)) != cudaSuccess ||
+        (e = cudaMalloc(&d_mpmap, sizeof(float) * 3 * maxM * maxM)) != cudaSuccess ||
+        (e = cudaMalloc(&d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||
+        (e = cudaMalloc(&d_cg, sizeof(float) * (size_t)T * maxP)) != cudaSuccess)
+        return fail_cuda(e, "sweep buffers");
+    if ((e = cudaMemsetAsync(d_u2, 0, sizeof(float2) * field, stream)) != cudaSuccess)  // zero halo
+        return fail_cuda(e, "sweep buffers");
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return fail_cuda(e, "sync");
     return ESRRF_OK;
 }
 
-extern "C" {
+esrrf_status Shard::create(const std::vector<float>& radii, int interp) {
+    Shard* s = this;
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail_cuda(e, "stream");
+    if (interp == ESRRF_INTERP_BIC) {
+        bic = true;
+        return create_bic(radii);
+    }
+    long maxP = 0;
+    int maxN = 0, maxWM = 0, maxS = 4;
+    total = 0;
+    for (auto& m : mp) {
+        if ((e = interp_plan_create(m.plan, w, h, m.M, 0)) != cudaSuccess) return fail_cuda(e, "interpolation plan");
+        const long P = (long)m.plan.WM * m.plan.HM;
+        maxP = std::max(maxP, P);
+        maxN = std::max(maxN, m.plan.N);
+        maxWM = std::max(maxWM, m.plan.WM);
+        for (int r : m.ri) {
+            FhtGeometry g = fht_geometry(m.M, radii[r], 1);
+            if (!fht_fused_supported(g))
+                return fail(ESRRF_ERR_INVALID, "radius " + std::to_string(radii[r]) + " at magnification " +
+                                                   std::to_string(m.M) + " needs a tap box wider than 32 pixels");
+            maxS = std::max(maxS, g.S);
+            FhtFusedTables t;
+            if (!drift && (e = fht_fused_tables(g, m.plan.WM, m.plan.HM, t, stream)) != cudaSuccess)
+                return fail_cuda(e, "RGC tables");
+            m.geo.push_back(std::move(g));
+            m.tables.push_back(t);
+            offsets.push_back(total);
+            total += (size_t)sens.size() * bstart.size() * 4 * P;
+        }
+        if (drift) {  // the shifts x M (loadDriftXYGPUbuffer, LiveSRRF_CL.java:586-589)
+            std::vector<float> sh(2 * (size_t)T);
+            for (int t = 0; t < T; ++t) {
+                sh[t] = m.M * dx[t];
+                sh[T + t] = m.M * dy[t];
+            }
+            if ((e = cudaMalloc(&m.d_shift, sizeof(float) * 2 * T)) != cudaSuccess ||
+                (e = cudaMemcpy(m.d_shift, sh.data(), sizeof(float) * 2 * T, cudaMemcpyHostToDevice)) != cudaSuccess)
+                return fail_cuda(e, "drift");
+        }
+    }
+    scratch.capacity = std::min(16, T);
+    const int Fi = scratch.capacity;
+    size_t maxHM = 0, maxRowT = 0, maxXs = 0;
+    for (auto& m : mp) {
+        maxHM = std::max(maxHM, (size_t)m.plan.HM);
+        maxRowT = std::max(maxRowT, interp_rowT_floats(m.plan));
+        maxXs = std::max(maxXs, interp_xs_floats(m.plan));
+    }
+    if (maxXs && (e = cudaMalloc(&scratch.xs, sizeof(float) * Fi * maxXs)) != cudaSuccess)
+        return fail_cuda(e, "sweep buffers");
+    if ((e = cudaMalloc(&scratch.rowT, sizeof(float) * Fi * maxRowT)) != cudaSuccess ||
+        (e = cudaMalloc(&scratch.alt, sizeof(float) * Fi * interp_alt_floats(maxN))) != cudaSuccess ||
+        (e = cudaMalloc(&scratch.vec, sizeof(float) * Fi * interp_vec_floats((int)maxHM, maxWM))) != cudaSuccess ||
+        (e = cudaMalloc(&d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||
+        (e = cudaMalloc(&d_cg, sizeof(float) * (size_t)T * maxP)) != cudaSuccess)
+        return fail_cuda(e, "sweep buffers");
+    if (drift && (e = fht_drift_tables_alloc(maxS, T, maxP, dtab)) != cudaSuccess) return fail_cuda(e, "drift tables");
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return fail_cuda(e, "sync");
+    return ESRRF_OK;
+}
 
-esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out) {
-    if (!sp || !out) return ESRRF_ERR_INVALID;
-    *out = nullptr;
-    auto reject = [](const std::string& m) {
-        std::lock_guard<std::mutex> lk(g_sweep_mu);
-        g_sweep_create_error = m;
-        return ESRRF_ERR_INVALID;
+// Reads every plan's tensor-core failure flag after the stream has drained.
+esrrf_status Shard::tc_check() {
+    Shard* s = this;
+    if (bic) return ESRRF_OK;
+    for (auto& m : mp) {
+        bool failed = false;
+        SK(interp_tc_check(m.plan, stream, &failed), "interpolation status");
+        if (failed) return fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
+    }
+    return ESRRF_OK;
+}
+
+esrrf_status Shard::run_device(const void* d_frames, int is_u16, float* d_out) {
+    Shard* s = this;
+    if (cudaSetDevice(device) != cudaSuccess) return fail(ESRRF_ERR_CUDA, "cudaSetDevice failed");
+    // The graph bakes in the input and output pointers: (re)capture when they change.
+    if (!exec || g_in != d_frames || g_out != d_out || g_u16 != is_u16) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        // one uncaptured pass sets the kernels' shared-memory attributes and checks the launches
+        esrrf_status r = enqueue(d_frames, is_u16, d_out);
+        if (r != ESRRF_OK) return r;
+        SK(cudaStreamSynchronize(stream), "sweep warm-up");
+        SK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        r = enqueue(d_frames, is_u16, d_out);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(stream, &g);
+        if (r != ESRRF_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        SK(ce, "end capture");
+        graph = g;
+        SK(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+        g_in = d_frames;
+        g_out = d_out;
+        g_u16 = is_u16;
+        SK(cudaStreamSynchronize(stream), "sweep");
+        return tc_check();
+    }
+    SK(cudaGraphLaunch(exec, stream), "graph launch");
+    SK(cudaStreamSynchronize(stream), "sweep");
+    return tc_check();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Partition of a sweep across devices.
+// ---------------------------------------------------------------------------------------------
+
+// Relative cost of one output pixel-frame of a (magnification, radius) pair: the taps of its disc
+// plus a fixed share for the interpolation, the gradient and the cumulants.
+double pair_cost_per_px(int M, float radius, int interp) {
+    if (interp == ESRRF_INTERP_BIC) {
+        const BicGeometry g = bic_geometry(radius, 1);
+        const double r2 = 2.0 * g.tSO;  // taps on the 2x gradient grid
+        return 3.14159265358979 * r2 * r2 + 30.0;
+    }
+    const FhtGeometry g = fht_geometry(M, radius, 1);
+    long taps = 0;
+    for (int ii = 0; ii < g.S; ++ii)
+        if (g.jlo[ii] <= g.jhi[ii]) taps += g.jhi[ii] - g.jlo[ii] + 1;
+    return (double)taps + 30.0;
+}
+
+struct ShardPlan {
+    int device = 0;
+    std::vector<int> pairs;   // mi * n_radius + ri
+    std::vector<int> blocks;  // global block indices
+    double cost = 0;
+};
+
+// Mode A: the pairs in longest-processing-time order onto the least-loaded device, every device
+// taking every block.  Mode B: every pair on every device, the blocks (by start) cut into contiguous
+// runs whose frame spans are balanced (binary search on the largest span).  The mode with the
+// smaller largest per-device cost wins; devices without work get no shard.
+std::vector<ShardPlan> plan_shards(const esrrf_sweep_params& p, const std::vector<int>& devices) {
+    const int nD = (int)devices.size(), nR = p.n_radius, nP = p.n_mag * p.n_radius, nB = p.n_blocks;
+    std::vector<double> pc(nP);
+    double pc_sum = 0;
+    for (int mi = 0; mi < p.n_mag; ++mi)
+        for (int ri = 0; ri < nR; ++ri) {
+            const int M = p.magnifications[mi];
+            pc[mi * nR + ri] = pair_cost_per_px(M, p.radii[ri], p.interp) * (double)p.width * M * p.height * M;
+            pc_sum += pc[mi * nR + ri];
+        }
+    int lo = p.n_frames, hi = 0;
+    for (int b = 0; b < nB; ++b) {
+        lo = std::min(lo, p.block_start[b]);
+        hi = std::max(hi, p.block_start[b] + p.block_length[b]);
+    }
+    const double span_all = hi - lo;
+    std::vector<int> all_blocks(nB), all_pairs(nP);
+    for (int b = 0; b < nB; ++b) all_blocks[b] = b;
+    for (int q = 0; q < nP; ++q) all_pairs[q] = q;
+    if (nD <= 1) {
+        ShardPlan s;
+        s.device = nD ? devices[0] : 0;
+        s.pairs = all_pairs;
+        s.blocks = all_blocks;
+        s.cost = pc_sum * span_all;
+        return {s};
+    }
+    // mode A
+    std::vector<ShardPlan> a(nD);
+    for (int d = 0; d < nD; ++d) a[d].device = devices[d];
+    std::vector<int> order(nP);
+    for (int q = 0; q < nP; ++q) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pc[x] > pc[y]; });
+    for (int q : order) {
+        int best = 0;
+        for (int d = 1; d < nD; ++d)
+            if (a[d].cost < a[best].cost) best = d;
+        a[best].pairs.push_back(q);
+        a[best].cost += pc[q] * span_all;
+    }
+    double make_a = 0;
+    for (auto& s : a) {
+        std::sort(s.pairs.begin(), s.pairs.end());
+        s.blocks = all_blocks;
+        make_a = std::max(make_a, s.cost);
+    }
+    // mode B
+    std::vector<int> bo(nB);
+    for (int b = 0; b < nB; ++b) bo[b] = b;
+    std::stable_sort(bo.begin(), bo.end(), [&](int x, int y) { return p.block_start[x] < p.block_start[y]; });
+    auto cut = [&](int L, std::vector<std::vector<int>>* groups) {
+        int n = 0, g0 = 0, gend = 0;
+        for (int k = 0; k < nB; ++k) {
+            const int b = bo[k], s = p.block_start[b], e = s + p.block_length[b];
+            if (k == 0 || std::max(gend, e) - g0 > L) {
+                ++n;
+                g0 = s;
+                gend = e;
+                if (groups) groups->emplace_back();
+            } else {
+                gend = std::max(gend, e);
+            }
+            if (groups) groups->back().push_back(b);
+        }
+        return n;
     };
+    int Lmin = 1, Lmax = (int)span_all;
+    for (int b = 0; b < nB; ++b) Lmin = std::max(Lmin, p.block_length[b]);
+    while (Lmin < Lmax) {
+        const int mid = Lmin + (Lmax - Lmin) / 2;
+        if (cut(mid, nullptr) <= nD) Lmax = mid;
+        else Lmin = mid + 1;
+    }
+    std::vector<std::vector<int>> groups;
+    cut(Lmin, &groups);
+    std::vector<ShardPlan> bplan;
+    double make_b = 0;
+    for (size_t g = 0; g < groups.size(); ++g) {
+        ShardPlan s;
+        s.device = devices[g];
+        s.pairs = all_pairs;
+        s.blocks = groups[g];
+        std::sort(s.blocks.begin(), s.blocks.end());
+        int glo = p.n_frames, ghi = 0;
+        for (int b : s.blocks) {
+            glo = std::min(glo, p.block_start[b]);
+            ghi = std::max(ghi, p.block_start[b] + p.block_length[b]);
+        }
+        s.cost = pc_sum * (ghi - glo);
+        make_b = std::max(make_b, s.cost);
+        bplan.push_back(std::move(s));
+    }
+    std::vector<ShardPlan> out;
+    for (auto& s : (make_b < make_a ? bplan : a))
+        if (!s.pairs.empty() && !s.blocks.empty()) out.push_back(std::move(s));
+    return out;
+}
+
+std::mutex g_sweep_mu;
+std::string g_sweep_create_error;
+
+esrrf_status reject(const std::string& m) {
+    std::lock_guard<std::mutex> lk(g_sweep_mu);
+    g_sweep_create_error = m;
+    return ESRRF_ERR_INVALID;
+}
+
+// Host-side validation shared by esrrf_sweep_create and esrrf_sweep_plan (no device work).
+esrrf_status validate(const esrrf_sweep_params* sp) {
     if (sp->width < 4 || sp->height < 4 || sp->n_frames < 1) return reject("bad stack size");
     if (sp->n_mag < 1 || !sp->magnifications || sp->n_radius < 1 || !sp->radii || sp->n_sens < 1 ||
         !sp->sensitivities || sp->n_blocks < 1 || !sp->block_start || !sp->block_length)
@@ -419,6 +700,78 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
     for (int i = 0; i < sp->n_sens; ++i)
         if (sp->sensitivities[i] < 0 || sp->sensitivities[i] > 64) return reject("sensitivity out of range");
     if (sp->interp != ESRRF_INTERP_FHT && sp->interp != ESRRF_INTERP_BIC) return reject("unknown interpolation");
+    if ((sp->drift_x == nullptr) != (sp->drift_y == nullptr))
+        return reject("drift_x and drift_y must both be given or both be NULL");
+    if (sp->drift_x && sp->interp == ESRRF_INTERP_BIC)
+        return reject("drift correction is available in the FHT sweep only (run the bicubic engine per block)");
+    if (sp->n_devices < 0 || (sp->n_devices > 0 && !sp->devices)) return reject("bad device list");
+    for (int d = 0; d < sp->n_devices; ++d)
+        for (int e = 0; e < d; ++e)
+            if (sp->devices[d] == sp->devices[e]) return reject("a device is listed twice");
+    return ESRRF_OK;
+}
+
+std::vector<int> device_list(const esrrf_sweep_params* sp) {
+    if (sp->n_devices > 0) return std::vector<int>(sp->devices, sp->devices + sp->n_devices);
+    return {sp->device >= 0 ? sp->device : 0};
+}
+
+}  // namespace
+
+struct esrrf_sweep {
+    esrrf_sweep_params p{};
+    std::vector<int> mags, sens, bstart, blen, devices;
+    std::vector<float> radii, dx, dy;
+    std::vector<Shard*> shards;
+    std::vector<size_t> offsets;  // global layout per (magnification, radius)
+    size_t total = 0;
+    std::string err;
+
+    // the single shard holds every pair and block in order: its layout is the global one
+    bool direct() const { return shards.size() == 1 && shards[0]->total == total && shards[0]->f0 == 0; }
+    esrrf_status fail(esrrf_status s, const std::string& m) {
+        err = m;
+        return s;
+    }
+    void release() {
+        for (Shard* s : shards) {
+            s->release();
+            delete s;
+        }
+        shards.clear();
+    }
+};
+
+extern "C" {
+
+esrrf_status esrrf_sweep_plan(const esrrf_sweep_params* sp, int* pair_device, int* block_device,
+                              double* device_cost) {
+    if (!sp) return ESRRF_ERR_INVALID;
+    esrrf_status r = validate(sp);
+    if (r != ESRRF_OK) return r;
+    const std::vector<int> devs = device_list(sp);
+    const std::vector<ShardPlan> plan = plan_shards(*sp, devs);
+    const int nP = sp->n_mag * sp->n_radius;
+    for (int q = 0; q < nP && pair_device; ++q) pair_device[q] = -2;  // not assigned
+    for (int b = 0; b < sp->n_blocks && block_device; ++b) block_device[b] = -2;
+    for (size_t d = 0; d < devs.size() && device_cost; ++d) device_cost[d] = 0;
+    for (const ShardPlan& s : plan) {
+        const int di = (int)(std::find(devs.begin(), devs.end(), s.device) - devs.begin());
+        const bool all_pairs = (int)s.pairs.size() == nP, all_blocks = (int)s.blocks.size() == sp->n_blocks;
+        if (pair_device)
+            for (int q : s.pairs) pair_device[q] = all_pairs && plan.size() > 1 ? -1 : s.device;
+        if (block_device)
+            for (int b : s.blocks) block_device[b] = all_blocks && plan.size() > 1 ? -1 : s.device;
+        if (device_cost) device_cost[di] = s.cost;
+    }
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out) {
+    if (!sp || !out) return ESRRF_ERR_INVALID;
+    *out = nullptr;
+    esrrf_status vr = validate(sp);
+    if (vr != ESRRF_OK) return vr;
 
     esrrf_sweep* s = new esrrf_sweep();
     s->p = *sp;
@@ -427,14 +780,23 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
     s->sens.assign(sp->sensitivities, sp->sensitivities + sp->n_sens);
     s->bstart.assign(sp->block_start, sp->block_start + sp->n_blocks);
     s->blen.assign(sp->block_length, sp->block_length + sp->n_blocks);
+    s->devices = device_list(sp);
+    bool any_drift = false;
+    if (sp->drift_x) {
+        s->dx.assign(sp->drift_x, sp->drift_x + sp->n_frames);
+        s->dy.assign(sp->drift_y, sp->drift_y + sp->n_frames);
+        for (int t = 0; t < sp->n_frames; ++t) any_drift |= s->dx[t] != 0.f || s->dy[t] != 0.f;
+    }
     s->p.magnifications = nullptr;
     s->p.radii = nullptr;
     s->p.sensitivities = nullptr;
     s->p.block_start = s->p.block_length = nullptr;
-    auto bail = [&](esrrf_status st) {
+    s->p.drift_x = s->p.drift_y = nullptr;
+    s->p.devices = nullptr;
+    auto bail = [&](esrrf_status st, const std::string& m) {
         {
             std::lock_guard<std::mutex> lk(g_sweep_mu);
-            g_sweep_create_error = s->err;
+            g_sweep_create_error = m;
         }
         s->release();
         delete s;
@@ -443,68 +805,67 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* sp, esrrf_sweep** out)
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
-        s->err = "no CUDA device";
-        return bail(ESRRF_ERR_NODEVICE);
+        return bail(ESRRF_ERR_NODEVICE, "no CUDA device");
     }
-    s->device = sp->device >= 0 ? sp->device : 0;
-    cudaError_t e;
-    if ((e = cudaSetDevice(s->device)) != cudaSuccess) return bail(s->fail_cuda(e, "cudaSetDevice"));
-    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess)
-        return bail(s->fail_cuda(e, "stream"));
-    if (sp->interp == ESRRF_INTERP_BIC) {
-        s->bic = true;
-        esrrf_status r = sweep_create_bic(s);
-        if (r != ESRRF_OK) return bail(r);
-        *out = s;
-        return ESRRF_OK;
-    }
-    long maxP = 0;
-    int maxN = 0, maxWM = 0;
+    for (int d : s->devices)
+        if (d < 0 || d >= ndev) return bail(ESRRF_ERR_INVALID, "device " + std::to_string(d) + " does not exist");
+    // global output layout
+    const int nR = (int)s->radii.size();
     s->total = 0;
-    for (int M : s->mags) {
-        s->mp.emplace_back();
-        MagPlan& m = s->mp.back();
-        m.M = M;
-        if ((e = interp_plan_create(m.plan, sp->width, sp->height, M, 0)) != cudaSuccess)
-            return bail(s->fail_cuda(e, "interpolation plan"));
-        const long P = (long)m.plan.WM * m.plan.HM;
-        maxP = std::max(maxP, P);
-        maxN = std::max(maxN, m.plan.N);
-        maxWM = std::max(maxWM, m.plan.WM);
-        for (float r : s->radii) {
-            FhtGeometry g = fht_geometry(M, r, 1);
-            if (!fht_fused_supported(g)) {
-                s->err = "radius " + std::to_string(r) + " at magnification " + std::to_string(M) +
-                         " needs a tap box wider than 32 pixels";
-                return bail(ESRRF_ERR_INVALID);
-            }
-            FhtFusedTables t;
-            if ((e = fht_fused_tables(g, m.plan.WM, m.plan.HM, t, s->stream)) != cudaSuccess)
-                return bail(s->fail_cuda(e, "RGC tables"));
-            m.geo.push_back(std::move(g));
-            m.tables.push_back(t);
+    for (int mi = 0; mi < sp->n_mag; ++mi)
+        for (int ri = 0; ri < nR; ++ri) {
             s->offsets.push_back(s->total);
-            s->total += (size_t)s->sens.size() * s->bstart.size() * 4 * P;
+            s->total += s->sens.size() * s->bstart.size() * 4 * (size_t)sp->width * s->mags[mi] * sp->height * s->mags[mi];
         }
+    // one shard per device of the plan, created in parallel
+    const std::vector<ShardPlan> plan = plan_shards(*sp, s->devices);
+    for (const ShardPlan& sp_ : plan) {
+        Shard* sh = new Shard();
+        sh->device = sp_.device;
+        sh->w = sp->width;
+        sh->h = sp->height;
+        sh->int_weighting = sp->int_weighting;
+        sh->sens = s->sens;
+        int lo = sp->n_frames, hi = 0;
+        for (int b : sp_.blocks) {
+            lo = std::min(lo, s->bstart[b]);
+            hi = std::max(hi, s->bstart[b] + s->blen[b]);
+        }
+        // a single-device sweep keeps the whole stack (its layout and frame indices are the caller's)
+        if (plan.size() == 1) {
+            lo = 0;
+            hi = sp->n_frames;
+        }
+        sh->f0 = lo;
+        sh->T = hi - lo;
+        for (int b : sp_.blocks) {
+            sh->bstart.push_back(s->bstart[b] - lo);
+            sh->blen.push_back(s->blen[b]);
+            sh->bglob.push_back(b);
+        }
+        for (int q : sp_.pairs) {
+            const int mi = q / nR, ri = q % nR;
+            if (sh->mp.empty() || sh->mp.back().mi != mi) {
+                sh->mp.emplace_back();
+                sh->mp.back().mi = mi;
+                sh->mp.back().M = s->mags[mi];
+            }
+            sh->mp.back().ri.push_back(ri);
+        }
+        if (any_drift) {
+            sh->drift = true;
+            sh->dx.assign(s->dx.begin() + lo, s->dx.begin() + hi);
+            sh->dy.assign(s->dy.begin() + lo, s->dy.begin() + hi);
+        }
+        s->shards.push_back(sh);
     }
-    const int T = sp->n_frames;
-    s->scratch.capacity = std::min(16, T);
-    const int Fi = s->scratch.capacity;
-    size_t maxHM = 0, maxRowT = 0, maxXs = 0;
-    for (auto& m : s->mp) {
-        maxHM = std::max(maxHM, (size_t)m.plan.HM);
-        maxRowT = std::max(maxRowT, interp_rowT_floats(m.plan));
-        maxXs = std::max(maxXs, interp_xs_floats(m.plan));
-    }
-    if (maxXs && (e = cudaMalloc(&s->scratch.xs, sizeof(float) * Fi * maxXs)) != cudaSuccess)
-        return bail(s->fail_cuda(e, "sweep buffers"));
-    if ((e = cudaMalloc(&s->scratch.rowT, sizeof(float) * Fi * maxRowT)) != cudaSuccess ||
-        (e = cudaMalloc(&s->scratch.alt, sizeof(float) * Fi * interp_alt_floats(maxN))) != cudaSuccess ||
-        (e = cudaMalloc(&s->scratch.vec, sizeof(float) * Fi * interp_vec_floats((int)maxHM, maxWM))) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_interp, sizeof(float) * (size_t)T * maxP)) != cudaSuccess ||
-        (e = cudaMalloc(&s->d_cg, sizeof(float) * (size_t)T * maxP)) != cudaSuccess)
-        return bail(s->fail_cuda(e, "sweep buffers"));
-    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return bail(s->fail_cuda(e, "sync"));
+    std::vector<esrrf_status> rs(s->shards.size(), ESRRF_OK);
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < s->shards.size(); ++i)
+        th.emplace_back([&, i] { rs[i] = s->shards[i]->create(s->radii, sp->interp); });
+    for (auto& t : th) t.join();
+    for (size_t i = 0; i < s->shards.size(); ++i)
+        if (rs[i] != ESRRF_OK) return bail(rs[i], s->shards[i]->err);
     *out = s;
     return ESRRF_OK;
 }
@@ -517,76 +878,79 @@ esrrf_status esrrf_sweep_output_layout(const esrrf_sweep* s, size_t* total_float
     return ESRRF_OK;
 }
 
-// Reads every plan's tensor-core failure flag after the stream has drained.
-static esrrf_status sweep_tc_check(esrrf_sweep* s) {
-    if (s->bic) return ESRRF_OK;
-    for (auto& m : s->mp) {
-        bool failed = false;
-        SK(interp_tc_check(m.plan, s->stream, &failed), "interpolation status");
-        if (failed) return s->fail(ESRRF_ERR_TIMEOUT, "interpolation tensor-core pass: a bounded wait gave up");
-    }
-    return ESRRF_OK;
-}
-
-static esrrf_status sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out) {
-    if (cudaSetDevice(s->device) != cudaSuccess) return s->fail(ESRRF_ERR_CUDA, "cudaSetDevice failed");
-    // The graph bakes in the input and output pointers: (re)capture when they change.
-    if (!s->exec || s->g_in != d_frames || s->g_out != d_out || s->g_u16 != is_u16) {
-        if (s->exec) cudaGraphExecDestroy(s->exec);
-        if (s->graph) cudaGraphDestroy(s->graph);
-        s->exec = nullptr;
-        s->graph = nullptr;
-        // one uncaptured pass sets the kernels' shared-memory attributes and checks the launches
-        esrrf_status r = s->enqueue(d_frames, is_u16, d_out);
-        if (r != ESRRF_OK) return r;
-        SK(cudaStreamSynchronize(s->stream), "sweep warm-up");
-        SK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        r = s->enqueue(d_frames, is_u16, d_out);
-        cudaGraph_t g = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
-        if (r != ESRRF_OK) {
-            if (g) cudaGraphDestroy(g);
-            return r;
-        }
-        SK(ce, "end capture");
-        s->graph = g;
-        SK(cudaGraphInstantiate(&s->exec, s->graph, 0), "graph instantiate");
-        s->g_in = d_frames;
-        s->g_out = d_out;
-        s->g_u16 = is_u16;
-        SK(cudaStreamSynchronize(s->stream), "sweep");
-        return sweep_tc_check(s);
-    }
-    SK(cudaGraphLaunch(s->exec, s->stream), "graph launch");
-    SK(cudaStreamSynchronize(s->stream), "sweep");
-    return sweep_tc_check(s);
-}
-
 esrrf_status esrrf_sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out) {
     if (!s || !d_frames || !d_out) return ESRRF_ERR_INVALID;
-    return sweep_run_device(s, d_frames, is_u16, d_out);
+    if (!s->direct())
+        return s->fail(ESRRF_ERR_INVALID, "a sweep split across devices takes host frames (esrrf_sweep_run)");
+    esrrf_status r = s->shards[0]->run_device(d_frames, is_u16, d_out);
+    if (r != ESRRF_OK) s->err = s->shards[0]->err;
+    return r;
 }
 
 esrrf_status esrrf_sweep_run(esrrf_sweep* s, const void* frames, int is_u16, float* out) {
     if (!s || !frames || !out) return ESRRF_ERR_INVALID;
-    if (cudaSetDevice(s->device) != cudaSuccess) return s->fail(ESRRF_ERR_CUDA, "cudaSetDevice failed");
-    const size_t in_bytes = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)s->p.width *
-                            s->p.height * s->p.n_frames;
-    if (!s->d_in) SK(cudaMalloc(&s->d_in, sizeof(float) * (size_t)s->p.width * s->p.height * s->p.n_frames),
-                     "input buffer");
-    if (!s->d_outbuf) SK(cudaMalloc(&s->d_outbuf, sizeof(float) * s->total), "output buffer");
-    SK(cudaMemcpyAsync(s->d_in, frames, in_bytes, cudaMemcpyHostToDevice, s->stream), "input copy");
-    esrrf_status r = sweep_run_device(s, s->d_in, is_u16, s->d_outbuf);
-    if (r != ESRRF_OK) return r;
-    SK(cudaMemcpyAsync(out, s->d_outbuf, sizeof(float) * s->total, cudaMemcpyDeviceToHost, s->stream),
-       "output copy");
-    SK(cudaStreamSynchronize(s->stream), "sweep");
+    const size_t fbytes = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)s->p.width * s->p.height;
+    const bool direct = s->direct();
+    std::vector<esrrf_status> rs(s->shards.size(), ESRRF_OK);
+    auto work = [&](size_t i) -> esrrf_status {
+        Shard* sh = s->shards[i];
+        if (cudaSetDevice(sh->device) != cudaSuccess) return sh->fail(ESRRF_ERR_CUDA, "cudaSetDevice failed");
+        if (!sh->d_in) SKS(cudaMalloc(&sh->d_in, sizeof(float) * (size_t)s->p.width * s->p.height * sh->T), "input buffer");
+        if (!sh->d_outbuf) SKS(cudaMalloc(&sh->d_outbuf, sizeof(float) * sh->total), "output buffer");
+        SKS(cudaMemcpyAsync(sh->d_in, (const unsigned char*)frames + fbytes * sh->f0, fbytes * sh->T,
+                            cudaMemcpyHostToDevice, sh->stream), "input copy");
+        esrrf_status r = sh->run_device(sh->d_in, is_u16, sh->d_outbuf);
+        if (r != ESRRF_OK) return r;
+        if (direct) {
+            SKS(cudaMemcpyAsync(out, sh->d_outbuf, sizeof(float) * s->total, cudaMemcpyDeviceToHost, sh->stream),
+                "output copy");
+        } else {  // gather: each (pair, sensitivity, local block) to its place in the global layout
+            const int nR = (int)s->radii.size(), nB = (int)s->bstart.size();
+            const int nS = (int)s->sens.size(), nBl = (int)sh->bstart.size();
+            size_t oi = 0;
+            for (const MagPlan& m : sh->mp) {
+                const size_t P = (size_t)s->p.width * m.M * s->p.height * m.M;
+                for (int ri : m.ri) {
+                    const float* src = sh->d_outbuf + sh->offsets[oi++];
+                    float* dst = out + s->offsets[m.mi * nR + ri];
+                    for (int si = 0; si < nS; ++si)
+                        for (int bl = 0; bl < nBl; ++bl)
+                            SKS(cudaMemcpyAsync(dst + ((size_t)si * nB + sh->bglob[bl]) * 4 * P,
+                                                src + ((size_t)si * nBl + bl) * 4 * P, sizeof(float) * 4 * P,
+                                                cudaMemcpyDeviceToHost, sh->stream),
+                                "output copy");
+                }
+            }
+        }
+        SKS(cudaStreamSynchronize(sh->stream), "sweep");
+        return ESRRF_OK;
+    };
+    if (s->shards.size() == 1) {
+        rs[0] = work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t i = 0; i < s->shards.size(); ++i) th.emplace_back([&, i] { rs[i] = work(i); });
+        for (auto& t : th) t.join();
+    }
+    for (size_t i = 0; i < s->shards.size(); ++i)
+        if (rs[i] != ESRRF_OK) {
+            s->err = "device " + std::to_string(s->shards[i]->device) + ": " + s->shards[i]->err;
+            return rs[i];
+        }
     return ESRRF_OK;
 }
 
 esrrf_status esrrf_sweep_launch_count(const esrrf_sweep* s, int* launches) {
     if (!s || !launches) return ESRRF_ERR_INVALID;
-    *launches = s->launches_per_run;
+    int n = 0;
+    for (const Shard* sh : s->shards) n += sh->launches_per_run;
+    *launches = n;
+    return ESRRF_OK;
+}
+
+esrrf_status esrrf_sweep_shard_count(const esrrf_sweep* s, int* shards) {
+    if (!s || !shards) return ESRRF_ERR_INVALID;
+    *shards = (int)s->shards.size();
     return ESRRF_OK;
 }
 

@@ -281,14 +281,31 @@ def esrrf_stack(stack, magnification, fwhm, sensitivity, frames_per_block=None, 
 
 class Sweep:
     """Batched parameter sweep / rolling analysis (esrrf_sweep_*): every (magnification, radius,
-    sensitivity, block) reconstruction of a stack in one captured CUDA graph.  Replaces the
-    per-combination engine loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519) and
+    sensitivity, block) reconstruction of a stack in one captured CUDA graph per device.  Replaces
+    the per-combination engine loop of ParametersSweep_.run (gui/ParametersSweep_.java:328-519) and
     the block loop of LiveSRRF_optimised_.run (gui/LiveSRRF_optimised_.java:276-389).
     ``interpolation``: "fht" or "bicubic" (the sweep's "Use FHT interpolation" option; the
-    bicubic sweep applies the MP correction, as the reference's sweep does)."""
+    bicubic sweep applies the MP correction, as the reference's sweep does).
+    ``drift``: (shift_x, shift_y), one shift per frame of the stack in raw pixels (the sweep's
+    vibration correction, gui/ParametersSweep_.java:282-290), FHT sweep only.
+    ``devices``: a list of CUDA ordinals to split the sweep across (``plan`` shows the split)."""
 
     def __init__(self, width, height, n_frames, magnifications, radii, sensitivities, blocks,
-                 int_weighting=True, device=-1, interpolation="fht"):
+                 int_weighting=True, device=-1, interpolation="fht", drift=None, devices=None):
+        self._h = None
+        self._p = self._params(width, height, n_frames, magnifications, radii, sensitivities, blocks,
+                               int_weighting, device, interpolation, drift, devices)
+        h = ctypes.c_void_p()
+        _lib.check(None, lib().esrrf_sweep_create(ctypes.byref(self._p), ctypes.byref(h)), sweep=True)
+        self._h = h
+        total = ctypes.c_size_t()
+        offs = (ctypes.c_size_t * (len(self.mags) * len(self.radii)))()
+        _lib.check(h, lib().esrrf_sweep_output_layout(h, ctypes.byref(total), offs), sweep=True)
+        self.total = total.value
+        self.offsets = list(offs)
+
+    def _params(self, width, height, n_frames, magnifications, radii, sensitivities, blocks,
+                int_weighting, device, interpolation, drift, devices):
         from ._lib import EsrrfSweepParams
 
         self.width, self.height, self.n_frames = int(width), int(height), int(n_frames)
@@ -300,20 +317,45 @@ class Sweep:
         self.blen = np.ascontiguousarray(blocks[:, 1], np.int32)
         ip = ctypes.POINTER(ctypes.c_int)
         fp = ctypes.POINTER(ctypes.c_float)
-        p = EsrrfSweepParams(self.width, self.height, self.n_frames, len(self.mags),
-                             self.mags.ctypes.data_as(ip), len(self.radii), self.radii.ctypes.data_as(fp),
-                             len(self.sens), self.sens.ctypes.data_as(ip), len(self.bstart),
-                             self.bstart.ctypes.data_as(ip), self.blen.ctypes.data_as(ip),
-                             int(bool(int_weighting)), int(device),
-                             {"fht": 0, "bicubic": 1}[interpolation])
-        h = ctypes.c_void_p()
-        _lib.check(None, lib().esrrf_sweep_create(ctypes.byref(p), ctypes.byref(h)), sweep=True)
-        self._h = h
-        total = ctypes.c_size_t()
-        offs = (ctypes.c_size_t * (len(self.mags) * len(self.radii)))()
-        _lib.check(h, lib().esrrf_sweep_output_layout(h, ctypes.byref(total), offs), sweep=True)
-        self.total = total.value
-        self.offsets = list(offs)
+        self._drift = None
+        if drift is not None:
+            dx = np.ascontiguousarray(drift[0], np.float32).reshape(-1)
+            dy = np.ascontiguousarray(drift[1], np.float32).reshape(-1)
+            if dx.size != self.n_frames or dy.size != self.n_frames:
+                raise EsrrfError("drift arrays must hold one shift per frame of the stack")
+            self._drift = (dx, dy)
+        self._devices = None if devices is None else np.ascontiguousarray(devices, np.int32)
+        return EsrrfSweepParams(self.width, self.height, self.n_frames, len(self.mags),
+                                self.mags.ctypes.data_as(ip), len(self.radii), self.radii.ctypes.data_as(fp),
+                                len(self.sens), self.sens.ctypes.data_as(ip), len(self.bstart),
+                                self.bstart.ctypes.data_as(ip), self.blen.ctypes.data_as(ip),
+                                int(bool(int_weighting)), int(device),
+                                {"fht": 0, "bicubic": 1}[interpolation],
+                                self._drift[0].ctypes.data_as(fp) if self._drift else None,
+                                self._drift[1].ctypes.data_as(fp) if self._drift else None,
+                                0 if self._devices is None else len(self._devices),
+                                self._devices.ctypes.data_as(ip) if self._devices is not None else None)
+
+    @staticmethod
+    def plan(width, height, n_frames, magnifications, radii, sensitivities, blocks, devices,
+             interpolation="fht"):
+        """The split esrrf_sweep_create would make across ``devices`` (host arithmetic only):
+        (pair_device [n_mag * n_radius], block_device [n_blocks], device_cost [n_devices]);
+        -1 = every device of the split, -2 = none."""
+        self = Sweep.__new__(Sweep)
+        p = self._params(width, height, n_frames, magnifications, radii, sensitivities, blocks, True, -1,
+                         interpolation, None, devices)
+        nP, nB = len(self.mags) * len(self.radii), len(self.bstart)
+        pd = (ctypes.c_int * nP)()
+        bd = (ctypes.c_int * nB)()
+        dc = (ctypes.c_double * max(1, len(devices)))()
+        _lib.check(None, lib().esrrf_sweep_plan(ctypes.byref(p), pd, bd, dc), sweep=True)
+        return list(pd), list(bd), list(dc)[:len(devices)]
+
+    def shard_count(self) -> int:
+        n = ctypes.c_int()
+        _lib.check(self._h, lib().esrrf_sweep_shard_count(self._h, ctypes.byref(n)), sweep=True)
+        return n.value
 
     @property
     def handle(self):
@@ -381,13 +423,52 @@ class Sweep:
 
 
 def rolling(stack, magnification, fwhm, sensitivity, blocks, int_weighting=True,
-            interpolation="fht"):
+            interpolation="fht", drift=None, devices=None):
     """Rolling analysis over arbitrary (start, length) blocks, each frame interpolated (or its
     gradients resampled, ``interpolation="bicubic"``) and run through the RGC once:
-    {(start, length): [4][HM][WM]}."""
+    {(start, length): [4][HM][WM]}.
+
+    ``drift``: one (shift_x, shift_y) pair of arrays per block, each of the block's length in raw
+    pixels -- the per-block arrays the analysis plugin computes relative to each block's first frame
+    (gui/LiveSRRF_optimised_.java:283-305).  Blocks that do not overlap run as one sweep with the
+    arrays laid end to end; overlapping blocks (a frame with two different shifts) run through the
+    engine block by block, as the plugin does.  ``devices``: CUDA ordinals to split the blocks
+    across (drift-free or non-overlapping blocks)."""
     a = np.asarray(stack)
+    blocks = [(int(st), int(ln)) for st, ln in blocks]
+    sweep_drift = None
+    if drift is not None:
+        if len(drift) != len(blocks):
+            raise EsrrfError("drift needs one (shift_x, shift_y) pair per block")
+        order = sorted(range(len(blocks)), key=lambda i: blocks[i][0])
+        overlap = any(blocks[order[k]][0] + blocks[order[k]][1] > blocks[order[k + 1]][0]
+                      for k in range(len(order) - 1))
+        if overlap:
+            out = {}
+            for (st, ln), (dx, dy) in zip(blocks, drift):
+                eng = LiveSRRF_CL()
+                eng.initialise(a.shape[-1], a.shape[-2], magnification, fwhm, sensitivity, ln, ln,
+                               intWeighting=int_weighting, doFHTinterpolation=interpolation == "fht")
+                try:
+                    eng.resetFramePosition()
+                    eng.loadDriftXYGPUbuffer(dx, dy)
+                    eng.calculateSRRF(a[st:st + ln])
+                    out[(st, ln)] = eng.readSRRFbuffer().copy()
+                finally:
+                    eng.release()
+            return out
+        fx = np.zeros(a.shape[0], np.float32)
+        fy = np.zeros(a.shape[0], np.float32)
+        for (st, ln), (dx, dy) in zip(blocks, drift):
+            dx = np.asarray(dx, np.float32).reshape(-1)
+            dy = np.asarray(dy, np.float32).reshape(-1)
+            if dx.size != ln or dy.size != ln:
+                raise EsrrfError("a block's drift arrays must hold one shift per frame of the block")
+            fx[st:st + ln] = dx
+            fy[st:st + ln] = dy
+        sweep_drift = (fx, fy)
     sw = Sweep(a.shape[-1], a.shape[-2], a.shape[0], [magnification], [fwhm], [sensitivity],
-               blocks, int_weighting, interpolation=interpolation)
+               blocks, int_weighting, interpolation=interpolation, drift=sweep_drift, devices=devices)
     try:
         res = sw.run(a)
         return {k[3]: v.copy() for k, v in res.items()}

@@ -93,6 +93,8 @@ class EsrrfSweepParams(ctypes.Structure):
         ("n_blocks", ctypes.c_int), ("block_start", ctypes.POINTER(ctypes.c_int)),
         ("block_length", ctypes.POINTER(ctypes.c_int)),
         ("int_weighting", ctypes.c_int), ("device", ctypes.c_int), ("interp", ctypes.c_int),
+        ("drift_x", _f32p), ("drift_y", _f32p),
+        ("n_devices", ctypes.c_int), ("devices", ctypes.POINTER(ctypes.c_int)),
     ]
 
 
@@ -135,6 +137,9 @@ SIGNATURES.update({
     "esrrf_sweep_run_device": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_int, _c.c_void_p]),
     "esrrf_sweep_run": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_int, _c.c_void_p]),
     "esrrf_sweep_launch_count": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
+    "esrrf_sweep_shard_count": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
+    "esrrf_sweep_plan": (_c.c_int, [_c.POINTER(EsrrfSweepParams), _c.POINTER(_c.c_int),
+                                    _c.POINTER(_c.c_int), _c.POINTER(_c.c_double)]),
     "esrrf_sweep_last_error": (_c.c_char_p, [_c.c_void_p]),
     "esrrf_sweep_destroy": (_c.c_int, [_c.c_void_p]),
     "esrrf_adjoint_create": (_c.c_int, [_c.c_int, _c.c_int, _c.c_int, _c.c_int, _c.c_int,

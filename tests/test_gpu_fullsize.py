@@ -1,0 +1,92 @@
+"""GPU parity at the benchmarked configurations, against the reference's own kernels.
+
+The checker is ``oracle/_ref`` (liveSRRF_noInterpolation.cl compiled for the host and replayed in
+LiveSRRF_CL.java's launch order) where it was built, else the C restatement that is bit-identical
+to it on every golden fixture.  The interpolated frames the checker reads come from the float64
+FFT form of FourierInterpolation.java's map.
+
+* 512 x 512 uint16 frames at M4, radius 1.5, sensitivity 2 (the headline workload's frame size
+  and parameters): a 4-frame block cut into launches of 2 frames, so that a launch edge falls
+  inside the block and TAC2 pairs across it.
+* The parameter sweep's per-frame CGLH mode at M2 and M4 with radii 0.5 and 3.0 (at M4 radius 3.0
+  has a 26-wide tap box, the largest of the sweep workload) on a 64 x 64 crop, uneven blocks.
+* The fidelity-loss adjoint at M4 (the 256 x 256 x 100 workload's magnification, 18-wide tap box)
+  on a 48 x 48 x 8 stack: radius, sensitivity, re-blur sigma and pixel gradients against central
+  finite differences (h = 1e-3) of the float64 loss.
+
+Tolerance: each slice within 1e-4 of its dynamic range; gradients within 1e-3 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def _ref_block(O, interp, M, fwhm, S, frames_per_load=0):
+    if O.ref_available():
+        return O.ref_fht_block(interp, M, fwhm, S, frames_per_load=frames_per_load)
+    return O.fht_block(interp, M, fwhm, S)
+
+
+def test_headline_frame_size_against_reference_kernels(esrrf_mod, oracle_mod):
+    from esrrf import synth
+    raw = synth.make_stack("fht512", frames=4)
+    assert raw.dtype == np.uint16 and raw.shape == (4, 512, 512)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(512, 512, 4, 1.5, 2, 4, 4, framesPerLaunch=2)
+    try:
+        eng.resetFramePosition()
+        assert not eng.calculateSRRF(raw)
+        got = eng.readSRRFbuffer().copy()
+    finally:
+        eng.release()
+    interp = oracle_mod.fht_interpolate_fft(raw.astype(np.float32), 4)
+    ref = _ref_block(oracle_mod, interp, 4, 1.5, 2, frames_per_load=2)
+    assert np.abs(ref[2]).max() > 0
+    for k in range(4):
+        e = rel_err(got[k], ref[k])
+        assert e < TOL, f"slice {k}: {e:.3g} of range"
+
+
+def test_sweep_cglh_mode_large_and_small_radii(esrrf_mod, oracle_mod):
+    from esrrf import synth
+    raw = synth.small_stack(61, 12, 64, 64, emitters=40)
+    mags, radii, sens = [2, 4], [0.5, 3.0], [1, 4]
+    blocks = [(0, 5), (5, 7), (2, 9)]
+    sw = esrrf_mod.Sweep(64, 64, 12, mags, radii, sens, blocks)
+    try:
+        res = sw.run(raw)
+    finally:
+        sw.release()
+    assert len(res) == len(mags) * len(radii) * len(sens) * len(blocks)
+    interp = {M: oracle_mod.fht_interpolate(raw.astype(np.float32), M) for M in mags}
+    for (M, r, S, (st, ln)), got in res.items():
+        ref = _ref_block(oracle_mod, interp[M][st:st + ln], M, r, S)
+        for k in range(4):
+            e = rel_err(got[k], ref[k])
+            assert e < TOL, (M, r, S, st, ln, k, e)
+
+
+def test_adjoint_at_m4_against_finite_differences(esrrf_mod):
+    from esrrf import synth
+    from oracle import adjoint_oracle as A
+    raw = synth.small_stack(72, 8, 48, 48, emitters=20).astype(np.float32)
+    M, fwhm, S, sig = 4, 1.5, 2.0, 1.3
+    pix = [(0, 5, 5), (3, 20, 30), (7, 47, 0), (5, 24, 24)]
+    fd = A.fd_gradient(raw, M, fwhm, S, sig, pixels=pix)
+    L64 = A.loss(raw, M, fwhm, S, sig)
+    adj = esrrf_mod.Adjoint(48, 48, 8, M)
+    try:
+        L, g, gf = adj.loss_and_grad(raw, fwhm, S, sig)
+        gf = gf.cpu().numpy()
+    finally:
+        adj.release()
+    assert abs(L - L64) <= 1e-4 * abs(L64), (L, L64)
+    for k in ("fwhm", "S", "sigma"):
+        assert abs(g[k] - fd[k]) <= 1e-3 * abs(fd[k]), (k, g[k], fd[k])
+    scale = max(abs(v) for v in fd["pixels"].values())
+    for (t, y, x), v in fd["pixels"].items():
+        assert abs(gf[t, y, x] - v) <= 1e-3 * max(abs(v), 0.05 * scale), ((t, y, x), gf[t, y, x], v)
