@@ -12,8 +12,14 @@ public host API (pinned host frames in, host results out, copies inside the time
 `--impl reference` times the reference's own kernels (oracle/_ref: liveSRRF_noInterpolation.cl
 compiled for the host, all cores) with the Fourier interpolation done by numpy's FFT, on a
 bounded sample of the same workload.
-Multi-GPU (torchrun): every rank runs the full workload on its own GPU (rolling blocks are
-independent; no collective on the data path), value = all ranks' input Mpx.frames / max time.
+Multi-GPU (torchrun): the blocks of a world-size times longer stack are split across the ranks
+by the library's planner (esrrf_sweep_plan: contiguous runs, one per GPU); blocks are independent,
+so there is no collective on the data path; value = all ranks' input Mpx.frames / max time (weak
+scaling: the per-GPU work is fixed).
+`--drift` gives every frame a seeded shift (vibration correction, loadDriftXYGPUbuffer).
+The ncu-derived figures (DRAM traffic, warp instructions per frame) are read from profiles/ only
+when that summary's `source_sha:` matches the current kernel sources; otherwise they are reported
+as unavailable.
 """
 from __future__ import annotations
 
@@ -368,6 +374,59 @@ def run_reference(args, world, rank):
 
 
 TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md", "rgc_fused_bic512": "rgc_bic_bic512.md"}
+# the kernel sources each summary's counts depend on
+SUMMARY_SOURCES = {
+    "rgc_fused_fht512": ["fht_fused.cuh", "rgc_fht.cu"],
+    "rgc_fused_bic512": ["rgc_bic.cu", "device_common.cuh"],
+}
+
+
+def source_sha(kernel):
+    """sha256 (first 16 hex digits) of the sources a kernel's ncu figures depend on."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in SUMMARY_SOURCES.get(kernel, []):
+        with open(os.path.join(PKG, "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def summary_stale(kernel):
+    """None if the committed ncu summary of `kernel` was taken of the current sources (its
+    `source_sha:` line), else why its figures cannot be used."""
+    name = TRAFFIC_SUMMARIES.get(kernel)
+    if not name:
+        return "no ncu summary for this kernel"
+    recorded = None
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if line.startswith("source_sha:"):
+                    recorded = line.split(":", 1)[1].strip()
+    except OSError:
+        return f"profiles/{name} missing"
+    if recorded != source_sha(kernel):
+        return (f"profiles/{name} was captured from other kernel sources (sha {recorded}, now "
+                f"{source_sha(kernel)}): re-capture before quoting its figures")
+    return None
+
+
+def shard_blocks(world, rank, n_blocks, nf):
+    """This rank's blocks under torchrun: the library's planner (esrrf_sweep_plan) splits the
+    world * n_blocks blocks of a world-size times longer stack into contiguous runs across the
+    ranks (one pair, so blocks are the unit); each rank's run is n_blocks long."""
+    if world == 1:
+        return list(range(n_blocks))
+    import esrrf
+
+    nb = world * n_blocks
+    _, bd, _ = esrrf.Sweep.plan(64, 64, nb * nf, [4], [1.5], [2], [(b * nf, nf) for b in range(nb)],
+                                list(range(world)))
+    mine = [b for b in range(nb) if bd[b] == rank]
+    if len(mine) != n_blocks:
+        raise RuntimeError(f"planner gave rank {rank} {len(mine)} blocks, expected {n_blocks}")
+    return mine
 
 
 def read_traffic_summary(kernel, key="traffic_bytes_per_launch"):
@@ -406,6 +465,14 @@ def run_ours(args, world, rank, local):
     L = esrrf.lib()
 
     bic = args.workload == "bic512"
+    # blocks of this rank: the stack stands for this rank's run of blocks of a world-size times
+    # longer stack, split by the library's planner (contiguous runs of balanced frame span)
+    blocks_here = shard_blocks(world, rank, n_blocks, nf)
+    # vibration correction: a seeded per-frame shift for every block (raw pixels, |s| < 1.5)
+    shifts = None
+    if args.drift:
+        rng = np.random.default_rng(4321)
+        shifts = rng.uniform(-1.5, 1.5, size=(n_blocks, 2, nf)).astype(np.float32)
     eng = esrrf.LiveSRRF_CL()
     eng.initialise(w, h, M, fwhm, S, nf, nf, chosenDevice=local, kernel=args.kernel,
                    framesPerLaunch=args.frames_per_launch, doFHTinterpolation=not bic,
@@ -425,10 +492,18 @@ def run_ours(args, world, rank, local):
     rgc_ms = [0.0]
     rgc_n = [0]
 
+    fp = ctypes.POINTER(ctypes.c_float)
+
+    def set_drift(b):
+        if shifts is not None:
+            esrrf._lib.check(H, L.esrrf_set_drift(H, shifts[b, 0].ctypes.data_as(fp),
+                                                  shifts[b, 1].ctypes.data_as(fp), nf))
+
     def step_device():
         base = d_stack.data_ptr()
         for b in range(n_blocks):
             esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
+            set_drift(b)
             esrrf._lib.check(H, L.esrrf_calculate_srrf_u16_device(
                 H, ctypes.c_void_p(base + b * nf * frame_bytes), nf))
             _, r_ms, nl = eng.lastTiming()
@@ -447,6 +522,7 @@ def run_ours(args, world, rank, local):
         base = h_stack.data_ptr()
         for b in range(n_blocks):
             esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
+            set_drift(b)
             esrrf._lib.check(H, L.esrrf_calculate_srrf_u16(
                 H, ctypes.c_void_p(base + b * nf * frame_bytes), nf))
             esrrf._lib.check(H, L.esrrf_read_srrf_async(H, ctypes.c_void_p(h_out[b].data_ptr())))
@@ -500,29 +576,35 @@ def run_ours(args, world, rank, local):
     avg_launch_s = (rgc_total_ms / 1000.0) / max(1, launches_rgc)
     taps = bic_taps_per_pixel(M, fwhm) if bic else taps_per_pixel(M, fwhm)
     peaks, peak_src = load_peaks()
-    # compulsory HBM bytes of the path per input pixel-frame: raw uint16 in, plus the four
-    # float outputs of each block amortised over its frames
-    bytes_per_unit = 2.0 + 4 * 4 * M * M / nf
+    # compulsory HBM bytes of the path per input pixel-frame: raw uint16 in, plus the block's
+    # three cumulant outputs (AVG, VAR, TAC2 in float) amortised over its frames -- the fixed
+    # convention of the workload table; INT, a by-product, is not counted
+    bytes_per_unit = 2.0 + 3 * 4 * M * M / nf
     alg_bytes_launch = F * h * w * bytes_per_unit
     achieved_gbs = alg_bytes_launch / avg_launch_s / 1e9
     ops_launch = F * WM * HM * taps * OPS_PER_TAP
     achieved_tflops = ops_launch / avg_launch_s / 1e12
     cpu = (cpu_reference_sample(stack, M, fwhm, S, 2 if bic else 1, bic=bic)
            if not args.no_cpu_baseline and world == 1 else None)
-    traffic = read_traffic_summary(f"rgc_{args.kernel}_{args.workload}")
+    summary_key = f"rgc_{args.kernel}_{args.workload}"
+    stale = summary_stale(summary_key)
+    traffic = None if stale or args.drift else read_traffic_summary(summary_key)
     # the kernel's real limit is instruction issue: warp instructions per launch (ncu count per
     # frame x frames) over the live launch time, against one warp instruction per cycle per
     # scheduler (148 SMs x 4) at the sampled SM clock
     clocks = clk.summary()
-    ipf = read_traffic_summary(f"rgc_{args.kernel}_{args.workload}", "warp_instructions_per_frame")
+    ipf = None if stale or args.drift else read_traffic_summary(summary_key, "warp_instructions_per_frame")
     roofline_issue = None
-    if ipf and avg_launch_s > 0:
+    if stale:
+        roofline_issue = {"unavailable": stale}
+    elif ipf and avg_launch_s > 0:
         mhz = clocks.get("sm_mhz") or 1965.0
         peak_issue = 148 * 4 * mhz * 1e6
         got = ipf * (nf / ((nf + F - 1) // F)) / avg_launch_s  # mean frames per launch
         roofline_issue = {"achieved": got, "peak": peak_issue, "unit": "warp instructions/s",
                           "frac": got / peak_issue, "instructions_per_frame": ipf,
-                          "source": "instructions per frame from the committed ncu summary, launch time live"}
+                          "source": "instructions per frame from the committed ncu summary of this "
+                                    "kernel source (sha recorded there), launch time live"}
     line = {
         "metric": f"input Mpx*frames/s (eSRRF {path_label(args.workload)})",
         "value": value, "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps,
@@ -537,7 +619,11 @@ def run_ours(args, world, rank, local):
                           f"inputs ({stack.nbytes / 1e6:.1f} MB) fit in L2, not flushed between steps "
                           "(small parity workload; the kernel reads its interpolated frames, "
                           f"{n * WM * HM * 4 / 1e6:.0f} MB, from HBM)"),
-                   "parallelism": f"replicas x{world}"},
+                   "drift": ("seeded per-frame shifts, |s| < 1.5 raw px (vibration correction)"
+                             if args.drift else "none"),
+                   "parallelism": (f"blocks sharded x{world} (esrrf_sweep_plan: contiguous runs of the "
+                                   f"{world * n_blocks} blocks of a {world * n}-frame stack; blocks "
+                                   f"{blocks_here[0]}..{blocks_here[-1]} here)" if world > 1 else "1 GPU")},
         "e2e": {"value": e2e_value, "unit": "Mpx*frames/s", "h2d_bytes_per_step": int(stack.nbytes),
                 "d2h_bytes_per_step": int(h_out.numel() * 4)},
         "gpu_launches": gpu_launches,
@@ -1060,6 +1146,8 @@ def main():
     ap.add_argument("--frames", type=int, default=None,
                     help="shorter stack (profiling runs); default: the workload's length")
     ap.add_argument("--block", type=int, default=0, help="frames per block override")
+    ap.add_argument("--drift", action="store_true",
+                    help="fht512/bic512: a seeded per-frame shift in every block (vibration correction)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

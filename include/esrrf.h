@@ -358,12 +358,18 @@ esrrf_status esrrf_adjoint_destroy(esrrf_adjoint* a);
  * block (FHT interpolation, mean-preserving scale, zero drift, fused RGC, FP64 cumulants) and
  * takes every temporary buffer from one 64 MiB static device array that each GPU loading the
  * library holds until exit; frame sizes whose tables, buffers and accumulators need more than
- * that (roughly widthM x heightM above 1.3 M pixels) are rejected with ESRRF_ERR_INVALID, as
- * are radii whose tap box exceeds 32 magnified pixels.
+ * that (roughly widthM x heightM above 1.2 M pixels) are rejected with ESRRF_ERR_INVALID, as
+ * are radii whose tap box exceeds 32 magnified pixels.  The interpolation's dense passes run on
+ * the FP32 SIMT kernels (the handle uses tensor cores on large frames): the results agree with
+ * the handle's to ~1e-6 of each slice's range.
  * d_frames: device [n_frames][height][width], uint16 (is_u16 = 1) or float.  d_out: device
- * [4][height*M][width*M] float (AVG, VAR, TAC2, INT).  stream: cudaStream_t or NULL; the call
- * only enqueues work on it.  err/err_len: optional buffer for a message on failure.
- * The first call on a device looks up the array's address (cudaGetSymbolAddress, with that
+ * [4][height*M][width*M] float (AVG, VAR, TAC2, INT).  stream: cudaStream_t or NULL.
+ * err/err_len: optional buffer for a message on failure.
+ * The tables (interpolation, tap weights) are kept in the array between calls: a call with the
+ * same frame size, magnification, radius and sensitivity as the previous call on its device only
+ * enqueues kernels; a call that changes them first builds them on the host and uploads them with
+ * pageable copies (which wait for the stream's earlier work), so make one such call at set-up.
+ * The first call on a device also looks up the array's address (cudaGetSymbolAddress, with that
  * device current) -- make it before any stream capture.  Calls share the array and it keeps
  * the last call's contents (the accumulators are cleared at the start of each call); calls
  * whose work overlaps on the GPU race on it. */

@@ -24,12 +24,38 @@ def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
+def _headers():
+    return (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+            glob.glob(os.path.join(INCLUDE, "*.h")))
+
+
 def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(INCLUDE, "*.h"))
-    return any(os.path.getmtime(d) > t for d in deps)
+    return any(os.path.getmtime(d) > t for d in sources() + _headers())
+
+
+def _deps(path: str, seen=None) -> set:
+    """The file and every header it reaches through #include "..." lines."""
+    import re
+
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path, errors="replace") as f:
+        for inc in re.findall(r'^\s*#\s*include\s+"([^"]+)"', f.read(), flags=re.M):
+            _deps(os.path.normpath(os.path.join(os.path.dirname(path), inc)), seen)
+    return seen
+
+
+def _obj_stale(src: str, obj: str) -> bool:
+    """An object is rebuilt when it is missing or older than its source or a header it includes."""
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in _deps(src))
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -42,17 +68,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     procs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-I", INCLUDE, "-c", src, "-o", obj]
+        objs.append(obj)
+        if not (force or verbose or _obj_stale(src, obj)):
+            continue
+        cmd = [NVCC, *ARCH, *FLAGS, "-I", INCLUDE, "-c", src, "-o", obj + ".tmp"]
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
-        objs.append(obj)
+        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
     failed = False
-    for src, p in procs:
+    for src, obj, p in procs:
         out, _ = p.communicate()
         if p.returncode != 0 or verbose:
             sys.stderr.write(out.decode())
         failed |= p.returncode != 0
+        if p.returncode == 0:
+            os.replace(obj + ".tmp", obj)
     if failed:
         raise RuntimeError("nvcc failed")
     tmp = LIB + ".tmp"

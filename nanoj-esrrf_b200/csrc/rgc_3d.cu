@@ -622,6 +622,226 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
     }
 }
 
+// rgc3d_zs_kernel with two cells per thread: thread (tx, ty) of a CTA computes the cells in rows
+// ty and ty + 8 of a 32 x 16 cell tile (same lateral phase, so the same entry list).  Each entry's
+// table values (offset, dx, dy, and per z-phase dz, w, w/d) are loaded once for both cells, and the
+// two cells' dot / cross / square-root chains are independent, which doubles the work each warp
+// has in flight per entry.  The per-voxel epilogue state is kept to the FP32 sums and previous
+// values (index, sum of weights and z-cubic position are recomputed at the end of a timepoint), so
+// that two CTAs of 256 threads run per SM without spilling.  Slab: the tile's 16 cell rows' 2x-grid
+// rows plus the tap reach (16 more rows than rgc3d_zs_kernel's), same columns; the entries' slab
+// offsets are the same (they depend on the row length only).
+template <int MZ>
+__global__ void __launch_bounds__(256, 2) rgc3d_z2_kernel(Rgc3dTabArgs a) {
+    extern __shared__ float4 sm4[];
+    constexpr int M = MZ;
+    const int es = a.tab.zes, nz = a.tab.znz;
+    const int lp = blockIdx.x, bx = blockIdx.y;
+    const int nby = (a.h + 15) / 16;
+    const int qz = blockIdx.z / nby, by = blockIdx.z - qz * nby;
+    const int px = lp % M, py = lp / M;
+    const int t0 = a.tab.zstart[lp], n = a.tab.zstart[lp + 1] - t0;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int row2 = 2 * a.tab.sl_nx;                       // float4s per slab row
+    const int rows = a.tab.sl_rows + 16;                    // slab rows of 16 cell rows
+    const int slab = rows * row2;                           // float4s per slab
+    float4* stab = sm4;                                     // [n][es]
+    int* sseg = reinterpret_cast<int*>(sm4 + a.tab.zmax_taps * es);  // [nz + 1]
+    float4* sbuf = sm4 + a.tab.zmax_taps * es + (nz + 4) / 4;        // [2][slab]
+    for (int i = tid; i < n * es; i += 256) {
+        float4 v = a.tab.ztab[(long)t0 * es + i];
+        if (i % es == 0) v.x = __int_as_float(a.tab.zsoff[t0 + i / es]);  // offset in the slab
+        stab[i] = v;
+    }
+    for (int i = tid; i <= nz; i += 256) sseg[i] = a.tab.zseg[lp * (nz + 1) + i];
+    const float* sf = reinterpret_cast<const float*>(stab);
+    const int qx_raw = bx * 32 + threadIdx.x;
+    int qy_raw[2];
+    qy_raw[0] = by * 16 + threadIdx.y;
+    qy_raw[1] = qy_raw[0] + 8;
+    const int WM = a.w * M, HM = a.h * M;
+    const long whM = (long)WM * HM, total = whM * a.P * M;
+    const long pl = (long)a.w * a.h;
+    const long fstride = (long)a.tab.Pp * a.tab.H2p * a.tab.W2p;
+    const int half = a.tab.W2p / 2;
+    const int row0 = 2 * by * 16 + a.tab.pady + a.tab.sl_symin;
+    const int cin0 = a.tab.padx / 2 + bx * 32 + a.tab.sl_fxmin;
+    const int tbase = 2 * threadIdx.y * row2 + threadIdx.x;  // cell 0 in the slab; cell 1 16 rows down
+    const int cell1 = 16 * row2;
+    float s0[2][MZ], s1[2][MZ], s2[2][MZ], s3[2][MZ], prev[2][MZ];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const bool valid = qx_raw < a.w && qy_raw[c] < a.h;
+        const int yM = min(qy_raw[c], a.h - 1) * M + py, xM = min(qx_raw, a.w - 1) * M + px;
+#pragma unroll
+        for (int p = 0; p < MZ; ++p) {
+            const long idx = (long)(qz * M + p) * whM + (long)yM * WM + xM;
+            prev[c][p] = valid ? a.st.prev[idx] : 0.f;
+            s0[c][p] = s1[c][p] = s2[c][p] = s3[c][p] = 0.f;
+        }
+    }
+    // the z-cubic's base planes: zlo is the lowest base plane of the cell's z-phases
+    int zlo = a.P;
+#pragma unroll
+    for (int p = 0; p < MZ; ++p) {
+        const float zcof = (float)(((double)(qz * M + p) + 0.5) / M) - 0.5f;
+        const int z0 = zcof < 0 ? 0 : (zcof >= (float)(a.P - 1) ? a.P - 2 : (int)floorf(zcof));
+        zlo = min(zlo, z0);
+    }
+    int splane[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) splane[k] = min(max(zlo - 1 + k, 0), a.P - 1);
+
+    int coff[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int rem = threadIdx.x + 32 * q;
+        const int par = rem >= a.tab.sl_nx ? 1 : 0, cin = cin0 + rem - par * a.tab.sl_nx;
+        coff[q] = rem < row2 && cin < half ? par * half + cin : -1;
+    }
+    auto stage = [&](int g) {
+        const int f = g / nz, sidx = g - f * nz;
+        const int plane = qz + a.tab.padz_lo + a.tab.zk0 + sidx;
+        const float4* Uf = a.U + f * fstride + (long)plane * a.tab.H2p * a.tab.W2p;
+        float4* dst = sbuf + (g & 1) * slab;
+        for (int ly = threadIdx.y; ly < rows; ly += 8) {
+            const int row = row0 + ly;
+            const bool rin = row < a.tab.H2p;
+            const float4* src = Uf + (long)row * a.tab.W2p;
+            float4* d = dst + ly * row2 + threadIdx.x;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if ((int)threadIdx.x + 32 * q >= row2) break;
+                const bool in = rin && coff[q] >= 0;
+                cp_async16(d + 32 * q, in ? (const void*)(src + coff[q]) : (const void*)a.U, in);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    const int G = a.F * nz;
+    if (G > 0) stage(0);
+    float cg[2][MZ];
+    for (int g = 0; g < G; ++g) {
+        const int f = g / nz, sidx = g - f * nz;
+        if (sidx == 0) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int p = 0; p < MZ; ++p) cg[c][p] = 0.f;
+        }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // slab g landed everywhere; buffer (g + 1) & 1 is no longer read
+        if (g + 1 < G) stage(g + 1);
+        const float4* sl = sbuf + (g & 1) * slab + tbase;
+        const int tb = sseg[sidx], te = sseg[sidx + 1];
+        for (int t = tb; t < te; ++t) {
+            const float* e = sf + (long)t * es * 4;
+            const int o = __float_as_int(e[0]);
+            const float dx = e[1], dy = e[2];
+            float4 u[2];
+            u[0] = sl[o];
+            u[1] = sl[o + cell1];
+            float part[2], cz2[2], dyuz[2], dxuz[2];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                part[c] = fmaf(u[c].x, dx, u[c].y * dy);
+                const float cz = fmaf(dx, u[c].y, -dy * u[c].x);  // dx gy - dy gx
+                cz2[c] = cz * cz;
+                dyuz[c] = dy * u[c].z;
+                dxuz[c] = dx * u[c].z;
+            }
+#pragma unroll
+            for (int p = 0; p < MZ; ++p) {
+                const float dz = e[3 + 3 * p], w = e[4 + 3 * p], wd = e[5 + 3 * p];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float dot = fmaf(u[c].z, dz, part[c]);
+                    if (dot < 0.f) {
+                        const float cx = fmaf(-dz, u[c].y, dyuz[c]);  // dy gz - dz gy
+                        const float cy = fmaf(dz, u[c].x, -dxuz[c]);  // dz gx - dx gz
+                        cg[c][p] += fmaf(-wd, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz2[c]))), w);
+                    }
+                }
+            }
+        }
+        if (sidx != nz - 1) continue;
+        const float* ap = a.apx + (long)f * a.P * pl;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int yM = min(qy_raw[c], a.h - 1) * M + py, xM = min(qx_raw, a.w - 1) * M + px;
+            float S[4];
+            dev::sample2d_x4(ap, pl, splane, a.w, a.h, (float)xM / (float)M - 0.5f,
+                             (float)yM / (float)M - 0.5f, S);
+#pragma unroll
+            for (int p = 0; p < MZ; ++p) {
+                const int zM = qz * M + p;
+                const long idx = (long)zM * whM + (long)yM * WM + xM;
+                const float zc = (float)(((double)zM + 0.5) / M);
+                const float zcof = zc - 0.5f;
+                const int z0 = zcof < 0 ? 0 : (zcof >= (float)(a.P - 1) ? a.P - 2 : (int)floorf(zcof));
+                const float zz = zc - (float)(z0 + 0.5f);
+                const float cgv = cglh_power(cg[c][p] / __ldg(a.tab.wsum + idx), a.sens);
+                const bool d1 = z0 != zlo;
+                const float v_1 = d1 ? S[1] : S[0];
+                const float v0 = d1 ? S[2] : S[1];
+                const float v1 = d1 ? S[3] : S[2];
+                const float v2 = v1;
+                const float ca = -0.5f * v_1 + 1.5f * v0 - 1.5f * v1 + 0.5f * v2;
+                const float cb = v_1 - 2.5f * v0 + 2.0f * v1 - 0.5f * v2;
+                const float cc = -0.5f * v_1 + 0.5f * v1;
+                const float v = ca * zz * zz * zz + cb * zz * zz + cc * zz + v0;
+                const float x = a.int_weighting ? v * cgv : cgv;
+                s0[c][p] += x;
+                s1[c][p] = fmaf(x, x, s1[c][p]);
+                if (a.t0 + f > 0) s2[c][p] = fmaf(x, prev[c][p], s2[c][p]);
+                s3[c][p] += v;
+                prev[c][p] = x;
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        if (qx_raw >= a.w || qy_raw[c] >= a.h) continue;
+        const int yM = qy_raw[c] * M + py, xM = qx_raw * M + px;
+#pragma unroll
+        for (int p = 0; p < MZ; ++p) {
+            const long idx = (long)(qz * M + p) * whM + (long)yM * WM + xM;
+            a.st.acc[idx] += (double)s0[c][p];
+            a.st.acc[total + idx] += (double)s1[c][p];
+            a.st.acc[2 * total + idx] += (double)s2[c][p];
+            a.st.acc[3 * total + idx] += (double)s3[c][p];
+            a.st.prev[idx] = prev[c][p];
+        }
+    }
+}
+
+size_t z2_smem_bytes(const Rgc3dTables& t) {
+    return sizeof(float4) * ((size_t)t.zmax_taps * t.zes + (t.znz + 4) / 4 +
+                             2 * (size_t)(t.sl_rows + 16) * 2 * t.sl_nx);
+}
+
+template <int MZ>
+cudaError_t launch_z2(const Rgc3dTabArgs& a, cudaStream_t stream) {
+    const size_t smem = z2_smem_bytes(a.tab);
+    static unsigned long long configured = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && !(configured & (1ull << dev))) {
+        if ((e = cudaFuncSetAttribute(rgc3d_z2_kernel<MZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      112 * 1024)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(rgc3d_z2_kernel<MZ>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+            return e;
+        configured |= 1ull << dev;
+    }
+    if (smem > 112 * 1024) return cudaErrorInvalidValue;
+    if ((a.w + 31) / 32 > 65535 || (long)((a.h + 15) / 16) * a.P > 65535) return cudaErrorInvalidValue;
+    const dim3 grid(MZ * MZ, (a.w + 31) / 32, ((a.h + 15) / 16) * a.P);
+    rgc3d_z2_kernel<MZ><<<grid, dim3(32, 8), smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
 size_t zs_smem_bytes(const Rgc3dTables& t) {
     return sizeof(float4) * ((size_t)t.zmax_taps * t.zes + (t.znz + 4) / 4 + 2 * (size_t)t.sl_rows * 2 * t.sl_nx);
 }
@@ -874,14 +1094,17 @@ cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream) {
     if (a.tab.ztab && !rgc3d_one_voxel()) {
         // slab-staged form where two CTAs' shared memory fits an SM (ESRRF_RGC3D=zb: the form
         // that reads the field through the L1 cache)
+        // and the two-cells-per-thread slab form where its taller slab fits too (ESRRF_RGC3D=zs:
+        // one cell per thread)
         const char* form = std::getenv("ESRRF_RGC3D");
         const bool slab = zs_smem_bytes(a.tab) <= 112 * 1024 && 2 * a.tab.sl_nx <= 128 &&
                           !(form && std::strcmp(form, "zb") == 0);
+        const bool two = slab && z2_smem_bytes(a.tab) <= 112 * 1024 && !(form && std::strcmp(form, "zs") == 0);
         switch (a.M) {
-            case 2: return slab ? launch_zs<2>(a, stream) : launch_zb<2>(a, stream);
-            case 3: return slab ? launch_zs<3>(a, stream) : launch_zb<3>(a, stream);
-            case 4: return slab ? launch_zs<4>(a, stream) : launch_zb<4>(a, stream);
-            case 5: return slab ? launch_zs<5>(a, stream) : launch_zb<5>(a, stream);
+            case 2: return two ? launch_z2<2>(a, stream) : slab ? launch_zs<2>(a, stream) : launch_zb<2>(a, stream);
+            case 3: return two ? launch_z2<3>(a, stream) : slab ? launch_zs<3>(a, stream) : launch_zb<3>(a, stream);
+            case 4: return two ? launch_z2<4>(a, stream) : slab ? launch_zs<4>(a, stream) : launch_zb<4>(a, stream);
+            case 5: return two ? launch_z2<5>(a, stream) : slab ? launch_zs<5>(a, stream) : launch_zb<5>(a, stream);
             default: break;
         }
     }
