@@ -76,7 +76,8 @@ typedef struct {
     int kernel;           /* 0: fused tile kernel where applicable, 1: plain per-pixel kernel */
     int frames_per_launch;/* frames per interpolation + RGC launch; 0: the block in equal launches of
                              at most 50 frames (FHT path, within ~4 GB of frame buffers) or 32
-                             (2-D bicubic path, within ~2 GB), 8 timepoints in 3-D */
+                             (2-D bicubic path, within ~2 GB), 8 timepoints in 3-D;
+                             ESRRF_FRAMES_PER_LAUNCH_TUNED: measured by the autotuner (below) */
     /* 3-D calibration, all arrays of length n_planes (NULL in 2-D). */
     int n_planes;
     const float* roi;
@@ -146,8 +147,23 @@ esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* d_out);
 esrrf_status esrrf_read_srrf_async(esrrf_handle* h, float* out);
 
 /* Frames (timepoints in 3-D) per interpolation + RGC launch: esrrf_params.frames_per_launch, or
- * the value chosen when that is 0 (no reference counterpart: the reference launches per frame). */
+ * the value chosen when that is 0 or ESRRF_FRAMES_PER_LAUNCH_TUNED (no reference counterpart: the
+ * reference launches per frame). */
 esrrf_status esrrf_frames_per_launch(const esrrf_handle* h, int* frames);
+
+/* Autotuner.  The reference sizes its GPU loads from a memory model (calculatenFrameOnGPU /
+ * predictMemoryUsed, gui/LiveSRRF_optimised_.java:763-877); here esrrf_create with
+ * frames_per_launch = ESRRF_FRAMES_PER_LAUNCH_TUNED measures instead: for the parameter set's
+ * frame size, magnification, tap box, path and block length it times one block of synthetic frames
+ * through a temporary engine for each candidate frames-per-launch value (every way to cut the
+ * block into equal launches of 8 to 64 frames that fits ~4 GB; in 3-D also the tabulated kernel's
+ * forms: two cells per thread, one cell per thread with the slab in shared memory, the field read
+ * through L1), keeps the fastest, and caches the choice in a text file keyed by the device name
+ * and those parameters (ESRRF_TUNE_CACHE, else esrrf_tune.txt beside libesrrf.so), so later
+ * handles with the same key are created without measuring.  esrrf_tune_report gives the choice,
+ * its source ("measured", "cache" or "off") and the candidates' times as JSON text. */
+#define ESRRF_FRAMES_PER_LAUNCH_TUNED (-1)
+esrrf_status esrrf_tune_report(const esrrf_handle* h, char* buf, size_t len);
 
 /* Output geometry (public fields widthS/heightS/nPlanes/nPlanesM, LiveSRRF_CL.java:41-45). */
 esrrf_status esrrf_output_shape(const esrrf_handle* h, int* width_m, int* height_m,

@@ -53,7 +53,8 @@ esrrf_status validate(const esrrf_params& p, std::string& msg) {
     if (p.sensitivity < 0 || p.sensitivity > 64) return msg = "sensitivity must be in [0, 64]", ESRRF_ERR_INVALID;
     if (p.n_frame_for_srrf < 1) return msg = "n_frame_for_srrf must be >= 1", ESRRF_ERR_INVALID;
     if (p.n_frames_on_gpu < 1) return msg = "n_frames_on_gpu must be >= 1", ESRRF_ERR_INVALID;
-    if (p.frames_per_launch < 0) return msg = "frames_per_launch must be >= 0", ESRRF_ERR_INVALID;
+    if (p.frames_per_launch < ESRRF_FRAMES_PER_LAUNCH_TUNED)
+        return msg = "frames_per_launch must be >= 0, or ESRRF_FRAMES_PER_LAUNCH_TUNED", ESRRF_ERR_INVALID;
     if (p.n_planes < 0) return msg = "n_planes must be >= 0", ESRRF_ERR_INVALID;
     if (p.n_planes > 0) {
         if (!p.roi || !p.theta_deg || !p.shift_x || !p.shift_y || !p.intensity_coeff)
@@ -514,6 +515,7 @@ esrrf_status esrrf_handle::process_chunk_bic3d(const void* src, bool is_u16, int
             ta.int_weighting = p.int_weighting;
             ta.tab = t3d;
             ta.st = st;
+            ta.form = form3d;
             CK(rgc_3d_tab(ta, stream));
             launches += 1;
         }
@@ -732,9 +734,23 @@ esrrf_status esrrf_create(const esrrf_params* params, esrrf_handle** out) {
         g_create_error = msg;
         return s;
     }
+    esrrf_params prm = *params;
+    TuneChoice tuned;
+    if (prm.frames_per_launch == ESRRF_FRAMES_PER_LAUNCH_TUNED) {
+        // measured (or cached) frames per launch and kernel form, then the handle proper
+        s = tune_engine(prm, tuned, msg);
+        if (s != ESRRF_OK) {
+            std::lock_guard<std::mutex> lk(g_err_mu);
+            g_create_error = msg;
+            return s;
+        }
+        prm.frames_per_launch = tuned.frames_per_launch;
+    }
     esrrf_handle* h = new (std::nothrow) esrrf_handle();
     if (!h) return ESRRF_ERR_NOMEM;
-    s = h->init(*params);
+    h->form3d = tuned.form;
+    h->tune_report = tuned.report;
+    s = h->init(prm);
     if (s != ESRRF_OK) {
         {
             std::lock_guard<std::mutex> lk(g_err_mu);
@@ -791,6 +807,14 @@ esrrf_status esrrf_read_srrf(esrrf_handle* h, float* out) {
 esrrf_status esrrf_read_srrf_device(esrrf_handle* h, float* out) {
     if (!h || !out) return ESRRF_ERR_INVALID;
     return h->read(out, true);
+}
+
+esrrf_status esrrf_tune_report(const esrrf_handle* h, char* buf, size_t len) {
+    if (!h || !buf || len == 0) return ESRRF_ERR_INVALID;
+    const std::string& r = h->tune_report.empty() ? std::string("{\"source\": \"off\"}") : h->tune_report;
+    strncpy(buf, r.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return r.size() < len ? ESRRF_OK : ESRRF_ERR_INVALID;
 }
 
 esrrf_status esrrf_frames_per_launch(const esrrf_handle* h, int* frames) {

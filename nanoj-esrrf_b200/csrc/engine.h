@@ -7,6 +7,16 @@
 #include "../../include/esrrf.h"
 #include "esrrf_internal.h"
 
+// Choice of the autotuner (tune.cu) for one parameter set.
+struct TuneChoice {
+    int frames_per_launch = 0;
+    int form = 0;
+    std::string report;
+};
+// Times candidate frames-per-launch values (and, in 3-D, kernel forms) on synthetic frames of the
+// parameters' size, or reads an earlier result from the cache file; fills `out`.
+esrrf_status tune_engine(const esrrf_params& p, TuneChoice& out, std::string& msg);
+
 struct esrrf_handle {
     enum class Mode { kFHT, kBIC, k3D };
 
@@ -91,6 +101,8 @@ struct esrrf_handle {
     float t_interp = 0.f, t_rgc = 0.f;
     int launches = 0, n_rgc_launches = 0;
     bool own_stream = true;
+    int form3d = 0;             // tabulated 3-D kernel form (kRgc3d*; 0: default choice)
+    std::string tune_report;    // what the autotuner measured or read (empty: not tuned)
 
     esrrf_status timing_event(cudaEvent_t* out);
     void collect_timing();

@@ -329,7 +329,11 @@ struct Rgc3dTabArgs {
     int int_weighting;
     Rgc3dTables tab;
     BlockState st;
+    int form = 0;        // kRgc3dForm*: which tabulated kernel (0: the default choice)
 };
+// Forms of the tabulated 3-D RGC (rgc_3d_tab); a form whose shared memory does not fit falls
+// back to the next one.
+constexpr int kRgc3dAuto = 0, kRgc3dTwoCells = 1, kRgc3dSlab = 2, kRgc3dL1 = 3;
 // unit gradient field from the 2x-resampled components (Gx read at x+1, Gy at y+1, Gz in place)
 // into the interior of the padded field; zero where no tap may read (plane 0, last column and
 // row).  The halo is zeroed once, when the field is allocated.

@@ -1096,10 +1096,12 @@ cudaError_t rgc_3d_tab(const Rgc3dTabArgs& a, cudaStream_t stream) {
         // that reads the field through the L1 cache)
         // and the two-cells-per-thread slab form where its taller slab fits too (ESRRF_RGC3D=zs:
         // one cell per thread)
-        const char* form = std::getenv("ESRRF_RGC3D");
-        const bool slab = zs_smem_bytes(a.tab) <= 112 * 1024 && 2 * a.tab.sl_nx <= 128 &&
-                          !(form && std::strcmp(form, "zb") == 0);
-        const bool two = slab && z2_smem_bytes(a.tab) <= 112 * 1024 && !(form && std::strcmp(form, "zs") == 0);
+        const char* env = std::getenv("ESRRF_RGC3D");
+        int form = a.form;
+        if (form == kRgc3dAuto && env)
+            form = std::strcmp(env, "zb") == 0 ? kRgc3dL1 : std::strcmp(env, "zs") == 0 ? kRgc3dSlab : kRgc3dAuto;
+        const bool slab = zs_smem_bytes(a.tab) <= 112 * 1024 && 2 * a.tab.sl_nx <= 128 && form != kRgc3dL1;
+        const bool two = slab && z2_smem_bytes(a.tab) <= 112 * 1024 && form != kRgc3dSlab;
         switch (a.M) {
             case 2: return two ? launch_z2<2>(a, stream) : slab ? launch_zs<2>(a, stream) : launch_zb<2>(a, stream);
             case 3: return two ? launch_z2<3>(a, stream) : slab ? launch_zs<3>(a, stream) : launch_zb<3>(a, stream);

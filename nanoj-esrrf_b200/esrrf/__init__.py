@@ -100,7 +100,8 @@ class LiveSRRF_CL:
         p.interp = 0 if doFHTinterpolation else 1
         p.fht_scale = {"mean_preserving": 0, "unitary_big": 1}[fhtScale]
         p.kernel = {"fused": 0, "plain": 1}[kernel]
-        p.frames_per_launch = int(framesPerLaunch)
+        # "auto": measured by the library's autotuner (cached per parameter set)
+        p.frames_per_launch = -1 if framesPerLaunch == "auto" else int(framesPerLaunch)
         p.axial_offset_nm = float(axialOffset)
         p.pixel_size_um = float(pixelSize)
         self._keep = []
@@ -217,6 +218,15 @@ class LiveSRRF_CL:
         f = ctypes.c_int()
         _lib.check(self._h, lib().esrrf_frames_per_launch(self._h, ctypes.byref(f)))
         return f.value
+
+    def tuneReport(self) -> dict:
+        """What the autotuner chose for this engine (esrrf_tune_report): source "measured",
+        "cache" or "off", frames_per_launch, form and the candidates' times."""
+        import json
+
+        buf = ctypes.create_string_buffer(8192)
+        _lib.check(self._h, lib().esrrf_tune_report(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
 
     def lastTiming(self):
         i, r, n = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()

@@ -138,6 +138,7 @@ SIGNATURES.update({
     "esrrf_sweep_run": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_int, _c.c_void_p]),
     "esrrf_sweep_launch_count": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
     "esrrf_sweep_shard_count": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
+    "esrrf_tune_report": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_size_t]),
     "esrrf_sweep_plan": (_c.c_int, [_c.POINTER(EsrrfSweepParams), _c.POINTER(_c.c_int),
                                     _c.POINTER(_c.c_int), _c.POINTER(_c.c_double)]),
     "esrrf_sweep_last_error": (_c.c_char_p, [_c.c_void_p]),
