@@ -110,6 +110,37 @@ def bic_taps_per_pixel(M, fwhm):
     return total / (M * M)
 
 
+def taps3d_per_voxel(M, fwhm):
+    """Interior tap count of the 3-D path averaged over the M^3 sub-pixel phases: lateral offsets on
+    the 2x gradient grid, z offsets on whole planes, inside the sphere, zero excluded
+    (live3DSRRF.cl:325-498 geometry, FP32 as the kernel evaluates it)."""
+    f = np.float32
+    sigma = f(fwhm) / f(2.354)
+    radius = f(int(f(4) * sigma)) / f(2) + f(1)
+    tSO = f(2) * sigma + f(1)
+    r0, r1 = -int(f(2) * radius), int(f(2) * radius + f(1))
+    k0, k1 = -int(radius), int(radius) + 1
+    total = 0
+    for pz in range(M):
+        zc = f((pz + 0.5) / M)
+        for py in range(M):
+            yc = f((py + 0.5) / M)
+            ky = int(f(2) * yc)
+            for px in range(M):
+                xc = f((px + 0.5) / M)
+                kx = int(f(2) * xc)
+                for j in range(r0, r1 + 1):
+                    dy = f(f(ky + j) / f(2)) - yc
+                    for i in range(r0, r1 + 1):
+                        dx = f(f(kx + i) / f(2)) - xc
+                        for k in range(k0, k1 + 1):
+                            dz = f(f(int(zc)) + f(k)) - zc
+                            d = np.sqrt(f(dx * dx + dy * dy + dz * dz))
+                            if d != 0 and d <= tSO:
+                                total += 1
+    return total / (M ** 3)
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -918,17 +949,22 @@ def run_3d(args, world, rank, local):
     eng.initialise(3 * w, 3 * h, M, fwhm, S, n, n, chosenDevice=local, doMPmapCorrection=True,
                    calibTable3DSRRF=calib, framesPerLaunch=args.frames_per_launch or 8, kernel=args.kernel)
     H = eng.handle
+    eng.setTiming(True)
     launches = [0]
+    rgc_ms = [0.0]
 
     def step():
         esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
         esrrf._lib.check(H, L.esrrf_calculate_srrf_u16_device(H, ctypes.c_void_p(d_cam.data_ptr()), n))
-        launches[0] += eng.lastTiming()[2] + 3
+        _, r_ms, nl = eng.lastTiming()
+        launches[0] += nl + 3
+        rgc_ms[0] += r_ms
         esrrf._lib.check(H, L.esrrf_read_srrf_device(H, ctypes.c_void_p(d_out.data_ptr())))
 
     for _ in range(args.warmup):
         step()
     launches[0] = 0
+    rgc_ms[0] = 0.0
     barrier(world)
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
@@ -943,6 +979,7 @@ def run_3d(args, world, rank, local):
         torch.cuda.synchronize()
     barrier(world)
     t_step = max_over_ranks(world, ev0.elapsed_time(ev1) / 1000.0 / args.steps)
+    rgc_timed = [rgc_ms[0]]
     h_cam = torch.from_numpy(cam.view(np.int16)).pin_memory()
     h_out = torch.empty((4 * P * M, h * M, w * M), dtype=torch.float32).pin_memory()
     t0 = time.perf_counter()
@@ -959,6 +996,16 @@ def run_3d(args, world, rank, local):
     shy = np.asarray(calib["Y-shift (pixels)"], np.float32)
     cpu = (cpu_3d_sample(planes, M, fwhm, S, th, shx, shy, 2)
            if not args.no_cpu_baseline and world == 1 else None)
+    # FP32 convention of the RGC launches: 22 ops per evaluated tap, taps per voxel averaged over
+    # the sub-pixel phases, RGC launch time from the engine's CUDA events over the timed steps
+    taps = taps3d_per_voxel(M, fwhm)
+    rgc_s = rgc_timed[0] / 1e3 / args.steps
+    ops = n * P * M * h * M * w * M * taps * OPS_PER_TAP
+    roofline_fp32 = ({"achieved": ops / rgc_s / 1e12, "peak": FP32_PEAK_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                      "frac": ops / rgc_s / 1e12 / FP32_PEAK_NOMINAL_TFLOPS, "ops_per_step": ops,
+                      "taps_per_voxel": taps, "rgc_ms_per_step": rgc_s * 1e3,
+                      "convention": "22 FP32 ops per evaluated tap; nominal peak at 1965 MHz"}
+                     if rgc_s > 0 else None)
     print(json.dumps({
         "metric": "input Mpx*frames/s (eSRRF 3-D MFM path)", "value": world * mpxf / t_step,
         "unit": "Mpx*frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -973,7 +1020,8 @@ def run_3d(args, world, rank, local):
                   "plain_1_timepoint_per_launch_mpx_frames_s": mpxf / (plain_ms / 1e3) if plain_ms else None},
         "e2e": {"value": mpxf / e2e, "unit": "Mpx*frames/s", "h2d_bytes_per_step": int(cam.nbytes),
                 "d2h_bytes_per_step": int(h_out.numel() * 4)},
-        "gpu_launches": launches[0], "clocks": clk.summary(), "cpu_baseline": cpu}))
+        "gpu_launches": launches[0], "roofline_fp32": roofline_fp32, "clocks": clk.summary(),
+        "cpu_baseline": cpu}))
 
 
 def drift_cpu_sample(stack, n):

@@ -23,6 +23,8 @@
 // then skips its stores and releases its TMEM.
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -368,6 +370,225 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_kernel(TcArgs g) {
     }
 }
 
+// Persistent form of tc_gemm_kernel: one CTA per SM walks the tiles t = blockIdx.x + i gridDim.x
+// (column tile fastest, then row tile, then frame).  The producer keeps streaming the next tile's
+// panels and the MMA warp keeps issuing into the two TMEM accumulators while the drain warps write
+// the previous tile's epilogue, so a tile's epilogue overlaps the next tile's first two runs and
+// the ring never drains between tiles.  Stage, run and parity counters run across tiles.  The
+// drain warps reload pass 2's per-column terms into shared memory per tile between two named
+// barriers of their own (bar 1, 256 threads).
+template <int PASS>
+__global__ void __launch_bounds__(TC_THREADS, 1) tc_gemm_pkernel(TcArgs g, int ntx, int nty, int nframes) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_empty[TC_STAGES], bar_accf[2], bar_acce[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ __align__(16) float4 colterm[TC_N];  // pass 2: (cx, ux, q, r) of the tile's columns
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nkb = g.nkb, nruns = (nkb + TC_RUN - 1) / TC_RUN;
+    const int T = ntx * nty * nframes;
+    const int my_tiles = (int)blockIdx.x < T ? (T - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+
+    if (tid == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(smem_u32(&bar_full[s]), 1);
+            mbar_init(smem_u32(&bar_empty[s]), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(smem_u32(&bar_accf[a]), 1);
+            mbar_init(smem_u32(&bar_acce[a]), 8);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 9) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    bool ok = true;
+
+    if (warp == 8) {
+        // ---------------- producer: panels of every tile of this CTA -> shared-memory ring ----------------
+        if (lane == 0) {
+            long q = 0;  // K blocks issued by this CTA
+            for (int i = 0; i < my_tiles && ok; ++i) {
+                const int t = (int)blockIdx.x + i * (int)gridDim.x;
+                const int nt = t % ntx, mt = (t / ntx) % nty, f = t / (ntx * nty);
+                const unsigned char* Ab = g.Ap + (long)f * g.a_frame + (long)mt * nkb * TC_A_BYTES;
+                const unsigned char* Bb = g.Bp + (long)f * g.b_frame + (long)nt * nkb * TC_B_BYTES;
+                for (int kb = 0; kb < nkb; ++kb, ++q) {
+                    const int s = (int)(q & (TC_STAGES - 1));
+                    const long u = q / TC_STAGES;
+                    if (u > 0 && !mbar_wait(smem_u32(&bar_empty[s]), (uint32_t)((u - 1) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t full = smem_u32(&bar_full[s]);
+                    const uint32_t dst = smem_u32(smem + s * TC_STAGE);
+                    mbar_expect_tx(full, TC_STAGE);
+                    bulk_g2s(dst, Ab + (long)kb * TC_A_BYTES, TC_A_BYTES, full);
+                    bulk_g2s(dst + TC_A_BYTES, Bb + (long)kb * TC_B_BYTES, TC_B_BYTES, full);
+                }
+            }
+            if (!ok) {
+                // let the copies in flight land before the CTA can leave
+                for (long k = q - TC_STAGES > 0 ? q - TC_STAGES : 0; k < q; ++k)
+                    mbar_wait(smem_u32(&bar_full[k & (TC_STAGES - 1)]), (uint32_t)((k / TC_STAGES) & 1));
+            }
+        }
+    } else if (warp == 9) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            long q = 0, issued = 0, rbase = 0;
+            for (int i = 0; i < my_tiles && ok; ++i, rbase += nruns) {
+                for (int kb = 0; kb < nkb; ++kb, ++q) {
+                    const int s = (int)(q & (TC_STAGES - 1));
+                    const long u = q / TC_STAGES;
+                    const long r = rbase + kb / TC_RUN;
+                    const int a = (int)(r & 1);
+                    const bool first = kb % TC_RUN == 0;
+                    // the accumulator of run r was last used by run r - 2: wait for its drain
+                    if (first && r >= 2 && !mbar_wait(smem_u32(&bar_acce[a]), (uint32_t)(((r >> 1) - 1) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    if (!mbar_wait(smem_u32(&bar_full[s]), (uint32_t)(u & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = smem_u32(smem + s * TC_STAGE);
+                    const uint32_t ahi = base, alo = base + TC_A_PANEL;
+                    const uint32_t bhi = base + TC_A_BYTES, blo = base + TC_A_BYTES + TC_B_PANEL;
+                    const uint32_t d = tmem + (uint32_t)(a * TC_N);
+#pragma unroll
+                    for (int ks = 0; ks < TC_BK / 8; ++ks) {
+                        const uint32_t ao = (uint32_t)(2 * ks * (TC_M / 8)) << 7;
+                        const uint32_t bo = (uint32_t)(2 * ks * (TC_N / 8)) << 7;
+                        const uint64_t dah = umma_desc(ahi + ao, (TC_M / 8) << 7, 128);
+                        const uint64_t dal = umma_desc(alo + ao, (TC_M / 8) << 7, 128);
+                        const uint64_t dbh = umma_desc(bhi + bo, (TC_N / 8) << 7, 128);
+                        const uint64_t dbl = umma_desc(blo + bo, (TC_N / 8) << 7, 128);
+                        tc_mma(d, dah, dbh, (first && ks == 0) ? 0u : 1u);
+                        tc_mma(d, dah, dbl, 1u);
+                        tc_mma(d, dal, dbh, 1u);
+                    }
+                    tc_commit(smem_u32(&bar_empty[s]));  // the stage can be refilled
+                    if (kb % TC_RUN == TC_RUN - 1 || kb == nkb - 1) tc_commit(smem_u32(&bar_accf[a]));
+                    issued = q + 1;
+                }
+            }
+            if (!ok && issued > 0) {
+                // the MMAs in flight must finish before the TMEM is released
+                const long k = issued - 1;
+                mbar_wait(smem_u32(&bar_empty[k & (TC_STAGES - 1)]), (uint32_t)((k / TC_STAGES) & 1));
+            }
+        }
+    } else {
+        // ---------------- drain warps: runs into FP32 registers, then the tile's epilogue ----------------
+        // Every drain thread runs the same number of iterations and reaches both named barriers of
+        // every tile, also after a wait gave up (it then skips the waits and stores), so the
+        // barriers cannot wait for a thread that left.
+        float racc[128];  // rows 32 (w % 4) + lane, columns (w / 4) * 128 .. +127
+        const uint32_t tq = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 128);
+        long R = 0;
+        for (int i = 0; i < my_tiles; ++i) {
+            const int t = (int)blockIdx.x + i * (int)gridDim.x;
+            const int nt = t % ntx, mt = (t / ntx) % nty, f = t / (ntx * nty);
+            const int m0 = mt * TC_M, n0 = nt * TC_N;
+#pragma unroll
+            for (int j = 0; j < 128; ++j) racc[j] = 0.f;
+            for (int rk = 0; rk < nruns; ++rk, ++R) {
+                if (!ok) continue;
+                const int a = (int)(R & 1);
+                const bool got =
+                    __all_sync(0xffffffffu, mbar_wait(smem_u32(&bar_accf[a]), (uint32_t)((R >> 1) & 1)));
+                if (!got) {
+                    ok = false;
+                    continue;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    float v[16];
+                    tmem_ld16(tq + (uint32_t)(a * TC_N + 16 * c), v);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) racc[16 * c + j] += v[j];
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&bar_acce[a]));
+            }
+            if (PASS == 2) {
+                // the tile's per-column terms, once every drain thread is done with the last tile's
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+                const float* vec = g.vec + (long)f * (2L * g.HM + 2L * g.WM + 1);
+                const int n = n0 + tid;
+                colterm[tid] = n < g.Nc ? make_float4(g.cx[n], g.ux[n], vec[2 * g.HM + n], vec[2 * g.HM + g.WM + n])
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+            }
+            if (!ok) continue;
+            const int row = m0 + 32 * (warp & 3) + lane;
+            const int cb = (warp >> 2) * 128;
+            if (PASS == 1) {
+                if (row < g.Mr) {
+                    unsigned char* P = g.Cp + (long)f * g.c_frame +
+                                       ((long)nt * (g.Mr / TC_BK) + row / TC_BK) * TC_B_BYTES;
+                    const int k = row % TC_BK;
+#pragma unroll
+                    for (int j = 0; j < 128; ++j) {
+                        const int rr = cb + j;
+                        if (n0 + rr >= g.Nc) break;
+                        const uint32_t off = panel_off(TC_N, rr, k >> 2) + ((k & 3) << 2);
+                        const float hi = tf32_rna(racc[j]);
+                        *reinterpret_cast<float*>(P + off) = hi;
+                        *reinterpret_cast<float*>(P + TC_B_PANEL + off) = tf32_rna(racc[j] - hi);
+                    }
+                }
+            } else if (row < g.Mr) {
+                const float* vec = g.vec + (long)f * (2L * g.HM + 2L * g.WM + 1);
+                const float pm = vec[row], tm = vec[g.HM + row];
+                const float cym = g.cy[row], uym = g.uy[row];
+                const float cback = vec[2 * g.HM + 2 * g.WM] * g.cscale;
+                float* out = g.C + (long)f * g.Mr * g.Nc + (long)row * g.Nc + n0 + cb;
+                const bool full = g.v8 && n0 + cb + 128 <= g.Nc;
+#pragma unroll
+                for (int qq = 0; qq < 16; ++qq) {
+                    float o[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const float4 ct = colterm[cb + 8 * qq + k];  // broadcast
+                        o[k] = racc[8 * qq + k] + pm * ct.x + cym * ct.z - uym * ct.w - tm * ct.y + cback;
+                    }
+                    if (full) {
+                        asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(out + 8 * qq),
+                                     "f"(o[0]), "f"(o[1]), "f"(o[2]), "f"(o[3]), "f"(o[4]), "f"(o[5]), "f"(o[6]),
+                                     "f"(o[7])
+                                     : "memory");
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k)
+                            if (n0 + cb + 8 * qq + k < g.Nc) out[8 * qq + k] = o[k];
+                    }
+                }
+            }
+        }
+    }
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!all_ok && tid == 0 && g.err) atomicExch(g.err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 9) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+    }
+}
+
 // Padded frame minus its mean, split into pass 1's A panels [f][mt][kb].  One thread per 16-byte
 // chunk; consecutive threads take consecutive rows of one chunk column (coalesced panel writes).
 __global__ void __launch_bounds__(256) x_split_kernel(const void* __restrict__ raw, int is_u16, int w, int h,
@@ -422,8 +643,17 @@ cudaError_t set_tc_smem() {
     if (bit && (done & bit)) return cudaSuccess;
     e = cudaFuncSetAttribute(tc_gemm_kernel<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TC_SMEM_BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc_gemm_pkernel<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TC_SMEM_BYTES);
     if (e == cudaSuccess) done |= bit;
     return e;
+}
+
+// ESRRF_TC_GEMM=tile selects one CTA per tile (the form before the persistent one; kept for A/B).
+bool tc_persistent() {
+    const char* s = std::getenv("ESRRF_TC_GEMM");
+    return !(s && std::strcmp(s, "tile") == 0);
 }
 
 // Host form of cvt.rna.tf32.f32 for finite values: round to nearest, ties away from zero, at the
@@ -539,7 +769,16 @@ cudaError_t tc_interp_passes(const InterpPlan& p, InterpScratch& sc, const void*
     g.b_frame = 0;
     g.Cp = reinterpret_cast<unsigned char*>(sc.rowT);
     g.c_frame = rowT_frame;
-    tc_gemm_kernel<1><<<dim3(ntiles, N / TC_M, F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g);
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    const bool pers = tc_persistent();
+    const int sms = sm_count(dev);
+    auto pgrid = [&](int tiles) { return (unsigned)std::max(1, std::min(tiles, sms)); };
+    if (pers)
+        tc_gemm_pkernel<1><<<pgrid(ntiles * (N / TC_M) * F), TC_THREADS, TC_SMEM_BYTES, stream>>>(
+            g, ntiles, N / TC_M, F);
+    else
+        tc_gemm_kernel<1><<<dim3(ntiles, N / TC_M, F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g);
     // pass 2: Dy times the first-pass rows, plus the rank-one terms
     g.Mr = p.HM;
     g.Nc = p.WM;
@@ -550,7 +789,11 @@ cudaError_t tc_interp_passes(const InterpPlan& p, InterpScratch& sc, const void*
     g.b_frame = rowT_frame;
     g.C = out;
     g.v8 = (p.WM % 8 == 0 && reinterpret_cast<uintptr_t>(out) % 32 == 0) ? 1 : 0;
-    tc_gemm_kernel<2><<<dim3(ntiles, (p.HM + TC_M - 1) / TC_M, F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g);
+    const int mtiles = (p.HM + TC_M - 1) / TC_M;
+    if (pers)
+        tc_gemm_pkernel<2><<<pgrid(ntiles * mtiles * F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g, ntiles, mtiles, F);
+    else
+        tc_gemm_kernel<2><<<dim3(ntiles, mtiles, F), TC_THREADS, TC_SMEM_BYTES, stream>>>(g);
     return cudaGetLastError();
 }
 
