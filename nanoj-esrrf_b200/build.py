@@ -8,6 +8,7 @@ import glob
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -74,15 +75,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
         cmd = [NVCC, *ARCH, *FLAGS, "-I", INCLUDE, "-c", src, "-o", obj + ".tmp"]
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        procs.append((src, obj, time.time(), subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
     failed = False
-    for src, obj, p in procs:
+    for src, obj, t_start, p in procs:
         out, _ = p.communicate()
         if p.returncode != 0 or verbose:
             sys.stderr.write(out.decode())
         failed |= p.returncode != 0
         if p.returncode == 0:
             os.replace(obj + ".tmp", obj)
+            # stamp the object with the time its compile started, so a source edited while it
+            # compiled is seen as newer on the next build
+            os.utime(obj, (t_start, t_start))
     if failed:
         raise RuntimeError("nvcc failed")
     tmp = LIB + ".tmp"

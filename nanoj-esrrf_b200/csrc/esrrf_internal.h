@@ -157,6 +157,7 @@ struct FhtDriftFrame {
     float wsum_int;     // sum of w over the disc, (j, i) order
     float fx, fy;       // frac(sx), frac(sy)
     int zero;           // 1: sx == sy == 0 (the interpolated pixel is the intensity)
+    float sx, sy;       // the shift itself (magnified pixels)
 };
 struct FhtDriftTables {
     int capacity = 0, S = 0;

@@ -33,10 +33,12 @@ constexpr int kTYT = 8;          // thread rows per CTA
 constexpr int kK = 8;            // outputs per thread (vertical)
 constexpr int kTH = kTYT * kK;   // output rows per CTA
 
-// Shared-memory layout for a tap box of side S (S = r1 - r0 + 1, always even).
-template <int S>
+// Shared-memory layout for a tap box of side S (S = r1 - r0 + 1, always even).  PAD = 1 (launches
+// with drift) adds a column and a row to the tiles: the reference's box of a pixel whose centre
+// rounds across an integer starts one source column or row further (see the kernel).
+template <int S, int PAD = 0>
 struct FusedLayout {
-    static constexpr int EW = kTX + S - 1, EH = kTH + S - 1;  // unit-gradient tile
+    static constexpr int EW = kTX + S - 1 + PAD, EH = kTH + S - 1 + PAD;  // unit-gradient tile
     static constexpr int IW = EW + 2, IH = EH + 2;            // intensity tile (+1 px margin)
     static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
     static constexpr size_t off_E = 0;
@@ -69,6 +71,7 @@ struct DriftParams {
     const int* jr;            // [F][2S] disc chord per column
     const double* pre;        // [F][S+1][S+1] 2-D prefix sums of w
     const float* v;           // [F][H][W] intensity at the shifted position
+    float tSS, tSO;           // the per-tap arithmetic of pixels whose box is moved
 };
 
 // One column offset i of the tap box for a thread's 8 outputs: source rows rr = 0 .. S+6 of the
@@ -83,11 +86,10 @@ struct DriftParams {
 // reciprocal, whose error only moves the threshold within rounding.  The two tests can disagree only
 // where g . (dx, dy) is within rounding of 0, where |g x (dx, dy)| = d and the contribution
 // w - (w / d) |g x (dx, dy)| vanishes quadratically.
-template <int S, bool CHECK>
+template <int S, int EW, bool CHECK>
 __device__ __forceinline__ void tap_column(const float2* __restrict__ col, float fi, float fr0, int lo,
                                            int hi, const float (&w)[S], const float (&wd)[S],
                                            float (&acc)[kK]) {
-    constexpr int EW = FusedLayout<S>::EW;
 #pragma unroll
     for (int rr = 0; rr < S + kK - 1; ++rr) {
         if (CHECK && (rr < lo || rr > hi)) continue;
@@ -113,10 +115,9 @@ __device__ __forceinline__ void tap_column(const float2* __restrict__ col, float
 
 // A column whose disc chord is the compile-time tap-row range [LO, HI]: only the chord's taps
 // are evaluated (rows LO .. HI + 7, and per row only the outputs whose tap row is in the chord).
-template <int S, int LO, int HI>
+template <int S, int EW, int LO, int HI>
 __device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float fi, float fr0,
                                           const float (&w)[S], const float (&wd)[S], float (&acc)[kK]) {
-    constexpr int EW = FusedLayout<S>::EW;
 #pragma unroll
     for (int rr = LO; rr <= HI + kK - 1; ++rr) {
         const float2 e = col[rr * EW];
@@ -141,40 +142,42 @@ __device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float 
 // Without drift the disc is symmetric in j, so a column's chord inside the box [-R, R+1] is
 // either the whole box or the rows -J .. J, i.e. tap rows [LO, S - 2 - LO]: one instantiation per
 // LO.  With drift the disc's centre sits at frac(sy) in [0, 1) of the box's row 0, so a chord
-// [lo, hi] that does not fill the box has lo + hi in {S - 2, S - 1, S} (D = 0, 1, 2 below).  Any
-// other range takes the generic row-checked loop.
-template <int S, int LO, int D>
-__device__ __forceinline__ void tap_dispatch(const float2* __restrict__ col, float fi, float fr0, int lo,
-                                             int hi, const float (&w)[S], const float (&wd)[S],
+// [lo, hi] that does not fill the box has lo + hi in {S - 2, S - 1, S}: key = 3 lo + (lo + hi -
+// S + 2) indexes the instantiations, found by a binary search over the key (about five compares
+// per column instead of a chain of up to 3 S / 2).  Any other range takes the generic
+// row-checked loop.
+template <int S, int EW, int A, int B>
+__device__ __forceinline__ bool tap_dispatch(const float2* __restrict__ col, float fi, float fr0, int key,
+                                             int lo, int hi, const float (&w)[S], const float (&wd)[S],
                                              float (&acc)[kK]) {
-    constexpr int HI = S - 2 - LO + D;
-    if constexpr (LO <= HI && HI <= S - 1) {
-        if (lo == LO && hi == HI) {
-            tap_chord<S, LO, HI>(col, fi, fr0, w, wd, acc);
-            return;
+    if constexpr (B - A == 1) {
+        constexpr int LO = A / 3, HI = S - 2 - LO + A % 3;
+        if constexpr (LO <= HI && HI <= S - 1) {
+            if (lo == LO && hi == HI) {
+                tap_chord<S, EW, LO, HI>(col, fi, fr0, w, wd, acc);
+                return true;
+            }
         }
-    }
-    if constexpr (D > 0) {
-        tap_dispatch<S, LO, D - 1>(col, fi, fr0, lo, hi, w, wd, acc);
-    } else if constexpr (LO < S / 2) {
-        tap_dispatch<S, LO + 1, 2>(col, fi, fr0, lo, hi, w, wd, acc);
+        return false;  // the caller takes the generic loop
     } else {
-        tap_column<S, true>(col, fi, fr0, lo, hi + kK - 1, w, wd, acc);
+        constexpr int MID = (A + B) / 2;
+        if (key < MID) return tap_dispatch<S, EW, A, MID>(col, fi, fr0, key, lo, hi, w, wd, acc);
+        return tap_dispatch<S, EW, MID, B>(col, fi, fr0, key, lo, hi, w, wd, acc);
     }
 }
 
-template <int S, int LO>
+template <int S, int EW, int LO>
 __device__ __forceinline__ void tap_dispatch_sym(const float2* __restrict__ col, float fi, float fr0, int lo,
                                                  int hi, const float (&w)[S], const float (&wd)[S],
                                                  float (&acc)[kK]) {
     if constexpr (LO <= (S - 2) / 2) {
         if (lo == LO && hi == S - 2 - LO) {
-            tap_chord<S, LO, S - 2 - LO>(col, fi, fr0, w, wd, acc);
+            tap_chord<S, EW, LO, S - 2 - LO>(col, fi, fr0, w, wd, acc);
             return;
         }
-        tap_dispatch_sym<S, LO + 1>(col, fi, fr0, lo, hi, w, wd, acc);
+        tap_dispatch_sym<S, EW, LO + 1>(col, fi, fr0, lo, hi, w, wd, acc);
     } else {
-        tap_column<S, true>(col, fi, fr0, lo, hi + kK - 1, w, wd, acc);
+        tap_column<S, EW, true>(col, fi, fr0, lo, hi + kK - 1, w, wd, acc);
     }
 }
 
@@ -204,7 +207,7 @@ __device__ __forceinline__ float drift_wsum(const FhtDriftFrame& d, const double
 // compiles the frame loop and the fold without the group bookkeeping.
 template <int S, bool GROUPED, bool DRIFT>
 __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, FusedParams fp, DriftParams dp) {
-    using L = FusedLayout<S>;
+    using L = FusedLayout<S, DRIFT ? 1 : 0>;
     constexpr int EW = L::EW, EH = L::EH, IW = L::IW, IH = L::IH;
     constexpr int r0c = -(S - 2) / 2;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -360,16 +363,56 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             }
             const float2* col = sE + (ty * kK) * EW + tx + ii;
             if (lo == 0 && hi == S - 1)
-                tap_chord<S, 0, S - 1>(col, fi, fj0, w, wd, acc);
-            else if constexpr (DRIFT)
-                tap_dispatch<S, 0, 2>(col, fi, fj0, lo, hi, w, wd, acc);
+                tap_chord<S, EW, 0, S - 1>(col, fi, fj0, w, wd, acc);
+            else if constexpr (DRIFT) {
+                const int key = min(max(3 * lo + lo + hi - S + 2, 0), 3 * (S / 2 + 1) - 1);
+                if (!tap_dispatch<S, EW, 0, 3 * (S / 2 + 1)>(col, fi, fj0, key, lo, hi, w, wd, acc))
+                    tap_column<S, EW, true>(col, fi, fj0, lo, hi + kK - 1, w, wd, acc);
+            }
             else
-                tap_dispatch_sym<S, 0>(col, fi, fj0, lo, hi, w, wd, acc);
+                tap_dispatch_sym<S, EW, 0>(col, fi, fj0, lo, hi, w, wd, acc);
         }
         if constexpr (DRIFT) {
             const double* pre = dp.pre + (long)f * (S + 1) * (S + 1);
 #pragma unroll
             for (int k = 0; k < kK; ++k) wsum[k] = drift_wsum<S>(df, pre, xM, y0 + ty * kK + k, r0c, W, H);
+            // The reference's box of pixel (xM, yM) starts at (int)(xc - 0.5) with
+            // xc = (float)(xM + 0.5 + sx) (liveSRRF_noInterpolation.cl:264-281): one column (row)
+            // further than the table's floor(sx) where the float rounding of xc reaches the next
+            // integer or the truncation of a negative xc - 0.5 goes towards zero.  Such pixels are
+            // evaluated here with the reference's per-tap arithmetic on the staged unit gradients
+            // (the tiles carry the extra column and row).
+            const float xc = (float)((double)xM + 0.5 + (double)df.sx);
+            const int bx = (int)((double)xc - 0.5);
+#pragma unroll
+            for (int k = 0; k < kK; ++k) {
+                const int yM = y0 + ty * kK + k;
+                const float yc = (float)((double)yM + 0.5 + (double)df.sy);
+                const int by = (int)((double)yc - 0.5);
+                if ((bx == xM + df.ix && by == yM + df.iy) || xM >= W || yM >= H) continue;
+                float cg = 0.f, ws = 0.f;
+                for (int j = r0c; j <= r0c + S - 1; ++j) {
+                    const float vy = (float)((double)((float)by + (float)j) + 0.5);
+                    if (!(vy > 0 && vy < (float)H)) continue;
+                    const int ey = by + j - (gY0 + 1);
+                    for (int i = r0c; i <= r0c + S - 1; ++i) {
+                        const float vx = (float)((double)((float)bx + (float)i) + 0.5);
+                        if (!(vx > 0 && vx < (float)W)) continue;
+                        const float dx = vx - xc, dy = vy - yc;
+                        const float d = sqrtf(dx * dx + dy * dy);
+                        if (!(d != 0.f && d <= dp.tSO)) continue;
+                        float w = d * expf(-(d * d) / dp.tSS);
+                        w = w * w * w * w;
+                        ws += w;
+                        const int ex = bx + i - (gX0 + 1);
+                        if (ex < 0 || ex >= EW || ey < 0 || ey >= EH) continue;  // outside the tile: no gradient
+                        const float2 g = sE[ey * EW + ex];
+                        if (g.x * dx + g.y * dy < 0.f) cg += w - (w / d) * fabsf(g.y * dx - g.x * dy);
+                    }
+                }
+                acc[k] = cg;
+                wsum[k] = ws;
+            }
         }
         // 4. normalisation, sensitivity, intensity weighting and cumulants
         if (emit) {
@@ -431,7 +474,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
 template <int S, bool DRIFT>
 cudaError_t launch_fused(int r0, float sens, const FusedParams& fp_in, const DriftParams& dp,
                          const FhtRgcArgs& a, cudaStream_t stream) {
-    constexpr size_t bytes = FusedLayout<S>::bytes;
+    constexpr size_t bytes = FusedLayout<S, DRIFT ? 1 : 0>::bytes;
     // The opt-in shared-memory size is a per-device function attribute: set it once per device
     // (also keeps the call out of CUDA-graph captures after the first, uncaptured launch).
     static unsigned long long configured = 0;

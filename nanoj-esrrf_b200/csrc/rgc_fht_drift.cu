@@ -12,11 +12,10 @@
 //
 // Residual against the reference's per-pixel arithmetic: the reference rounds xc to float per
 // pixel, so its centre offsets carry a rounding error of up to half an ulp of xM (6e-5 magnified
-// pixels below 2048); the tables use the exact fraction of the shift.  Where the rounding moves
-// (int)(xc - 0.5) by one (a fraction within rounding of 0 or 1, or truncation towards zero left of
-// the image), the reference's box differs from the table's only in its outermost column or row,
-// at distance > R + 1 from the centre, whose weight (d exp(-d^2/tSS))^4 is below 1e-7 of the
-// largest tap weight.
+// pixels below 2048); the tables use the exact fraction of the shift.  Where that rounding (a
+// fraction within rounding of 1) or the truncation of (int)(xc - 0.5) towards zero (left of or
+// above the image) moves a pixel's box by one source column or row, the tile kernel evaluates that
+// pixel with the reference's own per-tap arithmetic instead of the tables (see fht_fused.cuh).
 #include <math.h>
 
 #include "device_common.cuh"
@@ -99,6 +98,8 @@ __global__ void __launch_bounds__(256) drift_tables_kernel(const float* __restri
         d.fx = (float)fxd;
         d.fy = (float)fyd;
         d.zero = sxf == 0.f && syf == 0.f;
+        d.sx = sxf;
+        d.sy = syf;
         t.fr[f] = d;
     }
 }
@@ -172,7 +173,7 @@ cudaError_t fht_rgc_fused_drift(const FhtGeometry& g, const FhtDriftTables& t, c
                                 cudaStream_t stream) {
     if (a.F > t.capacity || g.S > t.S) return cudaErrorInvalidValue;
     const fused::FusedParams fp{g.r0, g.sensitivity, nullptr, nullptr, nullptr, nullptr};
-    const fused::DriftParams dp{t.fr, t.wt, t.jr, t.pre, t.v};
+    const fused::DriftParams dp{t.fr, t.wt, t.jr, t.pre, t.v, g.tSS, g.tSO};
     // tap boxes of 22 .. 32 are instantiated in rgc_fht_drift_wide.cu (compiled in parallel)
     if (g.S >= 22) return fht_rgc_fused_drift_wide(g.S, fp, dp, a, stream);
     return fused::launch_fused_in<true, 4, 20>(g.S, g.r0, g.sensitivity, fp, dp, a, stream);
