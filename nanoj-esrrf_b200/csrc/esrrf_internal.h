@@ -162,7 +162,7 @@ struct FhtDriftFrame {
 struct FhtDriftTables {
     int capacity = 0, S = 0;
     FhtDriftFrame* fr = nullptr;  // [F]
-    float2* wt = nullptr;         // [F][S][S] (w, w/d), [ii][jj]
+    float2* wt = nullptr;         // [F][S][S] (w, w/d), [ii][jj - lo_ii]: each column from its chord's first row
     int* jr = nullptr;            // [F][2S] per column: first and last tap row of the disc
     double* pre = nullptr;        // [F][S+1][S+1] prefix sums: pre[jj][ii] = sum over rows < jj, cols < ii
     float* v = nullptr;           // [F][H][W] intensity at the shifted position

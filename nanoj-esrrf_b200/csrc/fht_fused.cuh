@@ -141,28 +141,21 @@ __device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float 
 
 // Without drift the disc is symmetric in j, so a column's chord inside the box [-R, R+1] is
 // either the whole box or the rows -J .. J, i.e. tap rows [LO, S - 2 - LO]: one instantiation per
-// LO.  With drift the disc's centre sits at frac(sy) in [0, 1) of the box's row 0, so a chord
-// [lo, hi] that does not fill the box has lo + hi in {S - 2, S - 1, S}: key = 3 lo + (lo + hi -
-// S + 2) indexes the instantiations, found by a binary search over the key (about five compares
-// per column instead of a chain of up to 3 S / 2).  Any other range takes the generic
-// row-checked loop.
+// LO.  With drift the chords are not symmetric; a column's weights are stored from its chord's
+// first row on, so the chord runs as tap rows [0, L - 1] of a column and row origin moved down by
+// lo: one instantiation per chord length L, found by a binary search over L (about five compares
+// per column).
 template <int S, int EW, int A, int B>
-__device__ __forceinline__ bool tap_dispatch(const float2* __restrict__ col, float fi, float fr0, int key,
-                                             int lo, int hi, const float (&w)[S], const float (&wd)[S],
-                                             float (&acc)[kK]) {
+__device__ __forceinline__ void tap_length(const float2* __restrict__ col, float fi, float fr0, int L,
+                                           const float (&w)[S], const float (&wd)[S], float (&acc)[kK]) {
     if constexpr (B - A == 1) {
-        constexpr int LO = A / 3, HI = S - 2 - LO + A % 3;
-        if constexpr (LO <= HI && HI <= S - 1) {
-            if (lo == LO && hi == HI) {
-                tap_chord<S, EW, LO, HI>(col, fi, fr0, w, wd, acc);
-                return true;
-            }
-        }
-        return false;  // the caller takes the generic loop
+        tap_chord<S, EW, 0, A - 1>(col, fi, fr0, w, wd, acc);
     } else {
         constexpr int MID = (A + B) / 2;
-        if (key < MID) return tap_dispatch<S, EW, A, MID>(col, fi, fr0, key, lo, hi, w, wd, acc);
-        return tap_dispatch<S, EW, MID, B>(col, fi, fr0, key, lo, hi, w, wd, acc);
+        if (L < MID)
+            tap_length<S, EW, A, MID>(col, fi, fr0, L, w, wd, acc);
+        else
+            tap_length<S, EW, MID, B>(col, fi, fr0, L, w, wd, acc);
     }
 }
 
@@ -362,15 +355,14 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
                 wd[2 * q + 1] = v.w;
             }
             const float2* col = sE + (ty * kK) * EW + tx + ii;
-            if (lo == 0 && hi == S - 1)
+            if constexpr (DRIFT) {
+                // weights stored from the chord's first row: rows lo .. hi as 0 .. L - 1
+                tap_length<S, EW, 1, S + 1>(col + lo * EW, fi, fj0 + (float)lo, min(hi - lo + 1, S), w, wd, acc);
+            } else if (lo == 0 && hi == S - 1) {
                 tap_chord<S, EW, 0, S - 1>(col, fi, fj0, w, wd, acc);
-            else if constexpr (DRIFT) {
-                const int key = min(max(3 * lo + lo + hi - S + 2, 0), 3 * (S / 2 + 1) - 1);
-                if (!tap_dispatch<S, EW, 0, 3 * (S / 2 + 1)>(col, fi, fj0, key, lo, hi, w, wd, acc))
-                    tap_column<S, EW, true>(col, fi, fj0, lo, hi + kK - 1, w, wd, acc);
-            }
-            else
+            } else {
                 tap_dispatch_sym<S, EW, 0>(col, fi, fj0, lo, hi, w, wd, acc);
+            }
         }
         if constexpr (DRIFT) {
             const double* pre = dp.pre + (long)f * (S + 1) * (S + 1);

@@ -32,7 +32,9 @@ __global__ void __launch_bounds__(256) drift_tables_kernel(const float* __restri
                                                            const float* __restrict__ syp, int r0, int S,
                                                            float tSS, float tSO, FhtDriftTables t) {
     __shared__ float sw[32 * 32];            // [jj][ii] weights
+    __shared__ float swd[32 * 32];           // [jj][ii] weight / distance
     __shared__ unsigned char sin_[32 * 32];  // [jj][ii] 1: tap inside the disc
+    __shared__ int slo[32], shi[32];         // per column: first and last tap row of the disc
     __shared__ double spre[33 * 33];         // [jj][ii] prefix sums
     const int f = blockIdx.x, tid = threadIdx.x;
     const float sxf = sxp[f], syf = syp[f];
@@ -50,20 +52,29 @@ __global__ void __launch_bounds__(256) drift_tables_kernel(const float* __restri
             w = __fmul_rn(__fmul_rn(__fmul_rn(w, w), w), w);
             wd = w / d;
         }
-        t.wt[(long)f * S * S + idx] = make_float2(w, wd);
         sw[jj * S + ii] = w;
+        swd[jj * S + ii] = wd;
         sin_[jj * S + ii] = in ? 1 : 0;
     }
     __syncthreads();
-    if (tid < S) {  // column tid: its disc chord
+    if (tid < S) {  // column tid: its disc chord (a disc meets a column in one run of rows)
         int lo = S, hi = -1;
         for (int jj = 0; jj < S; ++jj)
             if (sin_[jj * S + tid]) {
                 lo = min(lo, jj);
                 hi = max(hi, jj);
             }
+        slo[tid] = lo;
+        shi[tid] = hi;
         t.jr[(long)f * 2 * S + 2 * tid] = lo;
         t.jr[(long)f * 2 * S + 2 * tid + 1] = hi;
+    }
+    __syncthreads();
+    // weights of column ii from its chord's first row on: entry jj' holds tap row lo + jj'
+    for (int idx = tid; idx < S * S; idx += blockDim.x) {
+        const int ii = idx / S, jq = idx - ii * S, jj = slo[ii] + jq;
+        t.wt[(long)f * S * S + idx] = jj <= shi[ii] ? make_float2(sw[jj * S + ii], swd[jj * S + ii])
+                                                    : make_float2(0.f, 0.f);
     }
     const int P = S + 1;
     if (tid <= S) {  // row prefix sums: spre[jj + 1][ii + 1] = sum of row jj up to column ii
