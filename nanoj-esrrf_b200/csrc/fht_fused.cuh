@@ -371,36 +371,42 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             // The reference's box of pixel (xM, yM) starts at (int)(xc - 0.5) with
             // xc = (float)(xM + 0.5 + sx) (liveSRRF_noInterpolation.cl:264-281): one column (row)
             // further than the table's floor(sx) where the float rounding of xc reaches the next
-            // integer or the truncation of a negative xc - 0.5 goes towards zero.  Such pixels are
-            // evaluated here with the reference's per-tap arithmetic on the staged unit gradients
-            // (the tiles carry the extra column and row).
+            // integer or the truncation of a negative xc - 0.5 goes towards zero.  The offsets of
+            // the taps the two boxes share agree (to the rounding of xc), so such a pixel's sums
+            // are corrected by its box's moved edges only: the taps of the table's first column
+            // (row) leave, those of column (row) S come in (the tiles carry that column and row).
             const float xc = (float)((double)xM + 0.5 + (double)df.sx);
-            const int bx = (int)((double)xc - 0.5);
+            const int mx = (int)((double)xc - 0.5) - (xM + df.ix);
 #pragma unroll
             for (int k = 0; k < kK; ++k) {
                 const int yM = y0 + ty * kK + k;
                 const float yc = (float)((double)yM + 0.5 + (double)df.sy);
-                const int by = (int)((double)yc - 0.5);
-                if ((bx == xM + df.ix && by == yM + df.iy) || xM >= W || yM >= H) continue;
-                float cg = 0.f, ws = 0.f;
-                for (int j = r0c; j <= r0c + S - 1; ++j) {
-                    const float vy = (float)((double)((float)by + (float)j) + 0.5);
-                    if (!(vy > 0 && vy < (float)H)) continue;
-                    const int ey = by + j - (gY0 + 1);
-                    for (int i = r0c; i <= r0c + S - 1; ++i) {
-                        const float vx = (float)((double)((float)bx + (float)i) + 0.5);
-                        if (!(vx > 0 && vx < (float)W)) continue;
-                        const float dx = vx - xc, dy = vy - yc;
-                        const float d = sqrtf(dx * dx + dy * dy);
-                        if (!(d != 0.f && d <= dp.tSO)) continue;
-                        float w = d * expf(-(d * d) / dp.tSS);
-                        w = w * w * w * w;
-                        ws += w;
-                        const int ex = bx + i - (gX0 + 1);
-                        if (ex < 0 || ex >= EW || ey < 0 || ey >= EH) continue;  // outside the tile: no gradient
-                        const float2 g = sE[ey * EW + ex];
-                        if (g.x * dx + g.y * dy < 0.f) cg += w - (w / d) * fabsf(g.y * dx - g.x * dy);
-                    }
+                const int my = (int)((double)yc - 0.5) - (yM + df.iy);
+                if ((mx == 0 && my == 0) || mx < 0 || mx > 1 || my < 0 || my > 1 || xM >= W || yM >= H) continue;
+                const int bx = xM + df.ix + r0c, by = yM + df.iy + r0c;  // source of table tap (0, 0)
+                float cg = acc[k], ws = wsum[k];
+                // tap (ii, jj) of the table's geometry, added (sign +1) or removed (-1)
+                auto edge = [&](int ii, int jj, float sign) {
+                    const int X = bx + ii, Y = by + jj;
+                    if (X < 0 || X >= W || Y < 0 || Y >= H) return;
+                    // the table's arithmetic (drift_tables_kernel): the removed taps cancel exactly
+                    const float dx = (float)((double)(r0c + ii) - (double)df.fx);
+                    const float dy = (float)((double)(r0c + jj) - (double)df.fy);
+                    const float d = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+                    if (!(d != 0.f && d <= dp.tSO)) return;
+                    float w = __fmul_rn(d, expf(-__fmul_rn(d, d) / dp.tSS));
+                    w = __fmul_rn(__fmul_rn(__fmul_rn(w, w), w), w);
+                    ws += sign * w;
+                    const float2 g = sE[(ty * kK + k + jj) * EW + tx + ii];
+                    if (g.x * dx + g.y * dy < 0.f) cg += sign * (w - (w / d) * fabsf(g.y * dx - g.x * dy));
+                };
+                if (mx == 1) {
+                    for (int jj = 0; jj < S; ++jj) edge(0, jj, -1.f);        // first column leaves
+                    for (int jj = my; jj < S + my; ++jj) edge(S, jj, 1.f);   // column S comes in
+                }
+                if (my == 1) {
+                    for (int ii = mx; ii < S; ++ii) edge(ii, 0, -1.f);       // first row leaves
+                    for (int ii = mx; ii < S; ++ii) edge(ii, S, 1.f);        // row S comes in
                 }
                 acc[k] = cg;
                 wsum[k] = ws;
