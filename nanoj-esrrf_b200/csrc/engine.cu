@@ -396,12 +396,13 @@ esrrf_status esrrf_handle::process_chunk(const void* src, bool is_u16, int F_now
         launches += 1;
     } else if (use_fused && d_drift) {
         // frames with drift: per-frame tap tables and shifted intensities, then the fused kernel
-        if (!dtab.fr) CK(fht_drift_tables_alloc(geo.S, F, (long)WM * HM, dtab));
+        // (the kernel samples the shifted intensities from its own tiles: no intensity planes)
+        if (!dtab.fr) CK(fht_drift_tables_alloc(geo.S, F, 0, dtab));
         const int n = p.n_frame_for_srrf;
-        CK(fht_drift_build(geo, d_drift + frame_in_block, d_drift + n + frame_in_block, F_now, d_interp,
-                           WM, HM, dtab, stream));
+        CK(fht_drift_tables_build(geo, d_drift + frame_in_block, d_drift + n + frame_in_block, F_now, dtab,
+                                  stream));
         CK(fht_rgc_fused_drift(geo, dtab, a, stream));
-        launches += 3;
+        launches += 2;
     } else {
         CK(cudaMemcpyAsync(d_shift, sh.data(), sizeof(float) * 2 * F_now, cudaMemcpyHostToDevice, stream));
         CK(fht_robx(d_interp, WM, HM, F_now, d_gx, d_gy, stream));

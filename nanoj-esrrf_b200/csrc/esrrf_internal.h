@@ -151,13 +151,14 @@ int sm_count(int dev);
 // weights over the whole disc in the reference's (j, i) order, the weight tables, each column's
 // disc chord and 2-D prefix sums of the weights (for output pixels whose tap box leaves the
 // image).
-struct FhtDriftFrame {
+struct alignas(16) FhtDriftFrame {  // 48 bytes: copied to shared memory in 16-byte pieces
     int ix, iy;         // floor of the shift
     float fi0, fj0;     // r0 - frac(sx), r0 - frac(sy)
     float wsum_int;     // sum of w over the disc, (j, i) order
     float fx, fy;       // frac(sx), frac(sy)
     int zero;           // 1: sx == sy == 0 (the interpolated pixel is the intensity)
     float sx, sy;       // the shift itself (magnified pixels)
+    int pad[2];
 };
 struct FhtDriftTables {
     int capacity = 0, S = 0;
@@ -170,16 +171,16 @@ struct FhtDriftTables {
 // Buffers for F frames of tap boxes up to S wide and `pixels` output pixels per frame (0: no
 // intensity planes).
 cudaError_t fht_drift_tables_alloc(int S, int F, long pixels, FhtDriftTables& t);
+// Tables of F frames with shifts sx[f], sy[f] (device, magnified pixels).
 cudaError_t fht_drift_tables_build(const FhtGeometry& g, const float* sx, const float* sy, int F,
                                    FhtDriftTables& t, cudaStream_t stream);
+// The intensity of every pixel of F frames at the frame's shift, into v [F][H][W]:
+// getInterpolatedValue(xM + sx, yM + sy) (bicubic, bilinear near the border; the pixel itself for a
+// frame with sx == sy == 0).  The sweep's per-frame mode needs these planes; the engine's launches
+// sample in the tile kernel.
 cudaError_t fht_shift_sample(const float* interp, int W, int H, int F, const float* sx, const float* sy,
                              float* v, cudaStream_t stream);
 void fht_drift_tables_free(FhtDriftTables& t);
-// Tables of F frames with shifts sx[f], sy[f] (device, magnified pixels) and the intensity of
-// each frame at the shifted position: getInterpolatedValue(xM + sx, yM + sy) (bicubic, bilinear
-// near the border; the pixel itself for a frame with sx == sy == 0).
-cudaError_t fht_drift_build(const FhtGeometry& g, const float* sx, const float* sy, int F,
-                            const float* interp, int W, int H, FhtDriftTables& t, cudaStream_t stream);
 // The fused kernel on a launch whose frames have the tables of `t` (built for this launch).
 cudaError_t fht_rgc_fused_drift(const FhtGeometry& g, const FhtDriftTables& t, const FhtRgcArgs& a,
                                 cudaStream_t stream);

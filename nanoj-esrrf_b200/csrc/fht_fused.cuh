@@ -13,9 +13,10 @@
 // (floor(sx), floor(sy)), and the contribution of an inward tap is w - (w/d) |g x (dx, dy)| on
 // the unit gradient g.  Without drift dx = i exactly and the tables are built once.
 //  * DRIFT = false: one table (FusedParams), intensity = the interpolated pixel.
-//  * DRIFT = true: per-frame tables (DriftParams), the source tile at the frame's integer shift,
-//    per-pixel sums of weights from a per-frame 2-D prefix table where the tap box leaves the
-//    image, intensity from a plane sampled at the shifted position (getInterpolatedValue).
+//  * DRIFT = true: per-frame tables (DriftParams, prefetched with the frame's tile), the source
+//    tile at the frame's integer shift, per-pixel sums of weights from a per-frame 2-D prefix table
+//    where the tap box leaves the image, intensity sampled from the tile at the shifted position
+//    (getInterpolatedValue).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -43,15 +44,19 @@ struct FusedLayout {
     static constexpr size_t I_bytes = (sizeof(float) * IW * IH + 15) & ~size_t(15);
     static constexpr size_t off_E = 0;
     static constexpr size_t off_I = off_E + ((sizeof(float2) * EW * EH + 15) & ~size_t(15));
-    static constexpr size_t tail = ((sizeof(float2) * S * S + sizeof(int) * 2 * S + 15) & ~size_t(15)) +
-                                   sizeof(float) * 5 * kTX * kTH;
+    // tap tables: weights [S][S] (w, w/d), chords [2S]; with drift also the frame's record and a
+    // second set (the next frame's tables arrive with its tile)
+    static constexpr size_t wt_bytes = (sizeof(float2) * S * S + 15) & ~size_t(15);
+    static constexpr size_t jr_bytes = (sizeof(int) * 2 * S + 15) & ~size_t(15);
+    static constexpr size_t tab_bytes = wt_bytes + jr_bytes + (PAD ? sizeof(FhtDriftFrame) : 0);
+    static constexpr int nT = PAD ? 2 : 1;
+    static constexpr size_t tail = nT * tab_bytes + sizeof(float) * 5 * kTX * kTH;
     // A second intensity buffer (the next frame's tile prefetched during this frame's taps) is
     // used where two CTAs of 256 threads still fit in an SM's 228 KB of shared memory.
     static constexpr bool kDB = 2 * (off_I + 2 * I_bytes + tail + 1024) <= 228 * 1024;
     static constexpr int nI = kDB ? 2 : 1;
-    static constexpr size_t off_wt = off_I + nI * I_bytes;
-    static constexpr size_t off_jr = off_wt + sizeof(float2) * S * S;
-    static constexpr size_t off_st = (off_jr + sizeof(int) * 2 * S + 15) & ~size_t(15);
+    static constexpr size_t off_wt = off_I + nI * I_bytes;  // table set t at off_wt + t tab_bytes
+    static constexpr size_t off_st = off_wt + nT * tab_bytes;
     static constexpr size_t bytes = off_st + sizeof(float) * 5 * kTX * kTH;
 };
 
@@ -70,7 +75,7 @@ struct DriftParams {
     const float2* wt;         // [F][S][S] (w, w/d), [ii][jj]
     const int* jr;            // [F][2S] disc chord per column
     const double* pre;        // [F][S+1][S+1] 2-D prefix sums of w
-    const float* v;           // [F][H][W] intensity at the shifted position
+    const float* v;           // [F][H][W] intensity at the shifted position (the sweep's planes; unused here)
     float tSS, tSO;           // the per-tap arithmetic of pixels whose box is moved
 };
 
@@ -174,6 +179,12 @@ __device__ __forceinline__ void tap_dispatch_sym(const float2* __restrict__ col,
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
                  "l"(src)
@@ -196,6 +207,35 @@ __device__ __forceinline__ float drift_wsum(const FhtDriftFrame& d, const double
                    pre[j0 * P + i0]);
 }
 
+// Intensity of output (xM, yM) of a frame with drift, as the reference reads it
+// (liveSRRF_noInterpolation.cl:355-357): the pixel itself for a frame without shift, else
+// getInterpolatedValue(xM + sx, yM + sy) -- bicubic from the staged tile where its 4 x 4 support is
+// interior (the support lies inside the tile: the tile starts at the frame's floor(sx) plus the
+// tap box's first column, less one), bilinear with extrapolation from global memory at the border.
+// Not inlined: the tap loop of the kernel that calls it keeps its registers.
+__device__ __noinline__ float drift_intensity(const FhtDriftFrame* d, const float* __restrict__ sI,
+                                              const float* __restrict__ frame, int W, int H, int xM, int yM,
+                                              int gX0, int gY0, int IW) {
+    if (xM >= W || yM >= H) return 0.f;
+    if (d->zero) return sI[(yM - gY0) * IW + (xM - gX0)];
+    const float x = (float)xM + d->sx, y = (float)yM + d->sy;
+    const int u0 = (int)floorf(x), v0 = (int)floorf(y);
+    if (!(u0 > 0 && u0 < W - 2 && v0 > 0 && v0 < H - 2)) return dev::sample2d(frame, W, H, x, y);
+    const float* r = sI + (v0 - 1 - gY0) * IW + (u0 - 1 - gX0);
+    float cx[4];
+#pragma unroll
+    for (int i = 0; i <= 3; ++i) cx[i] = dev::cubic(x - (float)(u0 - 1 + i));
+    float q = 0.f;
+#pragma unroll
+    for (int j = 0; j <= 3; ++j) {
+        float p = 0.f;
+#pragma unroll
+        for (int i = 0; i <= 3; ++i) p = p + r[j * IW + i] * cx[i];
+        q = q + p * dev::cubic(y - (float)(v0 - 1 + j));
+    }
+    return q;
+}
+
 // GROUPED: the launch may split its frames into groups (gridDim.z); the one-group instantiation
 // compiles the frame loop and the fold without the group bookkeeping.
 template <int S, bool GROUPED, bool DRIFT>
@@ -207,7 +247,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
     float2* sE = reinterpret_cast<float2*>(smem + L::off_E);
     float* sIb = reinterpret_cast<float*>(smem + L::off_I);  // nI buffers of L::I_bytes
     float2* swt = reinterpret_cast<float2*>(smem + L::off_wt);  // [ii][jj] = (w, w/d)
-    int* sjr = reinterpret_cast<int*>(smem + L::off_jr);
+    int* sjr = reinterpret_cast<int*>(smem + L::off_wt + L::wt_bytes);
     float* sst = reinterpret_cast<float*>(smem + L::off_st);    // [5][kTH][kTX]
 
     const int tid = threadIdx.x;
@@ -261,8 +301,9 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         gy0 = y0 + oy + r0c - 1;
     };
     // interpolated tile of frame f with a one-pixel margin beyond the gradient halo (clamped
-    // reads), copied asynchronously into dst
-    auto prefetch_tile = [&](int f, float* dst) {
+    // reads), copied asynchronously into dst; with drift also the frame's tap tables and record
+    // into table set tb
+    auto prefetch_tile = [&](int f, float* dst, int tb) {
         int gX0, gY0;
         origin(f, gX0, gY0);
         const float* fr = a.interp + (long)f * wh;
@@ -271,23 +312,41 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             for (int lx = tx; lx < IW; lx += kTX)
                 cp_async4(dst + ly * IW + lx, fr + grow + min(max(gX0 + lx, 0), W - 1));
         }
+        if constexpr (DRIFT) {
+            unsigned char* tab = smem + L::off_wt + tb * L::tab_bytes;
+            const unsigned char* gw = reinterpret_cast<const unsigned char*>(dp.wt + (long)f * S * S);
+            const unsigned char* gj = reinterpret_cast<const unsigned char*>(dp.jr + (long)f * 2 * S);
+            constexpr int nw = (int)(sizeof(float2) * S * S / 16), nj = (int)(sizeof(int) * 2 * S / 16);
+            constexpr int nr = (int)(sizeof(FhtDriftFrame) / 16);
+            for (int q = tid; q < nw + nj + nr; q += blockDim.x) {
+                if (q < nw)
+                    cp_async16(tab + 16 * q, gw + 16 * q);
+                else if (q < nw + nj)
+                    cp_async16(tab + L::wt_bytes + 16 * (q - nw), gj + 16 * (q - nw));
+                else
+                    cp_async16(tab + L::wt_bytes + L::jr_bytes + 16 * (q - nw - nj),
+                               reinterpret_cast<const unsigned char*>(dp.fr + f) + 16 * (q - nw - nj));
+            }
+        }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    if (L::kDB && fe > fs) prefetch_tile(fs, sIb);
+    if (L::kDB && fe > fs) prefetch_tile(fs, sIb, 0);
 
     for (int f = fs; f < fe; ++f) {
         float* sI = sIb + (L::kDB ? ((f - fs) & 1) * kIStride : 0);
         __syncthreads();
-        // 0. this frame's tap tables (drift)
+        // 0. this frame's tap tables (drift): prefetched with the tile, or loaded now
         FhtDriftFrame df{};
         float fi0 = (float)r0c, fj0 = (float)r0c;
+        const int tb = DRIFT && L::kDB ? ((f - fs) & 1) : 0;
         if constexpr (DRIFT) {
-            df = dp.fr[f];
-            fi0 = df.fi0;
-            fj0 = df.fj0;
-            const float2* wt = dp.wt + (long)f * S * S;
-            for (int idx = tid; idx < S * S; idx += blockDim.x) swt[idx] = wt[idx];
-            for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = dp.jr[(long)f * 2 * S + i];
+            swt = reinterpret_cast<float2*>(smem + L::off_wt + tb * L::tab_bytes);
+            sjr = reinterpret_cast<int*>(smem + L::off_wt + tb * L::tab_bytes + L::wt_bytes);
+            if (!L::kDB) {
+                const float2* wt = dp.wt + (long)f * S * S;
+                for (int idx = tid; idx < S * S; idx += blockDim.x) swt[idx] = wt[idx];
+                for (int i = tid; i < 2 * S; i += blockDim.x) sjr[i] = dp.jr[(long)f * 2 * S + i];
+            }
         }
         int gX0, gY0;
         origin(f, gX0, gY0);
@@ -303,6 +362,17 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             }
         }
         __syncthreads();
+        // the frame's record: in shared memory with its prefetched tables, else in global memory;
+        // only the tap origins are read before the tap loop (the rest after it, to keep the loop's
+        // registers free)
+        const FhtDriftFrame* rec =
+            L::kDB ? reinterpret_cast<const FhtDriftFrame*>(smem + L::off_wt + tb * L::tab_bytes + L::wt_bytes +
+                                                            L::jr_bytes)
+                   : dp.fr + f;
+        if constexpr (DRIFT) {
+            fi0 = rec->fi0;
+            fj0 = rec->fj0;
+        }
         // 2. unit gradient at each tap source: Gx read at min(X+1, W-1), Gy at min(Y+1, H-1),
         //    Roberts cross with max(.-1, 0) clamps (liveSRRF_noInterpolation.cl:144-155, 291-292)
         for (int ey = ty; ey < EH; ey += kTYT) {
@@ -335,7 +405,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
         }
         __syncthreads();
         // the next frame's tile goes into the other buffer while this frame's taps run
-        if (L::kDB && f + 1 < fe) prefetch_tile(f + 1, sIb + ((f + 1 - fs) & 1) * kIStride);
+        if (L::kDB && f + 1 < fe) prefetch_tile(f + 1, sIb + ((f + 1 - fs) & 1) * kIStride, (f + 1 - fs) & 1);
         // 3. tap loop, one box column at a time with its weights in registers
         float acc[kK];
 #pragma unroll
@@ -365,6 +435,9 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             }
         }
         if constexpr (DRIFT) {
+            df = *rec;
+            gX0 = x0 + df.ix + r0c - 1;
+            gY0 = y0 + df.iy + r0c - 1;
             const double* pre = dp.pre + (long)f * (S + 1) * (S + 1);
 #pragma unroll
             for (int k = 0; k < kK; ++k) wsum[k] = drift_wsum<S>(df, pre, xM, y0 + ty * kK + k, r0c, W, H);
@@ -428,8 +501,7 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             const float cg = dev::cglh_power(acc[k] / wsum[k], fp.sens);
             float v;
             if constexpr (DRIFT) {
-                const int yM = y0 + ty * kK + k;
-                v = xM < W && yM < H ? __ldg(dp.v + (long)f * wh + (long)yM * W + xM) : 0.f;
+                v = drift_intensity(rec, sI, a.interp + (long)f * wh, W, H, xM, y0 + ty * kK + k, gX0, gY0, IW);
             } else {
                 v = sI[(ty * kK + k + 1 - r0c) * IW + (tx + 1 - r0c)];
             }

@@ -173,13 +173,6 @@ cudaError_t fht_shift_sample(const float* interp, int W, int H, int F, const flo
     return cudaGetLastError();
 }
 
-cudaError_t fht_drift_build(const FhtGeometry& g, const float* sx, const float* sy, int F,
-                            const float* interp, int W, int H, FhtDriftTables& t, cudaStream_t stream) {
-    cudaError_t e = fht_drift_tables_build(g, sx, sy, F, t, stream);
-    if (e != cudaSuccess) return e;
-    return fht_shift_sample(interp, W, H, F, sx, sy, t.v, stream);
-}
-
 cudaError_t fht_rgc_fused_drift(const FhtGeometry& g, const FhtDriftTables& t, const FhtRgcArgs& a,
                                 cudaStream_t stream) {
     if (a.F > t.capacity || g.S > t.S) return cudaErrorInvalidValue;
