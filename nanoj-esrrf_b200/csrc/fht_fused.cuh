@@ -213,7 +213,7 @@ __device__ __forceinline__ float drift_wsum(const FhtDriftFrame& d, const double
 // interior (the support lies inside the tile: the tile starts at the frame's floor(sx) plus the
 // tap box's first column, less one), bilinear with extrapolation from global memory at the border.
 // Not inlined: the tap loop of the kernel that calls it keeps its registers.
-__device__ __noinline__ float drift_intensity(const FhtDriftFrame* d, const float* __restrict__ sI,
+static __device__ __noinline__ float drift_intensity(const FhtDriftFrame* d, const float* __restrict__ sI,
                                               const float* __restrict__ frame, int W, int H, int xM, int yM,
                                               int gX0, int gY0, int IW) {
     if (xM >= W || yM >= H) return 0.f;
