@@ -191,12 +191,13 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
                  : "memory");
 }
 
-// Sum of the tap weights of output (xM, yM) over its in-image taps for a frame with drift: the
-// whole table's sum (in the reference's (j, i) order) where the tap box lies inside the image,
-// else the in-image rectangle of the box from the frame's 2-D prefix table.
+// Sum of the tap weights of output (xM, yM) over its in-image taps for a frame with drift where
+// the tap box leaves the image: the in-image rectangle of the box from the frame's 2-D prefix
+// table (where the box is inside after all, the whole table's sum in the reference's (j, i)
+// order).  Called for the pixels of threads near the border only, so not inlined.
 template <int S>
-__device__ __forceinline__ float drift_wsum(const FhtDriftFrame& d, const double* __restrict__ pre, int xM,
-                                            int yM, int r0, int W, int H) {
+static __device__ __noinline__ float drift_wsum_border(const FhtDriftFrame& d, const double* __restrict__ pre,
+                                                       int xM, int yM, int r0, int W, int H) {
     const int bx = xM + d.ix + r0, by = yM + d.iy + r0;  // source of tap (ii, jj) = (0, 0)
     const int i0 = max(0, -bx), i1 = min(S - 1, W - 1 - bx);
     const int j0 = max(0, -by), j1 = min(S - 1, H - 1 - by);
@@ -206,6 +207,11 @@ __device__ __forceinline__ float drift_wsum(const FhtDriftFrame& d, const double
     return (float)(pre[(j1 + 1) * P + i1 + 1] - pre[j0 * P + i1 + 1] - pre[(j1 + 1) * P + i0] +
                    pre[j0 * P + i0]);
 }
+
+// (int)((double)xc - 0.5), the reference's tap-box start for a float centre xc, in FP32: the
+// subtraction rounded towards zero keeps the integer part of the exact difference (the integer
+// below |xc - 0.5| is representable and lies between the two), so the truncation agrees.
+__device__ __forceinline__ int box_start(float xc) { return __float2int_rz(__fsub_rz(xc, 0.5f)); }
 
 // Intensity of output (xM, yM) of a frame with drift, as the reference reads it
 // (liveSRRF_noInterpolation.cl:355-357): the pixel itself for a frame without shift, else
@@ -234,6 +240,47 @@ static __device__ __noinline__ float drift_intensity(const FhtDriftFrame* d, con
         q = q + p * dev::cubic(y - (float)(v0 - 1 + j));
     }
     return q;
+}
+
+// The reference's box of pixel (xM, yM) of a frame with drift starts at (int)(xc - 0.5) with
+// xc = (float)(xM + 0.5 + sx) (liveSRRF_noInterpolation.cl:264-281): one column (row) further than
+// the table's floor(sx) where the float rounding of xc reaches the next integer or the truncation
+// of a negative xc - 0.5 goes towards zero (mx, my = 1).  The offsets of the taps the two boxes
+// share agree (to the rounding of xc), so such a pixel's sums (cg, ws) are corrected by its box's
+// moved edges only: the taps of the table's first column (row) leave, those of column (row) S
+// come in (the tiles carry that column and row).  sEk: the unit-gradient tile at the pixel's
+// table tap (0, 0).  Rare (a fraction within rounding of 1, or pixels left of or above the
+// shifted image), so not inlined: the common path keeps its registers and its code compact.
+template <int S, int EW>
+static __device__ __noinline__ float2 drift_edge(const FhtDriftFrame& df, const float2* __restrict__ sEk, int xM,
+                                                 int yM, int mx, int my, int W, int H, float tSO, float tSS,
+                                                 float cg, float ws) {
+    constexpr int r0c = -(S - 2) / 2;
+    const int bx = xM + df.ix + r0c, by = yM + df.iy + r0c;  // source of table tap (0, 0)
+    // tap (ii, jj) of the table's geometry, added (sign +1) or removed (-1)
+    auto edge = [&](int ii, int jj, float sign) {
+        const int X = bx + ii, Y = by + jj;
+        if (X < 0 || X >= W || Y < 0 || Y >= H) return;
+        // the table's arithmetic (drift_tables_kernel): the removed taps cancel exactly
+        const float dx = (float)((double)(r0c + ii) - (double)df.fx);
+        const float dy = (float)((double)(r0c + jj) - (double)df.fy);
+        const float d = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+        if (!(d != 0.f && d <= tSO)) return;
+        float w = __fmul_rn(d, expf(-__fmul_rn(d, d) / tSS));
+        w = __fmul_rn(__fmul_rn(__fmul_rn(w, w), w), w);
+        ws += sign * w;
+        const float2 g = sEk[jj * EW + ii];
+        if (g.x * dx + g.y * dy < 0.f) cg += sign * (w - (w / d) * fabsf(g.y * dx - g.x * dy));
+    };
+    if (mx == 1) {
+        for (int jj = 0; jj < S; ++jj) edge(0, jj, -1.f);        // first column leaves
+        for (int jj = my; jj < S + my; ++jj) edge(S, jj, 1.f);   // column S comes in
+    }
+    if (my == 1) {
+        for (int ii = mx; ii < S; ++ii) edge(ii, 0, -1.f);       // first row leaves
+        for (int ii = mx; ii < S; ++ii) edge(ii, S, 1.f);        // row S comes in
+    }
+    return make_float2(cg, ws);
 }
 
 // GROUPED: the launch may split its frames into groups (gridDim.z); the one-group instantiation
@@ -438,51 +485,37 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             df = *rec;
             gX0 = x0 + df.ix + r0c - 1;
             gY0 = y0 + df.iy + r0c - 1;
-            const double* pre = dp.pre + (long)f * (S + 1) * (S + 1);
+            // sums of weights: the table's where the thread's 8 tap boxes lie inside the image
+            {
+                const int bx = xM + df.ix + r0c, by = y0 + ty * kK + df.iy + r0c;
+                const bool inside = bx >= 0 && bx + S - 1 < W && by >= 0 && by + kK - 1 + S - 1 < H;
+                const double* pre = dp.pre + (long)f * (S + 1) * (S + 1);
 #pragma unroll
-            for (int k = 0; k < kK; ++k) wsum[k] = drift_wsum<S>(df, pre, xM, y0 + ty * kK + k, r0c, W, H);
-            // The reference's box of pixel (xM, yM) starts at (int)(xc - 0.5) with
-            // xc = (float)(xM + 0.5 + sx) (liveSRRF_noInterpolation.cl:264-281): one column (row)
-            // further than the table's floor(sx) where the float rounding of xc reaches the next
-            // integer or the truncation of a negative xc - 0.5 goes towards zero.  The offsets of
-            // the taps the two boxes share agree (to the rounding of xc), so such a pixel's sums
-            // are corrected by its box's moved edges only: the taps of the table's first column
-            // (row) leave, those of column (row) S come in (the tiles carry that column and row).
-            const float xc = (float)((double)xM + 0.5 + (double)df.sx);
-            const int mx = (int)((double)xc - 0.5) - (xM + df.ix);
+                for (int k = 0; k < kK; ++k)
+                    wsum[k] = inside ? df.wsum_int : drift_wsum_border<S>(df, pre, xM, y0 + ty * kK + k, r0c, W, H);
+            }
+            // pixels whose reference box starts one column or row further (drift_edge).  The
+            // centre xc = (float)(xM + 0.5 + sx) (liveSRRF_noInterpolation.cl:264-265): xM + 0.5
+            // is exact in FP32, so one rounded addition gives it.  mx once per thread; my per row
+            // only where it can be non-zero, i.e. where the rounding of yc (at most half an ulp of
+            // |yc| <= H + |sy| + 1, below 2^-24 of it) can reach the next integer, or for rows at
+            // or above the shifted image's top
+            const float xc = __fadd_rn((float)xM + 0.5f, df.sx);
+            const int mx = box_start(xc) - (xM + df.ix);
+            const bool ychk = (1.f - df.fy) * 4194304.f <= (float)H + fabsf(df.sy) + 2.f || y0 + ty * kK + df.iy < 1;
+            if (mx != 0 || ychk) {
 #pragma unroll
-            for (int k = 0; k < kK; ++k) {
-                const int yM = y0 + ty * kK + k;
-                const float yc = (float)((double)yM + 0.5 + (double)df.sy);
-                const int my = (int)((double)yc - 0.5) - (yM + df.iy);
-                if ((mx == 0 && my == 0) || mx < 0 || mx > 1 || my < 0 || my > 1 || xM >= W || yM >= H) continue;
-                const int bx = xM + df.ix + r0c, by = yM + df.iy + r0c;  // source of table tap (0, 0)
-                float cg = acc[k], ws = wsum[k];
-                // tap (ii, jj) of the table's geometry, added (sign +1) or removed (-1)
-                auto edge = [&](int ii, int jj, float sign) {
-                    const int X = bx + ii, Y = by + jj;
-                    if (X < 0 || X >= W || Y < 0 || Y >= H) return;
-                    // the table's arithmetic (drift_tables_kernel): the removed taps cancel exactly
-                    const float dx = (float)((double)(r0c + ii) - (double)df.fx);
-                    const float dy = (float)((double)(r0c + jj) - (double)df.fy);
-                    const float d = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
-                    if (!(d != 0.f && d <= dp.tSO)) return;
-                    float w = __fmul_rn(d, expf(-__fmul_rn(d, d) / dp.tSS));
-                    w = __fmul_rn(__fmul_rn(__fmul_rn(w, w), w), w);
-                    ws += sign * w;
-                    const float2 g = sE[(ty * kK + k + jj) * EW + tx + ii];
-                    if (g.x * dx + g.y * dy < 0.f) cg += sign * (w - (w / d) * fabsf(g.y * dx - g.x * dy));
-                };
-                if (mx == 1) {
-                    for (int jj = 0; jj < S; ++jj) edge(0, jj, -1.f);        // first column leaves
-                    for (int jj = my; jj < S + my; ++jj) edge(S, jj, 1.f);   // column S comes in
+                for (int k = 0; k < kK; ++k) {
+                    const int yM = y0 + ty * kK + k;
+                    const float yc = __fadd_rn((float)yM + 0.5f, df.sy);
+                    const int my = box_start(yc) - (yM + df.iy);
+                    if ((mx == 0 && my == 0) || mx < 0 || mx > 1 || my < 0 || my > 1 || xM >= W || yM >= H)
+                        continue;
+                    const float2 r = drift_edge<S, EW>(df, sE + (ty * kK + k) * EW + tx, xM, yM, mx, my, W, H,
+                                                       dp.tSO, dp.tSS, acc[k], wsum[k]);
+                    acc[k] = r.x;
+                    wsum[k] = r.y;
                 }
-                if (my == 1) {
-                    for (int ii = mx; ii < S; ++ii) edge(ii, 0, -1.f);       // first row leaves
-                    for (int ii = mx; ii < S; ++ii) edge(ii, S, 1.f);        // row S comes in
-                }
-                acc[k] = cg;
-                wsum[k] = ws;
             }
         }
         // 4. normalisation, sensitivity, intensity weighting and cumulants
@@ -495,13 +528,68 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             continue;
         }
         const int tglob = a.t0 + f;
+        // Intensities of a frame with drift, separably: the thread's 8 outputs share their column,
+        // so the x weights of getInterpolatedValue's bicubic; where the 8 shifted rows
+        // (float)(yM + sy) also share their fraction (all of them in binades where the rounding of
+        // yM + sy gives the same fraction, which the first and last row decide) they share the y
+        // weights, and the horizontal sum of a tile row (the bicubic's inner loop) is the same for
+        // each of the 4 outputs whose support holds the row: 11 row sums serve the 8 outputs, each
+        // output's sums in the reference's order.  Otherwise (borders, binade changes, zero shift)
+        // each output is sampled alone (drift_intensity).
+        bool sep = false;
+        float cxw[4], cyw[4], hp0 = 0.f, hp1 = 0.f, hp2 = 0.f;
+        const float* hr = sI;
+        if constexpr (DRIFT) {
+            const int yA = y0 + ty * kK, yB = yA + kK - 1;
+            if (!rec->zero && xM < W && yB < H) {
+                const float x = (float)xM + rec->sx;
+                const int u0 = (int)floorf(x);
+                const float ya = (float)yA + rec->sy, yb = (float)yB + rec->sy;
+                const int va = (int)floorf(ya), vb = (int)floorf(yb);
+                sep = u0 > 0 && u0 < W - 2 && va > 0 && vb < H - 2 && vb - va == kK - 1 &&
+                      ya - (float)va == yb - (float)vb;
+                if (sep) {
+#pragma unroll
+                    for (int i = 0; i <= 3; ++i) {
+                        cxw[i] = dev::cubic(x - (float)(u0 - 1 + i));
+                        cyw[i] = dev::cubic(ya - (float)(va - 1 + i));
+                    }
+                    hr = sI + (va - 1 - gY0) * IW + (u0 - 1 - gX0);
+                    auto hrow = [&](int m) {
+                        float p = 0.f;
+#pragma unroll
+                        for (int i = 0; i <= 3; ++i) p = p + hr[m * IW + i] * cxw[i];
+                        return p;
+                    };
+                    hp0 = hrow(0);
+                    hp1 = hrow(1);
+                    hp2 = hrow(2);
+                }
+            }
+        }
 #pragma unroll
         for (int k = 0; k < kK; ++k) {
             const int o = (ty * kK + k) * kTX + tx;
             const float cg = dev::cglh_power(acc[k] / wsum[k], fp.sens);
             float v;
             if constexpr (DRIFT) {
-                v = drift_intensity(rec, sI, a.interp + (long)f * wh, W, H, xM, y0 + ty * kK + k, gX0, gY0, IW);
+                if (sep) {
+                    float hp3 = 0.f;
+#pragma unroll
+                    for (int i = 0; i <= 3; ++i) hp3 = hp3 + hr[(k + 3) * IW + i] * cxw[i];
+                    float q = 0.f;
+                    q = q + hp0 * cyw[0];
+                    q = q + hp1 * cyw[1];
+                    q = q + hp2 * cyw[2];
+                    q = q + hp3 * cyw[3];
+                    v = q;
+                    hp0 = hp1;
+                    hp1 = hp2;
+                    hp2 = hp3;
+                } else {
+                    v = drift_intensity(rec, sI, a.interp + (long)f * wh, W, H, xM, y0 + ty * kK + k, gX0, gY0,
+                                        IW);
+                }
             } else {
                 v = sI[(ty * kK + k + 1 - r0c) * IW + (tx + 1 - r0c)];
             }
