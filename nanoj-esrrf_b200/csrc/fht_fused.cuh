@@ -164,6 +164,118 @@ __device__ __forceinline__ void tap_length(const float2* __restrict__ col, float
     }
 }
 
+// One source row of a chord (already loaded: e, its offset fr) for the outputs KLO .. KHI, the
+// weights of output k in slot (Q - k) & 7 of an 8-entry register window: the per-tap arithmetic of
+// tap_chord.
+template <int KLO, int KHI, int Q>
+__device__ __forceinline__ void rot_row(float2 e, float fr, float fi, const float (&w8)[8], const float (&wd8)[8],
+                                        float (&acc)[kK]) {
+    float rgy;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rgy) : "f"(e.y));
+    const float thr = fmaf(e.x * rgy, fi, fr);
+    const bool neg = e.y < 0.f;
+    const float cr0 = fmaf(-e.x, fr, e.y * fi);
+#pragma unroll
+    for (int k = KLO; k <= KHI; ++k) {
+        const float ck = k == 0 ? cr0 : fmaf((float)k, e.x, cr0);
+        const float t = fmaf(-fabsf(ck), wd8[(Q - k) & 7], w8[(Q - k) & 7]);
+        if (((float)k > thr) != neg) acc[k] += t;
+    }
+}
+
+// Head rows RR .. 6 of a chord: outputs 0 .. RR (tap rows RR .. 0, window slots RR - k).
+template <int EW, int RR>
+__device__ __forceinline__ void rot_head(const float2* __restrict__ col, float fr0, float fi, const float (&w8)[8],
+                                         const float (&wd8)[8], float (&acc)[kK]) {
+    if constexpr (RR < 7) {
+        rot_row<0, RR, RR>(col[RR * EW], fr0 + (float)RR, fi, w8, wd8, acc);
+        rot_head<EW, RR + 1>(col, fr0, fi, w8, wd8, acc);
+    }
+}
+
+// Body rows at chunk positions Q .. 7 (Q .. NQ - 1), all outputs; the row at position q is tap
+// row 8 + 8m + q, whose weight enters slot q.  frr: the row index as a float (exact), so that the
+// row's offset is fr0 + (float)rr as in tap_chord.
+template <int EW, int Q, int NQ>
+__device__ __forceinline__ void rot_body(const float2* __restrict__ p, const float2* __restrict__ pw, float fr0,
+                                         float& frr, float fi, float (&w8)[8], float (&wd8)[8], float (&acc)[kK]) {
+    if constexpr (Q < NQ) {
+        const float2 wv = pw[Q];
+        w8[Q] = wv.x;
+        wd8[Q] = wv.y;
+        rot_row<0, 7, Q>(p[Q * EW], fr0 + frr, fi, w8, wd8, acc);
+        frr += 1.f;
+        rot_body<EW, Q + 1, NQ>(p, pw, fr0, frr, fi, w8, wd8, acc);
+    }
+}
+
+// The remainder rows of the body: positions Q .. n - 1 (n < 8 at run time).
+template <int EW, int Q>
+__device__ __forceinline__ void rot_rest(const float2* __restrict__ p, const float2* __restrict__ pw, int n,
+                                         float fr0, float& frr, float fi, float (&w8)[8], float (&wd8)[8],
+                                         float (&acc)[kK]) {
+    if constexpr (Q < 7) {
+        if (Q < n) {
+            rot_body<EW, Q, Q + 1>(p, pw, fr0, frr, fi, w8, wd8, acc);
+            rot_rest<EW, Q + 1>(p, pw, n, fr0, frr, fi, w8, wd8, acc);
+        }
+    }
+}
+
+// Tail rows L + T .. L + 6: outputs T + 1 .. 7, tap rows L + T - k in slot T + 7 - k of the
+// window reloaded with tap rows L - 7 .. L - 1.  Rows above 7 (chords shorter than 7) were head
+// rows and are skipped.
+template <int EW, int T>
+__device__ __forceinline__ void rot_tail(const float2* __restrict__ pt, int L, float fr0, float frL, float fi,
+                                         const float (&w8)[8], const float (&wd8)[8], float (&acc)[kK]) {
+    if constexpr (T < 7) {
+        if (L + T >= 7) rot_row<T + 1, 7, T + 7>(pt[T * EW], fr0 + (frL + (float)T), fi, w8, wd8, acc);
+        rot_tail<EW, T + 1>(pt, L, fr0, frL, fi, w8, wd8, acc);
+    }
+}
+
+// A chord of runtime length L (tap rows 0 .. L - 1 of the column from col, weights from wc, both
+// from the chord's first row; wc is zero beyond L up to S - 1, S >= 8) in one code path for every
+// length, so that the code a frame runs stays small: the weights live in an 8-slot register window
+// (tap row jj in slot jj & 7) that advances with the rows.  Head rows 0 .. 6 (outputs 0 .. rr; for
+// L < 7 the rows past the chord add taps of weight 0), row 7 and the body rows 8 .. L - 1 (all
+// outputs; 8-row chunks, then up to 7 remainder rows), and tail rows L .. L + 6 (outputs
+// rr - L + 1 .. 7) with the chord's last 7 weights reloaded in a fixed order.  Each output's taps
+// are added in increasing tap row, as in tap_chord, so the sums are the same.
+template <int S, int EW>
+__device__ __forceinline__ void tap_rot(const float2* __restrict__ col, const float2* __restrict__ wc, float fi,
+                                        float fr0, int L, float (&acc)[kK]) {
+    static_assert(S >= 8, "the head window reads 8 weights of the column");
+    float w8[8], wd8[8];
+    const float4* w4 = reinterpret_cast<const float4*>(wc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 v = w4[q];
+        w8[2 * q] = v.x;
+        wd8[2 * q] = v.y;
+        w8[2 * q + 1] = v.z;
+        wd8[2 * q + 1] = v.w;
+    }
+    rot_head<EW, 0>(col, fr0, fi, w8, wd8, acc);
+    if (L >= 8) {
+        rot_row<0, 7, 7>(col[7 * EW], fr0 + 7.f, fi, w8, wd8, acc);
+        int rr = 8;
+        float frr = 8.f;
+        const float2* p = col + 8 * EW;
+        const float2* pw = wc + 8;
+#pragma unroll 1
+        for (; rr + 8 <= L; rr += 8, p += 8 * EW, pw += 8) rot_body<EW, 0, 8>(p, pw, fr0, frr, fi, w8, wd8, acc);
+        rot_rest<EW, 0>(p, pw, L - rr, fr0, frr, fi, w8, wd8, acc);
+    }
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+        const float2 wv = wc[max(L - 7 + j, 0)];
+        w8[j] = wv.x;
+        wd8[j] = wv.y;
+    }
+    rot_tail<EW, 0>(col + L * EW, L, fr0, (float)L, fi, w8, wd8, acc);
+}
+
 template <int S, int EW, int LO>
 __device__ __forceinline__ void tap_dispatch_sym(const float2* __restrict__ col, float fi, float fr0, int lo,
                                                  int hi, const float (&w)[S], const float (&wd)[S],
@@ -461,6 +573,12 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
             const int lo = sjr[2 * ii], hi = sjr[2 * ii + 1];
             if (lo > hi) continue;  // no tap of the disc in this column
             const float fi = fi0 + (float)ii;
+            if constexpr (DRIFT && S >= 8) {
+                // weights stored from the chord's first row: rows lo .. hi as 0 .. L - 1
+                tap_rot<S, EW>(sE + (ty * kK + lo) * EW + tx + ii, swt + ii * S, fi, fj0 + (float)lo,
+                               min(hi - lo + 1, S), acc);
+                continue;
+            }
             float w[S], wd[S];
             const float4* wc = reinterpret_cast<const float4*>(swt + ii * S);
 #pragma unroll
