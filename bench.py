@@ -404,22 +404,35 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md", "rgc_fused_bic512": "rgc_bic_bic512.md"}
+TRAFFIC_SUMMARIES = {"rgc_fused_fht512": "rgc_fused_fht512.md", "rgc_fused_bic512": "rgc_bic_bic512.md",
+                     "rgc_fused_fht512_drift": "rgc_fused_drift_fht512.md"}
 # the kernel sources each summary's counts depend on
 SUMMARY_SOURCES = {
     "rgc_fused_fht512": ["fht_fused.cuh", "rgc_fht.cu"],
     "rgc_fused_bic512": ["rgc_bic.cu", "device_common.cuh"],
+    "rgc_fused_fht512_drift": ["fht_fused.cuh", "rgc_fht_drift.cu"],
 }
 
 
+def _code_only(text):
+    """A C++/CUDA source without its comments, trailing blanks and empty lines (what the compiler
+    sees; the kernel sources have no '//' or '/*' inside string literals)."""
+    import re
+
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    lines = (line.split("//", 1)[0].rstrip() for line in text.splitlines())
+    return "\n".join(line for line in lines if line)
+
+
 def source_sha(kernel):
-    """sha256 (first 16 hex digits) of the sources a kernel's ncu figures depend on."""
+    """sha256 (first 16 hex digits) of the code of the sources a kernel's ncu figures depend on
+    (comments and blank lines removed, so that editing a comment keeps a capture current)."""
     import hashlib
 
     h = hashlib.sha256()
     for name in SUMMARY_SOURCES.get(kernel, []):
-        with open(os.path.join(PKG, "csrc", name), "rb") as f:
-            h.update(f.read())
+        with open(os.path.join(PKG, "csrc", name), encoding="utf-8") as f:
+            h.update(_code_only(f.read()).encode())
     return h.hexdigest()[:16]
 
 
@@ -617,14 +630,14 @@ def run_ours(args, world, rank, local):
     achieved_tflops = ops_launch / avg_launch_s / 1e12
     cpu = (cpu_reference_sample(stack, M, fwhm, S, 2 if bic else 1, bic=bic)
            if not args.no_cpu_baseline and world == 1 else None)
-    summary_key = f"rgc_{args.kernel}_{args.workload}"
+    summary_key = f"rgc_{args.kernel}_{args.workload}" + ("_drift" if args.drift else "")
     stale = summary_stale(summary_key)
-    traffic = None if stale or args.drift else read_traffic_summary(summary_key)
+    traffic = None if stale else read_traffic_summary(summary_key)
     # the kernel's real limit is instruction issue: warp instructions per launch (ncu count per
     # frame x frames) over the live launch time, against one warp instruction per cycle per
     # scheduler (148 SMs x 4) at the sampled SM clock
     clocks = clk.summary()
-    ipf = None if stale or args.drift else read_traffic_summary(summary_key, "warp_instructions_per_frame")
+    ipf = None if stale else read_traffic_summary(summary_key, "warp_instructions_per_frame")
     roofline_issue = None
     if stale:
         roofline_issue = {"unavailable": stale}

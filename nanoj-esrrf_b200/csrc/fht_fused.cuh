@@ -148,8 +148,8 @@ __device__ __forceinline__ void tap_chord(const float2* __restrict__ col, float 
 // either the whole box or the rows -J .. J, i.e. tap rows [LO, S - 2 - LO]: one instantiation per
 // LO.  With drift the chords are not symmetric; a column's weights are stored from its chord's
 // first row on, so the chord runs as tap rows [0, L - 1] of a column and row origin moved down by
-// lo: one instantiation per chord length L, found by a binary search over L (about five compares
-// per column).
+// lo.  Tap boxes of 8 and more take tap_rot (one code path for every L); the small boxes (S 4 and
+// 6) one instantiation per chord length L, found by a binary search over L.
 template <int S, int EW, int A, int B>
 __device__ __forceinline__ void tap_length(const float2* __restrict__ col, float fi, float fr0, int L,
                                            const float (&w)[S], const float (&wd)[S], float (&acc)[kK]) {

@@ -7,15 +7,16 @@
 // plugins set it per SR block (gui/LiveSRRF_optimised_.java:283-305) or once for the whole sweep
 // (gui/ParametersSweep_.java:282-290, :452-454).  A shift is uniform over a frame, so here each
 // frame of a launch gets its own tap tables (drift_tables_kernel: weights, disc chords, prefix
-// sums) and its intensity plane at the shifted position (shift_sample_kernel), and the fused tile
-// kernel (fht_fused.cuh, DRIFT = true) runs on them at full tap rate.
+// sums, the frame's record), and the fused tile kernel (fht_fused.cuh, DRIFT = true) runs on them
+// at full tap rate, sampling the shifted intensities from its staged tile.  shift_sample_kernel
+// writes whole intensity planes at the shifted positions for the sweep's per-frame mode.
 //
 // Residual against the reference's per-pixel arithmetic: the reference rounds xc to float per
 // pixel, so its centre offsets carry a rounding error of up to half an ulp of xM (6e-5 magnified
 // pixels below 2048); the tables use the exact fraction of the shift.  Where that rounding (a
 // fraction within rounding of 1) or the truncation of (int)(xc - 0.5) towards zero (left of or
-// above the image) moves a pixel's box by one source column or row, the tile kernel evaluates that
-// pixel with the reference's own per-tap arithmetic instead of the tables (see fht_fused.cuh).
+// above the image) moves a pixel's box by one source column or row, the tile kernel corrects that
+// pixel's sums by the box's moved edges with the reference's per-tap arithmetic (fht_fused.cuh).
 #include <math.h>
 
 #include "device_common.cuh"
