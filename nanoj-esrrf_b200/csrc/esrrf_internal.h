@@ -314,6 +314,12 @@ struct Rgc3dTables {
     int* zseg = nullptr;
     int* zsoff = nullptr;
     int zk0 = 0, znz = 0;
+    // Within a plane offset the entries are grouped by the range [a, b] of z-phases they are taps
+    // of (a contiguous range: dz is monotonic in the z-phase), the full range first, then the
+    // others in (a, b) order (z3d_class_range); zcseg[lp (znz zncls + 1) + s zncls + c] is the
+    // first entry of class c of plane s, the last value the phase's entry count.
+    int* zcseg = nullptr;
+    int zncls = 0;             // M (M + 1) / 2 classes
     int sl_symin = 0, sl_fxmin = 0, sl_rows = 0, sl_nx = 0;
 };
 // Tables for planes of w x h pixels, P planes; the per-voxel sums of weights are computed on

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "device_common.cuh"
@@ -29,6 +30,21 @@ BicGeometry bic_geometry(float fwhm, int sensitivity) {
     g.tSO = 2 * g.sigma + 1;
     g.sensitivity = (float)sensitivity;
     return g;
+}
+
+// The z-phase ranges [a, b] of z-blocked entries (M z-phases; an entry is a tap of a contiguous
+// range of z-phases, dz being monotonic in the z-phase): class 0 is the full range [0, M - 1],
+// then the others in (a, b) order.  upper: b, else a.
+__host__ __device__ constexpr int z3d_class_range(int M, int c, bool upper) {
+    if (c == 0) return upper ? M - 1 : 0;
+    int k = 1;
+    for (int a = 0; a < M; ++a)
+        for (int b = a; b < M; ++b) {
+            if (a == 0 && b == M - 1) continue;
+            if (k == c) return upper ? b : a;
+            ++k;
+        }
+    return -1;
 }
 
 namespace {
@@ -622,6 +638,54 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
     }
 }
 
+// Entries [tb, te) of a slab that are taps of z-phases A .. B only (the other z-phases' weights
+// are 0 there, so leaving them out changes no sum), for the two cells of rgc3d_z2_kernel.
+template <int MZ, int A, int B>
+__device__ __forceinline__ void z2_entries(const float* __restrict__ sf, int es, const float4* __restrict__ sl,
+                                           int cell1, int tb, int te, float (&cg)[2][MZ]) {
+    for (int t = tb; t < te; ++t) {
+        const float* e = sf + (long)t * es * 4;
+        const int o = __float_as_int(e[0]);
+        const float dx = e[1], dy = e[2];
+        float4 u[2];
+        u[0] = sl[o];
+        u[1] = sl[o + cell1];
+        float part[2], cz2[2], dyuz[2], dxuz[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            part[c] = fmaf(u[c].x, dx, u[c].y * dy);
+            const float cz = fmaf(dx, u[c].y, -dy * u[c].x);  // dx gy - dy gx
+            cz2[c] = cz * cz;
+            dyuz[c] = dy * u[c].z;
+            dxuz[c] = dx * u[c].z;
+        }
+#pragma unroll
+        for (int p = A; p <= B; ++p) {
+            const float dz = e[3 + 3 * p], w = e[4 + 3 * p], wd = e[5 + 3 * p];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const float dot = fmaf(u[c].z, dz, part[c]);
+                if (dot < 0.f) {
+                    const float cx = fmaf(-dz, u[c].y, dyuz[c]);  // dy gz - dz gy
+                    const float cy = fmaf(dz, u[c].x, -dxuz[c]);  // dz gx - dx gz
+                    cg[c][p] += fmaf(-wd, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz2[c]))), w);
+                }
+            }
+        }
+    }
+}
+
+// The classes C .. of a slab's entries in turn (cs: the slab's class starts, cs[ncls] its end).
+template <int MZ, int C>
+__device__ __forceinline__ void z2_classes(const int* __restrict__ cs, const float* __restrict__ sf, int es,
+                                           const float4* __restrict__ sl, int cell1, float (&cg)[2][MZ]) {
+    if constexpr (C < MZ * (MZ + 1) / 2) {
+        z2_entries<MZ, z3d_class_range(MZ, C, false), z3d_class_range(MZ, C, true)>(sf, es, sl, cell1, cs[C],
+                                                                                   cs[C + 1], cg);
+        z2_classes<MZ, C + 1>(cs, sf, es, sl, cell1, cg);
+    }
+}
+
 // rgc3d_zs_kernel with two cells per thread: thread (tx, ty) of a CTA computes the cells in rows
 // ty and ty + 8 of a 32 x 16 cell tile (same lateral phase, so the same entry list).  Each entry's
 // table values (offset, dx, dy, and per z-phase dz, w, w/d) are loaded once for both cells, and the
@@ -645,15 +709,16 @@ __global__ void __launch_bounds__(256, 2) rgc3d_z2_kernel(Rgc3dTabArgs a) {
     const int row2 = 2 * a.tab.sl_nx;                       // float4s per slab row
     const int rows = a.tab.sl_rows + 16;                    // slab rows of 16 cell rows
     const int slab = rows * row2;                           // float4s per slab
+    constexpr int NC = MZ * (MZ + 1) / 2;                   // z-phase range classes
     float4* stab = sm4;                                     // [n][es]
-    int* sseg = reinterpret_cast<int*>(sm4 + a.tab.zmax_taps * es);  // [nz + 1]
-    float4* sbuf = sm4 + a.tab.zmax_taps * es + (nz + 4) / 4;        // [2][slab]
+    int* sseg = reinterpret_cast<int*>(sm4 + a.tab.zmax_taps * es);  // [nz NC + 1] class starts
+    float4* sbuf = sm4 + a.tab.zmax_taps * es + (nz * NC + 4) / 4;   // [2][slab]
     for (int i = tid; i < n * es; i += 256) {
         float4 v = a.tab.ztab[(long)t0 * es + i];
         if (i % es == 0) v.x = __int_as_float(a.tab.zsoff[t0 + i / es]);  // offset in the slab
         stab[i] = v;
     }
-    for (int i = tid; i <= nz; i += 256) sseg[i] = a.tab.zseg[lp * (nz + 1) + i];
+    for (int i = tid; i <= nz * NC; i += 256) sseg[i] = a.tab.zcseg[lp * (nz * NC + 1) + i];
     const float* sf = reinterpret_cast<const float*>(stab);
     const int qx_raw = bx * 32 + threadIdx.x;
     int qy_raw[2];
@@ -733,37 +798,7 @@ __global__ void __launch_bounds__(256, 2) rgc3d_z2_kernel(Rgc3dTabArgs a) {
         __syncthreads();  // slab g landed everywhere; buffer (g + 1) & 1 is no longer read
         if (g + 1 < G) stage(g + 1);
         const float4* sl = sbuf + (g & 1) * slab + tbase;
-        const int tb = sseg[sidx], te = sseg[sidx + 1];
-        for (int t = tb; t < te; ++t) {
-            const float* e = sf + (long)t * es * 4;
-            const int o = __float_as_int(e[0]);
-            const float dx = e[1], dy = e[2];
-            float4 u[2];
-            u[0] = sl[o];
-            u[1] = sl[o + cell1];
-            float part[2], cz2[2], dyuz[2], dxuz[2];
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                part[c] = fmaf(u[c].x, dx, u[c].y * dy);
-                const float cz = fmaf(dx, u[c].y, -dy * u[c].x);  // dx gy - dy gx
-                cz2[c] = cz * cz;
-                dyuz[c] = dy * u[c].z;
-                dxuz[c] = dx * u[c].z;
-            }
-#pragma unroll
-            for (int p = 0; p < MZ; ++p) {
-                const float dz = e[3 + 3 * p], w = e[4 + 3 * p], wd = e[5 + 3 * p];
-#pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const float dot = fmaf(u[c].z, dz, part[c]);
-                    if (dot < 0.f) {
-                        const float cx = fmaf(-dz, u[c].y, dyuz[c]);  // dy gz - dz gy
-                        const float cy = fmaf(dz, u[c].x, -dxuz[c]);  // dz gx - dx gz
-                        cg[c][p] += fmaf(-wd, sqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz2[c]))), w);
-                    }
-                }
-            }
-        }
+        z2_classes<MZ, 0>(sseg + sidx * NC, sf, es, sl, cell1, cg);
         if (sidx != nz - 1) continue;
         const float* ap = a.apx + (long)f * a.P * pl;
 #pragma unroll
@@ -816,7 +851,7 @@ __global__ void __launch_bounds__(256, 2) rgc3d_z2_kernel(Rgc3dTabArgs a) {
 }
 
 size_t z2_smem_bytes(const Rgc3dTables& t) {
-    return sizeof(float4) * ((size_t)t.zmax_taps * t.zes + (t.znz + 4) / 4 +
+    return sizeof(float4) * ((size_t)t.zmax_taps * t.zes + (t.znz * t.zncls + 4) / 4 +
                              2 * (size_t)(t.sl_rows + 16) * 2 * t.sl_nx);
 }
 
@@ -964,7 +999,7 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
     // z-blocked entries: per lateral phase, the (j, i, k) taps valid for at least one z-phase
     std::vector<float4> Z;
     std::vector<int> zstart(M * M + 1, 0);
-    std::vector<int> zsx, zsy, zsz, zsoff, zseg;
+    std::vector<int> zsx, zsy, zsz, zcls, zsoff, zseg, zcseg;
     if (M <= 5) {
         t.zes = (3 + 3 * M + 3) / 4;
         int zmax = 0;
@@ -975,13 +1010,18 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
                 const float xc = (float)(((double)px + 0.5) / M);
                 const float yc = (float)(((double)py + 0.5) / M);
                 const int kx = (int)(2.0f * xc), ky = (int)(2.0f * yc);
-                for (int k = k0; k <= k1; ++k) {  // entries ordered by plane offset
+                for (int k = k0; k <= k1; ++k) {  // entries ordered by plane offset, then by class
+                    struct ZEnt {
+                        int cls, sx, sy, sz;
+                        std::vector<float> ent;
+                    };
+                    std::vector<ZEnt> plane;
                     for (int j = r0; j <= r1; ++j) {
                         const float vy = ((float)ky + (float)j) / 2.0f;
                         for (int i = r0; i <= r1; ++i) {
                             const float vx = ((float)kx + (float)i) / 2.0f;
                             std::vector<float> ent(4 * t.zes, 0.f);
-                            bool any = false;
+                            int pa = M, pb = -1, nin = 0;  // z-phases of which this is a tap
                             const float dx = vx - xc, dy = vy - yc;
                             for (int pz = 0; pz < M; ++pz) {
                                 const float zc = (float)(((double)pz + 0.5) / M);
@@ -993,20 +1033,35 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
                                 wt = wt * wt * wt * wt;
                                 ent[4 + 3 * pz] = wt;
                                 ent[5 + 3 * pz] = wt / d;
-                                any = true;
+                                pa = std::min(pa, pz);
+                                pb = std::max(pb, pz);
+                                ++nin;
                             }
-                            if (!any) continue;
+                            if (nin == 0) continue;
+                            // the class of [pa, pb]; a non-contiguous set (none for a sphere)
+                            // would take the full range, whose other phases have weight 0
+                            int cls = 0;
+                            if (nin == pb - pa + 1)
+                                for (int c = 0; c < M * (M + 1) / 2; ++c)
+                                    if (z3d_class_range(M, c, false) == pa && z3d_class_range(M, c, true) == pb)
+                                        cls = c;
                             const int sx = kx + i - 1, sy = ky + j - 1, sz = k;
                             const int off = sz * t.W2p * t.H2p + sy * t.W2p + (sx & 1) * (t.W2p / 2) + (sx >> 1);
                             std::memcpy(&ent[0], &off, 4);
                             ent[1] = dx;
                             ent[2] = dy;
-                            for (int q = 0; q < t.zes; ++q)
-                                Z.push_back(make_float4(ent[4 * q], ent[4 * q + 1], ent[4 * q + 2], ent[4 * q + 3]));
-                            zsx.push_back(sx);
-                            zsy.push_back(sy);
-                            zsz.push_back(sz);
+                            plane.push_back(ZEnt{cls, sx, sy, sz, std::move(ent)});
                         }
+                    }
+                    std::stable_sort(plane.begin(), plane.end(),
+                                     [](const ZEnt& x, const ZEnt& y) { return x.cls < y.cls; });
+                    for (const ZEnt& z : plane) {
+                        for (int q = 0; q < t.zes; ++q)
+                            Z.push_back(make_float4(z.ent[4 * q], z.ent[4 * q + 1], z.ent[4 * q + 2], z.ent[4 * q + 3]));
+                        zsx.push_back(z.sx);
+                        zsy.push_back(z.sy);
+                        zsz.push_back(z.sz);
+                        zcls.push_back(z.cls);
                     }
                 }
                 zmax = std::max(zmax, (int)(Z.size() / t.zes) - zstart[lp]);
@@ -1036,6 +1091,20 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
                 zseg[(size_t)lp * (t.znz + 1) + sidx] = e - e0;
             }
         }
+        t.zncls = M * (M + 1) / 2;
+        const int ncs = t.znz * t.zncls + 1;
+        zcseg.assign((size_t)M * M * ncs, 0);
+        for (int lp = 0; lp < M * M; ++lp) {
+            const int e0 = zstart[lp], e1 = zstart[lp + 1];
+            int e = e0;
+            for (int sidx = 0; sidx < t.znz; ++sidx)
+                for (int c = 0; c < t.zncls; ++c) {
+                    zcseg[(size_t)lp * ncs + sidx * t.zncls + c] = e - e0;
+                    while (e < e1 && zsz[e] - szmin == sidx && zcls[e] == c) ++e;
+                }
+            zcseg[(size_t)lp * ncs + t.znz * t.zncls] = e1 - e0;
+            if (e != e1) return cudaErrorInvalidValue;  // entries not grouped by plane and class
+        }
         t.sl_symin = symin;
         t.sl_fxmin = fxmin;
         t.sl_rows = 2 * 7 + symax - symin + 1;
@@ -1054,7 +1123,8 @@ cudaError_t rgc3d_tables_build(const BicGeometry& g, int M, int w, int h, int P,
         (e = up(&t.start, start)) != cudaSuccess)
         return e;
     if (M <= 5 && ((e = up(&t.ztab, Z)) != cudaSuccess || (e = up(&t.zstart, zstart)) != cudaSuccess ||
-                   (e = up(&t.zseg, zseg)) != cudaSuccess || (e = up(&t.zsoff, zsoff)) != cudaSuccess))
+                   (e = up(&t.zseg, zseg)) != cudaSuccess || (e = up(&t.zsoff, zsoff)) != cudaSuccess ||
+                   (e = up(&t.zcseg, zcseg)) != cudaSuccess))
         return e;
     const long total = (long)w * M * h * M * P * M;
     if ((e = cudaMalloc((void**)&t.wsum, sizeof(float) * total)) != cudaSuccess) return e;
@@ -1079,6 +1149,7 @@ void rgc3d_tables_free(Rgc3dTables& t) {
     cudaFree(t.ztab);
     cudaFree(t.zstart);
     cudaFree(t.zseg);
+    cudaFree(t.zcseg);
     cudaFree(t.zsoff);
     t = Rgc3dTables();
 }
