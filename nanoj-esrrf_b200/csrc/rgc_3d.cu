@@ -641,10 +641,22 @@ __global__ void __launch_bounds__(256, MZ <= 3 ? 3 : 2) rgc3d_zs_kernel(Rgc3dTab
 // Entries [tb, te) of a slab that are taps of z-phases A .. B only (the other z-phases' weights
 // are 0 there, so leaving them out changes no sum), for the two cells of rgc3d_z2_kernel.
 template <int MZ, int A, int B>
-__device__ __forceinline__ void z2_entries(const float* __restrict__ sf, int es, const float4* __restrict__ sl,
+__device__ __forceinline__ void z2_entries(const float* __restrict__ sf, const float4* __restrict__ sl,
                                            int cell1, int tb, int te, float (&cg)[2][MZ]) {
+    // two entries per iteration (their loads and dot products overlap), each entry's table row
+    // read as whole float4s (ES float4s per entry, the tables' zes)
+    constexpr int ES = (3 + 3 * MZ + 3) / 4;
+#pragma unroll 2
     for (int t = tb; t < te; ++t) {
-        const float* e = sf + (long)t * es * 4;
+        float e[4 * ES];
+#pragma unroll
+        for (int q = 0; q < ES; ++q) {
+            const float4 v = reinterpret_cast<const float4*>(sf)[(long)t * ES + q];
+            e[4 * q] = v.x;
+            e[4 * q + 1] = v.y;
+            e[4 * q + 2] = v.z;
+            e[4 * q + 3] = v.w;
+        }
         const int o = __float_as_int(e[0]);
         const float dx = e[1], dy = e[2];
         float4 u[2];
@@ -677,12 +689,12 @@ __device__ __forceinline__ void z2_entries(const float* __restrict__ sf, int es,
 
 // The classes C .. of a slab's entries in turn (cs: the slab's class starts, cs[ncls] its end).
 template <int MZ, int C>
-__device__ __forceinline__ void z2_classes(const int* __restrict__ cs, const float* __restrict__ sf, int es,
+__device__ __forceinline__ void z2_classes(const int* __restrict__ cs, const float* __restrict__ sf,
                                            const float4* __restrict__ sl, int cell1, float (&cg)[2][MZ]) {
     if constexpr (C < MZ * (MZ + 1) / 2) {
-        z2_entries<MZ, z3d_class_range(MZ, C, false), z3d_class_range(MZ, C, true)>(sf, es, sl, cell1, cs[C],
+        z2_entries<MZ, z3d_class_range(MZ, C, false), z3d_class_range(MZ, C, true)>(sf, sl, cell1, cs[C],
                                                                                    cs[C + 1], cg);
-        z2_classes<MZ, C + 1>(cs, sf, es, sl, cell1, cg);
+        z2_classes<MZ, C + 1>(cs, sf, sl, cell1, cg);
     }
 }
 
@@ -798,7 +810,7 @@ __global__ void __launch_bounds__(256, 2) rgc3d_z2_kernel(Rgc3dTabArgs a) {
         __syncthreads();  // slab g landed everywhere; buffer (g + 1) & 1 is no longer read
         if (g + 1 < G) stage(g + 1);
         const float4* sl = sbuf + (g & 1) * slab + tbase;
-        z2_classes<MZ, 0>(sseg + sidx * NC, sf, es, sl, cell1, cg);
+        z2_classes<MZ, 0>(sseg + sidx * NC, sf, sl, cell1, cg);
         if (sidx != nz - 1) continue;
         const float* ap = a.apx + (long)f * a.P * pl;
 #pragma unroll
