@@ -960,8 +960,10 @@ def run_3d(args, world, rank, local):
     plain_ms = per_launch_form(1) if world == 1 else None
     eng = esrrf.LiveSRRF_CL()
     eng.initialise(3 * w, 3 * h, M, fwhm, S, n, n, chosenDevice=local, doMPmapCorrection=True,
-                   calibTable3DSRRF=calib, framesPerLaunch=args.frames_per_launch or 8, kernel=args.kernel)
+                   calibTable3DSRRF=calib, framesPerLaunch=args.frames_per_launch, kernel=args.kernel)
     H = eng.handle
+    tpl = ctypes.c_int(0)
+    esrrf._lib.check(H, L.esrrf_frames_per_launch(H, ctypes.byref(tpl)))  # the engine's choice
     eng.setTiming(True)
     launches = [0]
     rgc_ms = [0.0]
@@ -1027,7 +1029,7 @@ def run_3d(args, world, rank, local):
         "config": {"workload": f"mfm3d: {P} planes of {w}x{h} x {n} timepoints, M3, radius 1.5, S1, "
                                "AVG+VAR (+TAC2, INT), MP correction, one block",
                    "kernel": "tabulated taps" if args.kernel == "fused" else "plain per-voxel",
-                   "timepoints_per_launch": args.frames_per_launch or 8},
+                   "timepoints_per_launch": tpl.value},
         "forms": {"batched_timepoints_per_launch_ms": t_step * 1e3,
                   "plain_1_timepoint_per_launch_ms": plain_ms,
                   "plain_1_timepoint_per_launch_mpx_frames_s": mpxf / (plain_ms / 1e3) if plain_ms else None},

@@ -138,6 +138,17 @@ esrrf_status esrrf_handle::init(const esrrf_params& params) {
         const int nb = std::max(1, p.n_frame_for_srrf);
         const int launches = (nb + fmax - 1) / fmax;
         F = (nb + launches - 1) / launches;
+    } else if (p.frames_per_launch == 0 && mode == Mode::k3D) {
+        // 3-D path: equal launches of at most 32 timepoints (fewer launches amortise loading the
+        // tap tables and the previous values and folding the sums; 9 x 128^2 planes at M3, 200
+        // timepoints: 264 Mpx.frames/s against 258 with 8), within ~2 GB of per-timepoint buffers
+        // (the camera frame's planes, their 2x gradients and the padded unit-gradient field: ~40
+        // camera-frame planes)
+        const double per_frame = 40.0 * sizeof(float) * (double)p.width * p.height;
+        const int fmax = (int)std::max(1.0, std::min(32.0, 2e9 / per_frame));
+        const int nb = std::max(1, p.n_frame_for_srrf);
+        const int launches = (nb + fmax - 1) / fmax;
+        F = (nb + launches - 1) / launches;
     }
 
     if (mode == Mode::kFHT) return init_fht();

@@ -108,12 +108,12 @@ void cache_put(const std::string& path, const std::string& key, const TuneChoice
 }
 
 // Candidate frames per launch for blocks of n frames: every equal cut of the block into launches
-// of about 8 .. 64 frames (3-D: 4 .. 16 timepoints) that fits the per-frame buffer budget.
+// of about 8 .. 64 frames (3-D: 4 .. 32 timepoints) that fits the per-frame buffer budget.
 std::vector<int> candidates(const esrrf_params& p, int n) {
     std::vector<int> targets;
     double per_frame = 0, budget = 4e9;
     if (p.n_planes > 0) {
-        targets = {4, 8, 16};
+        targets = {4, 8, 16, 32};
         per_frame = 40.0 * sizeof(float) * (double)p.width * p.height;
         budget = 2e9;
     } else if (p.interp == ESRRF_INTERP_FHT) {
