@@ -745,8 +745,35 @@ __global__ void __launch_bounds__(256, 2) fht_rgc_fused_kernel(FhtRgcArgs a, Fus
     }
 }
 
-// Launch of one tap-box size: the grid, the frame groups for small frames and the copy of the
-// last group's previous values.
+// Frames of a launch split into g groups across CTAs (blockIdx.z): the g that minimises the
+// launch's modelled time, waves(g) x (frames of the largest group + extra), with waves(g) =
+// ceil(tiles g / slots) for `slots` resident CTAs.  In the cumulant mode a later group also runs
+// the frame before its range (TAC2's previous value), one extra frame, and keeps at least 4
+// frames; in the per-frame mode (emit) the frames are independent.  A quarter frame per CTA
+// stands for its fixed work (tables, the first tile); g = 1 unless another count is 2 % faster.
+// (64 x 64 frames at M5, 50 tiles on 296 slots, 50 frames: 5 groups fit one wave where the
+// fewest groups that cover every slot, 6, spill 4 CTAs into a second one.)
+inline int frame_groups(int tiles, int F, int slots, bool emit) {
+    if (F <= 1 || tiles <= 0 || slots <= 0) return 1;
+    const int gmax = std::min(emit ? std::min(F, 64) : std::max(1, F / 4), 65535);
+    auto cost = [&](int g) {
+        const long waves = ((long)tiles * g + slots - 1) / slots;
+        return (double)waves * ((F + g - 1) / g + (g > 1 && !emit ? 1.0 : 0.0) + 0.25);
+    };
+    int best = 1;
+    double tbest = cost(1);
+    for (int g = 2; g <= gmax; ++g) {
+        const double t = cost(g);
+        if (t < 0.98 * tbest) {
+            best = g;
+            tbest = t;
+        }
+    }
+    return best;
+}
+
+// Launch of one tap-box size: the grid, the frame groups and the copy of the last group's
+// previous values.
 template <int S, bool DRIFT>
 cudaError_t launch_fused(int r0, float sens, const FusedParams& fp_in, const DriftParams& dp,
                          const FhtRgcArgs& a, cudaStream_t stream) {
@@ -769,13 +796,9 @@ cudaError_t launch_fused(int r0, float sens, const FusedParams& fp_in, const Dri
     fp.r0 = r0;
     fp.sens = sens;
     dim3 grid((a.W + kTX - 1) / kTX, (a.H + kTH - 1) / kTH);
-    // frames split into groups across CTAs only where the tiles alone give fewer than two CTAs
-    // per SM (small frames); a group keeps at least 4 frames when it pays an extra frame
     const int tiles = (int)(grid.x * grid.y), slots = 2 * sm_count(dev);
-    if (tiles < slots && a.F > 1 && (a.cg_out || a.prev_out)) {
-        const int gmax = a.cg_out ? a.F : std::max(1, a.F / 4);
-        grid.z = (unsigned)std::max(1, std::min({(slots + tiles - 1) / tiles, gmax, 65535}));
-    }
+    if (a.F > 1 && (a.cg_out || a.prev_out))
+        grid.z = (unsigned)frame_groups(tiles, a.F, slots, a.cg_out != nullptr);
     if (grid.z > 1)
         fht_rgc_fused_kernel<S, true, DRIFT><<<grid, 256, bytes, stream>>>(a, fp, dp);
     else
