@@ -8,11 +8,12 @@
 // alpha, beta = least-squares fit F ~ alpha D + beta, loss = mean((alpha D + beta - F)^2).
 // alpha and beta are refitted for every evaluation, so their own derivatives drop out.
 //
-// Backward pass, per chunk of frames (nothing per frame is kept from the forward pass except
-// C_t; the unit-gradient field and the tap sums are recomputed):
-//   kernel A: recompute C_t and dC/dtSS at every output pixel from the tap loop, emit
-//             b = dL/dN (N = C * sum of weights), the intensity-weighting term of dL/dI_t, and
-//             accumulate dL/dS and dL/dtSS;
+// The forward pass of a gradient evaluation runs kernel A's tap loop in its emit form: per frame
+// and output pixel C_t and the d^2-weighted sum of the inward taps' terms (what dC/dtSS needs),
+// kept for the backward pass with the interpolated frames (a loss-only evaluation runs the fused
+// forward kernel instead).  Backward pass, per chunk of frames:
+//   kernel A's terms (adj_tail_kernel, per pixel): b = dL/dN (N = C * sum of weights), the
+//             intensity-weighting term of dL/dI_t, and the sums dL/dS and dL/dtSS;
 //   kernel B: at every tap source, gather dL/dg over the taps whose outputs it feeds
 //             (dphi/dg = [g.t < 0] (w/d) sgn(c) (t_y, -t_x), c = g_y t_x - g_x t_y), project onto
 //             the unit-vector tangent, and scatter through the Roberts cross (atomics) into
@@ -68,6 +69,10 @@ struct AdjAArgs {
     float* b;            // [F][H][W] dL/dN
     float* gI;           // [F][H][W] initialised with the intensity-weighting term
     double* acc;         // [2]: dL/dS, dL/dtSS
+    // forward of a gradient evaluation: if set, write C = CGLH / sum of weights and the
+    // d^2-weighted inward tap sum per frame and pixel instead of the backward terms (b, gI, acc)
+    float* c_out = nullptr;  // [F][H][W]
+    float* q_out = nullptr;  // [F][H][W]
 };
 
 // One tap column of kernel A restricted to its disc chord [LO, HI] (compile-time, as in the fused
@@ -236,6 +241,17 @@ __global__ void __launch_bounds__(256, 2) adj_a_kernel(AdjAArgs g) {
 #pragma unroll
             for (int k = 0; k < kK; ++k) acc2[k] = fmaf(fi * fi, acc[k] - before[k], acc2[k]);
         }
+        if (g.c_out) {
+#pragma unroll
+            for (int k = 0; k < kK; ++k) {
+                const int yM = y0 + ty * kK + k;
+                if (xM >= W || yM >= H) continue;
+                const long pix = (long)yM * W + xM;
+                g.c_out[(long)f * wh + pix] = acc[k] / __ldg(g.wsum + pix);
+                g.q_out[(long)f * wh + pix] = acc2[k];
+            }
+            continue;
+        }
 #pragma unroll
         for (int k = 0; k < kK; ++k) {
             const int yM = y0 + ty * kK + k;
@@ -268,7 +284,7 @@ __global__ void __launch_bounds__(256, 2) adj_a_kernel(AdjAArgs g) {
         red[1][ty] = dT;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && g.acc) {  // (none in the emit form)
         double s0 = 0, s1 = 0;
         for (int i = 0; i < kTYT; ++i) {
             s0 += red[0][i];
@@ -471,6 +487,65 @@ __global__ void __launch_bounds__(256, 2) adj_b_kernel(AdjBArgs g) {
     }
 }
 
+// Kernel A's per-pixel terms from the forward's planes (kernel A in its emit form wrote C and the
+// d^2-weighted tap sum Q of every frame, so the backward pass needs no second tap loop): the same
+// arithmetic as kernel A's epilogue, over the F frames of a chunk, grid-stride over (frame, pixel).
+struct AdjTailArgs {
+    const float* I;      // [F][P] interpolated frames of the chunk
+    const float* C;      // [F][P] CGLH / sum of weights
+    const float* Q;      // [F][P] sum over the inward taps of d^2 (w - (w/d) |c|)
+    const float* a;      // [P] dL/dR / T
+    const float* wsum;   // [P]
+    const float* dwsum;  // [P] d(sum of weights)/dtSS
+    long P;
+    int F;
+    float kscale, sens;
+    float* b;            // [F][P] dL/dN
+    float* gI;           // [F][P] the intensity-weighting term of dL/dI
+    double* acc;         // [2]: dL/dS, dL/dtSS
+};
+
+__global__ void __launch_bounds__(256) adj_tail_kernel(AdjTailArgs g) {
+    double dS = 0.0, dT = 0.0;
+    const long n = g.P * g.F;
+    for (long o = (long)blockIdx.x * blockDim.x + threadIdx.x; o < n; o += (long)gridDim.x * blockDim.x) {
+        const long pix = o % g.P;
+        const float v = g.I[o], C = g.C[o];
+        const float ws = __ldg(g.wsum + pix), av = __ldg(g.a + pix);
+        float Cs = 0.f, b = 0.f;
+        if (C > 0.f && C < INFINITY) {
+            const float lc = logf(C);
+            Cs = expf(g.sens * lc);
+            const float dC = av * v * g.sens * Cs / C;
+            b = dC / ws;
+            dS += (double)av * v * Cs * lc;
+            dT += (double)b * (g.Q[o] * g.kscale - C * __ldg(g.dwsum + pix));
+        }
+        g.gI[o] = av * Cs;
+        g.b[o] = b;
+    }
+    __shared__ double red[2][8];
+    for (int s = 16; s > 0; s >>= 1) {
+        dS += __shfl_xor_sync(0xffffffffu, dS, s);
+        dT += __shfl_xor_sync(0xffffffffu, dT, s);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[0][warp] = dS;
+        red[1][warp] = dT;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0, s1 = 0;
+        for (int i = 0; i < 8; ++i) {
+            s0 += red[0][i];
+            s1 += red[1][i];
+        }
+        atomicAdd(g.acc, s0);
+        atomicAdd(g.acc + 1, s1);
+    }
+}
+
 // ---- loss side ---------------------------------------------------------------------------------
 struct Gauss {
     int r;
@@ -668,6 +743,8 @@ struct esrrf_adjoint {
     float* kwtab = nullptr;            // [S][S] kappa * w (for d sum w / dtSS)
     float* dwsum = nullptr;            // [HM][WM]
     float *I = nullptr, *C = nullptr;  // [T][HM][WM]
+    float* Q = nullptr;                // [T][HM][WM] d^2-weighted inward tap sums (gradient forward)
+    bool q_valid = false;              // C and Q come from a gradient forward at the current radius
     float *R = nullptr, *tmp = nullptr, *Bb = nullptr, *gB = nullptr, *gR = nullptr, *t1 = nullptr, *t2 = nullptr;
     float *Fm = nullptr, *D = nullptr, *dF = nullptr;  // [h][w]
     float *bbuf = nullptr, *gI = nullptr;              // [Fc][HM][WM]
@@ -687,7 +764,8 @@ struct esrrf_adjoint {
                     std::string(what) + ": " + cudaGetErrorName(e));
     }
     esrrf_status set_radius(float fwhm);
-    esrrf_status forward(const float* frames, float fwhm, float sens, float sigma_b, double* loss);
+    esrrf_status forward(const float* frames, float fwhm, float sens, float sigma_b, double* loss,
+                         bool for_grad = false);
     esrrf_status backward(const float* frames, float fwhm, float sens, float sigma_b, double* grads,
                           float* graw);
     void release();
@@ -739,7 +817,8 @@ esrrf_status esrrf_adjoint::set_radius(float fwhm) {
     return ESRRF_OK;
 }
 
-esrrf_status esrrf_adjoint::forward(const float* frames, float fwhm, float sens, float sigma_b, double* loss) {
+esrrf_status esrrf_adjoint::forward(const float* frames, float fwhm, float sens, float sigma_b, double* loss,
+                                    bool for_grad) {
     esrrf_status r = set_radius(fwhm);
     if (r != ESRRF_OK) return r;
     if (!(sigma_b > 0.f) || 4.0 * sigma_b > (kMaxGauss - 1) / 2) return fail(ESRRF_ERR_INVALID, "sigma out of range");
@@ -750,14 +829,34 @@ esrrf_status esrrf_adjoint::forward(const float* frames, float fwhm, float sens,
         AK(interp_run(plan, scratch, frames + (size_t)t * w * h, false, n, I + (size_t)t * P, stream, nullptr),
            "interpolation");
     }
-    FhtRgcArgs a{};
-    a.interp = I;
-    a.W = WM;
-    a.H = HM;
-    a.F = T;
-    a.int_weighting = 1;
-    a.cg_out = C;
-    AK(fht_rgc_fused(geo, tables, a, stream), "RGC");
+    q_valid = false;
+    if (for_grad) {
+        // the backward pass needs, besides C, each pixel's d^2-weighted tap sum: kernel A's tap
+        // loop produces both in one pass, so the backward pass has no second tap loop
+        AdjAArgs A{};
+        A.I = I;
+        A.tab = tabA;
+        A.wsum = tables.wsum;
+        A.jr = tables.jrange;
+        A.W = WM;
+        A.H = HM;
+        A.F = T;
+        A.r0 = geo.r0;
+        A.c_out = C;
+        A.q_out = Q;
+        AdjBArgs B{};
+        AK(launch_adj_any(geo.S, A, B, false, stream), "RGC with tap sums");
+        q_valid = true;
+    } else {
+        FhtRgcArgs a{};
+        a.interp = I;
+        a.W = WM;
+        a.H = HM;
+        a.F = T;
+        a.int_weighting = 1;
+        a.cg_out = C;
+        AK(fht_rgc_fused(geo, tables, a, stream), "RGC");
+    }
     recon_kernel<<<(unsigned)((P + 255) / 256), 256, 0, stream>>>(I, C, T, P, sens, R);
     const Gauss g = make_gauss(sigma_b, false);
     blur1d_kernel<<<dim3((WM + 127) / 128, HM), 128, 0, stream>>>(R, WM, HM, 0, g, tmp);
@@ -825,7 +924,29 @@ esrrf_status esrrf_adjoint::backward(const float* frames, float fwhm, float sens
         B.F = n;
         B.r1 = geo.r1;
         B.gI = gI;
-        AK(launch_adj_any(geo.S, A, B, false, stream), "adjoint A");
+        if (!q_valid) return fail(ESRRF_ERR_STATE, "the backward pass needs the gradient forward's tap sums");
+        AdjTailArgs Tl{};
+        Tl.I = A.I;
+        Tl.C = C + (size_t)t * P;
+        Tl.Q = Q + (size_t)t * P;
+        Tl.a = gR;
+        Tl.wsum = tables.wsum;
+        Tl.dwsum = dwsum;
+        Tl.P = P;
+        Tl.F = n;
+        Tl.kscale = A.kscale;
+        Tl.sens = sens;
+        Tl.b = bbuf;
+        Tl.gI = gI;
+        Tl.acc = dstat + 5;
+        {
+            int dev = 0, nsm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            const long blocks = std::min<long>((P * n + 255) / 256, 8L * std::max(nsm, 1));
+            adj_tail_kernel<<<(unsigned)blocks, 256, 0, stream>>>(Tl);
+        }
+        AK(cudaGetLastError(), "adjoint A terms");
         AK(launch_adj_any(geo.S, A, B, true, stream), "adjoint B");
         float* gr = out + (size_t)t * p;
         init_graw_kernel<<<(unsigned)((p * n + 255) / 256), 256, 0, stream>>>(dF, p, n, 1.0f / T, gr);
@@ -850,7 +971,7 @@ void esrrf_adjoint::release() {
     interp_plan_destroy(plan);
     fht_fused_tables_free(tables);
     for (void* q : {(void*)scratch.rowT, (void*)scratch.xs, (void*)scratch.alt, (void*)scratch.vec, (void*)dx, (void*)tabA,
-                    (void*)wdB, (void*)kwtab, (void*)dwsum, (void*)I, (void*)C, (void*)R, (void*)tmp,
+                    (void*)wdB, (void*)kwtab, (void*)dwsum, (void*)I, (void*)C, (void*)Q, (void*)R, (void*)tmp,
                     (void*)Bb, (void*)gB, (void*)gR, (void*)t1, (void*)t2, (void*)Fm, (void*)D, (void*)dF,
                     (void*)bbuf, (void*)gI, (void*)T1, (void*)gX, (void*)proj, (void*)dvec,
                     (void*)graw_tmp, (void*)dstat})
@@ -918,6 +1039,7 @@ esrrf_status esrrf_adjoint_create(int width, int height, int n_frames, int magni
         (e = al(&a->dwsum, sizeof(float) * P)) != cudaSuccess ||
         (e = al(&a->I, sizeof(float) * P * n_frames)) != cudaSuccess ||
         (e = al(&a->C, sizeof(float) * P * n_frames)) != cudaSuccess ||
+        (e = al(&a->Q, sizeof(float) * P * n_frames)) != cudaSuccess ||
         (e = al(&a->R, sizeof(float) * P)) != cudaSuccess || (e = al(&a->tmp, sizeof(float) * P)) != cudaSuccess ||
         (e = al(&a->Bb, sizeof(float) * P)) != cudaSuccess || (e = al(&a->gB, sizeof(float) * P)) != cudaSuccess ||
         (e = al(&a->gR, sizeof(float) * P)) != cudaSuccess || (e = al(&a->t1, sizeof(float) * P)) != cudaSuccess ||
@@ -950,7 +1072,7 @@ esrrf_status esrrf_loss_and_grad(esrrf_adjoint* a, const float* d_frames, float 
                                  float sigma_b, double* loss, double* grads, float* d_grad_frames) {
     if (!a || !d_frames) return ESRRF_ERR_INVALID;
     if (cudaSetDevice(a->device) != cudaSuccess) return a->fail(ESRRF_ERR_CUDA, "cudaSetDevice");
-    esrrf_status r = a->forward(d_frames, fwhm, sensitivity, sigma_b, loss);
+    esrrf_status r = a->forward(d_frames, fwhm, sensitivity, sigma_b, loss, true);
     if (r != ESRRF_OK) return r;
     return a->backward(d_frames, fwhm, sensitivity, sigma_b, grads, d_grad_frames);
 }
