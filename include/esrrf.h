@@ -230,7 +230,9 @@ esrrf_status esrrf_last_timing(const esrrf_handle* h, float* interp_ms, float* r
  * with the arrays laid end to end.
  * Devices: n_devices > 1 splits the sweep across those CUDA ordinals (esrrf_sweep_plan says how);
  * each device keeps its own copy of the frames it needs, nothing is exchanged between devices, and
- * esrrf_sweep_run gathers every output into the host buffer.  n_devices = 0 uses `device`. */
+ * esrrf_sweep_run gathers every output into the host buffer.  n_devices = 0 uses `device`.  A
+ * device listed k times takes up to k shards, which run concurrently on it (each with its own
+ * stream, frame copy and graph). */
 typedef struct {
     int width, height, n_frames;
     int n_mag;
@@ -260,8 +262,8 @@ esrrf_status esrrf_sweep_create(const esrrf_sweep_params* params, esrrf_sweep** 
  * leaves devices idle or unbalanced -- the blocks, cut by start into contiguous runs of balanced
  * frame span, every pair on every device; the split with the smaller largest cost is used.
  * pair_device[m * n_radius + r] / block_device[b]: the device ordinal, -1 = every device of the
- * split, -2 = none.  device_cost[d] (per entry of the device list): the relative cost.  Each may
- * be NULL. */
+ * split, -2 = none.  device_cost[d] (per entry of the device list, so per shard where a device is
+ * listed twice): the relative cost.  Each may be NULL. */
 esrrf_status esrrf_sweep_plan(const esrrf_sweep_params* params, int* pair_device, int* block_device,
                               double* device_cost);
 /* Output layout: for magnification m, radius r the floats from offsets[m * n_radius + r] hold

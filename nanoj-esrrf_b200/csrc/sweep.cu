@@ -567,6 +567,7 @@ double pair_cost_per_px(int M, float radius, int interp) {
 
 struct ShardPlan {
     int device = 0;
+    int slot = 0;             // index in the caller's device list (a device may be listed twice)
     std::vector<int> pairs;   // mi * n_radius + ri
     std::vector<int> blocks;  // global block indices
     double cost = 0;
@@ -598,6 +599,7 @@ std::vector<ShardPlan> plan_shards(const esrrf_sweep_params& p, const std::vecto
     if (nD <= 1) {
         ShardPlan s;
         s.device = nD ? devices[0] : 0;
+        s.slot = 0;
         s.pairs = all_pairs;
         s.blocks = all_blocks;
         s.cost = pc_sum * span_all;
@@ -605,7 +607,10 @@ std::vector<ShardPlan> plan_shards(const esrrf_sweep_params& p, const std::vecto
     }
     // mode A
     std::vector<ShardPlan> a(nD);
-    for (int d = 0; d < nD; ++d) a[d].device = devices[d];
+    for (int d = 0; d < nD; ++d) {
+        a[d].device = devices[d];
+        a[d].slot = d;
+    }
     std::vector<int> order(nP);
     for (int q = 0; q < nP; ++q) order[q] = q;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return pc[x] > pc[y]; });
@@ -656,6 +661,7 @@ std::vector<ShardPlan> plan_shards(const esrrf_sweep_params& p, const std::vecto
     for (size_t g = 0; g < groups.size(); ++g) {
         ShardPlan s;
         s.device = devices[g];
+        s.slot = (int)g;
         s.pairs = all_pairs;
         s.blocks = groups[g];
         std::sort(s.blocks.begin(), s.blocks.end());
@@ -705,9 +711,6 @@ esrrf_status validate(const esrrf_sweep_params* sp) {
     if (sp->drift_x && sp->interp == ESRRF_INTERP_BIC)
         return reject("drift correction is available in the FHT sweep only (run the bicubic engine per block)");
     if (sp->n_devices < 0 || (sp->n_devices > 0 && !sp->devices)) return reject("bad device list");
-    for (int d = 0; d < sp->n_devices; ++d)
-        for (int e = 0; e < d; ++e)
-            if (sp->devices[d] == sp->devices[e]) return reject("a device is listed twice");
     return ESRRF_OK;
 }
 
@@ -756,7 +759,7 @@ esrrf_status esrrf_sweep_plan(const esrrf_sweep_params* sp, int* pair_device, in
     for (int b = 0; b < sp->n_blocks && block_device; ++b) block_device[b] = -2;
     for (size_t d = 0; d < devs.size() && device_cost; ++d) device_cost[d] = 0;
     for (const ShardPlan& s : plan) {
-        const int di = (int)(std::find(devs.begin(), devs.end(), s.device) - devs.begin());
+        const int di = s.slot;
         const bool all_pairs = (int)s.pairs.size() == nP, all_blocks = (int)s.blocks.size() == sp->n_blocks;
         if (pair_device)
             for (int q : s.pairs) pair_device[q] = all_pairs && plan.size() > 1 ? -1 : s.device;

@@ -92,3 +92,51 @@ def test_bicubic_rolling_matches_engine_blocks(esrrf_mod):
             eng.release()
         for k in range(4):
             assert rel_err(res[(st, ln)][k], ref[k]) < TOL, (st, ln, k)
+
+
+def _shards_vs_single(esrrf_mod, raw, mags, radii, sens, blocks, by, **kw):
+    """The same sweep on one device and split into shards of a device listed twice (each shard
+    with its own frame range, stream and graph, gathered into the caller's layout); ``by``: the
+    split the planner must choose ("pairs" or "blocks")."""
+    h, w = raw.shape[1:]
+    pd, bd, _ = esrrf_mod.Sweep.plan(w, h, raw.shape[0], mags, radii, sens, blocks, [0, 0],
+                                     interpolation=kw.get("interpolation", "fht"))
+    if by == "pairs":
+        assert bd == [-1] * len(blocks) and pd == [0] * len(pd)
+    else:
+        assert pd == [-1] * len(pd) and bd == [0] * len(blocks)
+    one = esrrf_mod.Sweep(w, h, raw.shape[0], mags, radii, sens, blocks, **kw)
+    two = esrrf_mod.Sweep(w, h, raw.shape[0], mags, radii, sens, blocks, devices=[0, 0], **kw)
+    try:
+        assert one.shard_count() == 1 and two.shard_count() == 2
+        ref = one.run(raw)
+        got = two.run(raw)
+        again = two.run(raw)
+    finally:
+        one.release()
+        two.release()
+    assert got.keys() == ref.keys()
+    for key in ref:
+        np.testing.assert_array_equal(again[key], got[key])
+        for k in range(4):
+            assert rel_err(got[key][k], ref[key][k]) < 1e-6, (key, k, rel_err(got[key][k], ref[key][k]))
+
+
+def test_sweep_split_by_pairs_gathers_the_single_device_layout(esrrf_mod):
+    """The multi-device split by (magnification, radius) pairs, run as two shards on this device:
+    every output lands in its place of the global layout, equal to the unsplit sweep."""
+    from esrrf import synth
+    raw = synth.small_stack(55, 24, 32, 40, emitters=16)
+    _shards_vs_single(esrrf_mod, raw, [2, 3], [1.0, 1.5, 2.5], [1, 2], [(0, 10), (10, 14), (5, 7)], "pairs")
+
+
+def test_rolling_split_by_blocks_gathers_the_single_device_layout(esrrf_mod):
+    """The split by contiguous runs of blocks (one pair): each shard copies only its frame range
+    and its part of the per-frame drift; FHT with drift and bicubic without."""
+    from esrrf import synth
+    raw = synth.small_stack(56, 40, 32, 32, emitters=16)
+    blocks = [(0, 10), (10, 10), (20, 10), (30, 10)]
+    rng = np.random.default_rng(7)
+    drift = (rng.uniform(-1.2, 1.2, 40).astype(np.float32), rng.uniform(-1.2, 1.2, 40).astype(np.float32))
+    _shards_vs_single(esrrf_mod, raw, [4], [1.5], [2], blocks, "blocks", drift=drift)
+    _shards_vs_single(esrrf_mod, raw, [3], [1.5], [1], blocks, "blocks", interpolation="bicubic")

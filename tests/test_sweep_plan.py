@@ -67,10 +67,22 @@ def test_overlapping_blocks_stay_together(esrrf_mod):
     assert bd == [0, 0, 1, 1]
 
 
-def test_bad_device_lists_are_rejected(esrrf_mod):
+def test_a_device_listed_twice_takes_two_shards(esrrf_mod):
+    """Entries of the device list are shards: a device listed twice is planned like two devices
+    (costs per entry), and the reported device of each unit is the ordinal."""
+    radii = [0.5 + 0.25 * k for k in range(11)]
+    blocks = [(0, 37), (37, 64), (101, 99), (0, 100)]
+    pd2, bd2, cost2 = plan(esrrf_mod, 200, [2, 4], radii, blocks, [0, 1])
+    pd, bd, cost = plan(esrrf_mod, 200, [2, 4], radii, blocks, [5, 5])
+    assert cost == cost2 and bd == bd2
+    assert pd == [5] * len(pd)
+    blocks = [(100 * k, 100) for k in range(4)]
+    pd, bd, cost = plan(esrrf_mod, 400, [4], [1.5], blocks, [0, 0])
+    assert pd == [-1] and bd == [0, 0, 0, 0] and cost[0] == cost[1] > 0
+
+
+def test_drift_in_a_bicubic_sweep_is_rejected(esrrf_mod):
     from esrrf import EsrrfError
-    with pytest.raises(EsrrfError, match="twice"):
-        plan(esrrf_mod, 10, [2], [1.0], [(0, 10)], [0, 0])
     with pytest.raises(EsrrfError, match="drift"):
         esrrf_mod.Sweep(16, 16, 10, [2], [1.0], [1], [(0, 10)], interpolation="bicubic",
                         drift=(np.zeros(10), np.zeros(10)), devices=[0])
