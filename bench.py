@@ -1212,11 +1212,13 @@ def main():
     ap.add_argument("--drift", action="store_true",
                     help="fht512/bic512: a seeded per-frame shift in every block (vibration correction)")
     args = ap.parse_args()
+    if args.impl == "reference":
+        # rank 0 alone times the CPU reference; it takes no collective, so no process group
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
     world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
-            run_reference(args, world, rank)
-        elif args.workload == "sweep256":
+        if args.workload == "sweep256":
             run_sweep(args, world, rank, local)
         elif args.workload == "mfm3d":
             run_3d(args, world, rank, local)
