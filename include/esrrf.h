@@ -271,7 +271,8 @@ esrrf_status esrrf_sweep_plan(const esrrf_sweep_params* params, int* pair_device
 esrrf_status esrrf_sweep_output_layout(const esrrf_sweep* s, size_t* total_floats, size_t* offsets);
 /* frames: [n_frames][height][width] uint16 (is_u16 = 1) or float; device pointers here (a sweep on
  * one device only), host pointers in esrrf_sweep_run.  The first run with given pointers captures
- * the graph. */
+ * the graph.  esrrf_sweep_run with a pinned `out` (page-locked, e.g. cudaHostAlloc) on a one-device
+ * sweep copies each (magnification, radius) pair's outputs while the later pairs compute. */
 esrrf_status esrrf_sweep_run_device(esrrf_sweep* s, const void* d_frames, int is_u16, float* d_out);
 esrrf_status esrrf_sweep_run(esrrf_sweep* s, const void* frames, int is_u16, float* out);
 /* Kernels in one run (the graphs' node count over all devices). */

@@ -178,7 +178,13 @@ struct Shard {
     cudaGraphExec_t exec = nullptr;
     const void* g_in = nullptr;
     float* g_out = nullptr;
+    float* g_hout = nullptr;
     int g_u16 = -1;
+    // host-output runs into pinned memory: each pair's outputs are copied out on copy_stream as
+    // soon as its cumulants are written, while the next pairs compute
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> pair_ev;  // per (mp entry, radius entry)
+    cudaEvent_t copy_done = nullptr;
     int launches_per_run = 0;
     std::string err;
 
@@ -192,10 +198,12 @@ struct Shard {
     }
     esrrf_status create(const std::vector<float>& radii, int interp);
     esrrf_status create_bic(const std::vector<float>& radii);
-    esrrf_status enqueue(const void* frames, int is_u16, float* out);
-    esrrf_status enqueue_bic(const void* frames, int is_u16, float* out);
+    esrrf_status enqueue(const void* frames, int is_u16, float* out, float* hout);
+    esrrf_status enqueue_bic(const void* frames, int is_u16, float* out, float* hout);
+    esrrf_status copy_pair(size_t oi, const float* out, float* hout);
+    esrrf_status copy_join(float* hout);
     esrrf_status tc_check();
-    esrrf_status run_device(const void* d_frames, int is_u16, float* d_out);
+    esrrf_status run_device(const void* d_frames, int is_u16, float* d_out, float* h_out = nullptr);
     void release();
 };
 
@@ -210,11 +218,34 @@ struct Shard {
         if (_e != cudaSuccess) return sh->fail_cuda(_e, what);  \
     } while (0)
 
-esrrf_status Shard::enqueue(const void* frames, int is_u16, float* out) {
+// Pair oi's outputs (its sensitivities and blocks, contiguous in the shard's layout) to the
+// same place of the pinned host buffer, on copy_stream once the compute stream has written them.
+esrrf_status Shard::copy_pair(size_t oi, const float* out, float* hout) {
+    Shard* s = this;
+    if (!hout) return ESRRF_OK;
+    const size_t n = (oi + 1 < offsets.size() ? offsets[oi + 1] : total) - offsets[oi];
+    SK(cudaEventRecord(pair_ev[oi], stream), "pair event");
+    SK(cudaStreamWaitEvent(copy_stream, pair_ev[oi], 0), "copy wait");
+    SK(cudaMemcpyAsync(hout + offsets[oi], out + offsets[oi], sizeof(float) * n, cudaMemcpyDeviceToHost,
+                       copy_stream),
+       "output copy");
+    return ESRRF_OK;
+}
+
+// The compute stream waits for the last copy (joins copy_stream back, also inside a capture).
+esrrf_status Shard::copy_join(float* hout) {
+    Shard* s = this;
+    if (!hout) return ESRRF_OK;
+    SK(cudaEventRecord(copy_done, copy_stream), "copy event");
+    SK(cudaStreamWaitEvent(stream, copy_done, 0), "copy join");
+    return ESRRF_OK;
+}
+
+esrrf_status Shard::enqueue(const void* frames, int is_u16, float* out, float* hout) {
     Shard* s = this;
     const size_t fb = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)w * h;
     int launches = 0;
-    if (bic) return enqueue_bic(frames, is_u16, out);
+    if (bic) return enqueue_bic(frames, is_u16, out, hout);
     size_t oi = 0;
     for (size_t mi = 0; mi < mp.size(); ++mi) {
         const MagPlan& m = mp[mi];
@@ -272,13 +303,15 @@ esrrf_status Shard::enqueue(const void* frames, int is_u16, float* out) {
                     SK(cudaGetLastError(), "cumulants");
                     ++launches;
                 }
+            esrrf_status r = copy_pair(oi, out, hout);
+            if (r != ESRRF_OK) return r;
         }
     }
     launches_per_run = launches;
-    return ESRRF_OK;
+    return copy_join(hout);
 }
 
-esrrf_status Shard::enqueue_bic(const void* frames, int is_u16, float* out) {
+esrrf_status Shard::enqueue_bic(const void* frames, int is_u16, float* out, float* hout) {
     Shard* s = this;
     int launches = 0;
     SK(bic_prepare(frames, is_u16, w, h, T, d_fraw, d_gx, d_gy, d_gxi, d_gyi, stream), "gradients");
@@ -334,15 +367,18 @@ esrrf_status Shard::enqueue_bic(const void* frames, int is_u16, float* out) {
                 SK(mp_correct(base + q * 4 * P, w, h, 1, m.M, 0, d_mpmap, stream), "MP correction");
                 launches += 2;
             }
+            esrrf_status r = copy_pair(oi, out, hout);
+            if (r != ESRRF_OK) return r;
         }
     }
     launches_per_run = launches;
-    return ESRRF_OK;
+    return copy_join(hout);
 }
 
 void Shard::release() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     exec = nullptr;
@@ -370,6 +406,12 @@ void Shard::release() {
     cudaFree(d_outbuf);
     d_interp = d_cg = d_outbuf = nullptr;
     d_in = nullptr;
+    for (cudaEvent_t e : pair_ev) cudaEventDestroy(e);
+    pair_ev.clear();
+    if (copy_done) cudaEventDestroy(copy_done);
+    copy_done = nullptr;
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }
@@ -511,21 +553,29 @@ esrrf_status Shard::tc_check() {
     return ESRRF_OK;
 }
 
-esrrf_status Shard::run_device(const void* d_frames, int is_u16, float* d_out) {
+// h_out: a pinned host buffer in the shard's layout that the run also fills (each pair's outputs
+// copied while the next pairs compute), or null.
+esrrf_status Shard::run_device(const void* d_frames, int is_u16, float* d_out, float* h_out) {
     Shard* s = this;
     if (cudaSetDevice(device) != cudaSuccess) return fail(ESRRF_ERR_CUDA, "cudaSetDevice failed");
+    if (h_out && !copy_stream) {
+        SK(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "copy stream");
+        SK(cudaEventCreateWithFlags(&copy_done, cudaEventDisableTiming), "copy event");
+        pair_ev.assign(offsets.size(), nullptr);
+        for (auto& e : pair_ev) SK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "pair event");
+    }
     // The graph bakes in the input and output pointers: (re)capture when they change.
-    if (!exec || g_in != d_frames || g_out != d_out || g_u16 != is_u16) {
+    if (!exec || g_in != d_frames || g_out != d_out || g_hout != h_out || g_u16 != is_u16) {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
         graph = nullptr;
         // one uncaptured pass sets the kernels' shared-memory attributes and checks the launches
-        esrrf_status r = enqueue(d_frames, is_u16, d_out);
+        esrrf_status r = enqueue(d_frames, is_u16, d_out, h_out);
         if (r != ESRRF_OK) return r;
         SK(cudaStreamSynchronize(stream), "sweep warm-up");
         SK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        r = enqueue(d_frames, is_u16, d_out);
+        r = enqueue(d_frames, is_u16, d_out, h_out);
         cudaGraph_t g = nullptr;
         cudaError_t ce = cudaStreamEndCapture(stream, &g);
         if (r != ESRRF_OK) {
@@ -537,6 +587,7 @@ esrrf_status Shard::run_device(const void* d_frames, int is_u16, float* d_out) {
         SK(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
         g_in = d_frames;
         g_out = d_out;
+        g_hout = h_out;
         g_u16 = is_u16;
         SK(cudaStreamSynchronize(stream), "sweep");
         return tc_check();
@@ -894,6 +945,14 @@ esrrf_status esrrf_sweep_run(esrrf_sweep* s, const void* frames, int is_u16, flo
     if (!s || !frames || !out) return ESRRF_ERR_INVALID;
     const size_t fbytes = (is_u16 ? sizeof(uint16_t) : sizeof(float)) * (size_t)s->p.width * s->p.height;
     const bool direct = s->direct();
+    // a pinned output buffer of a one-shard sweep is filled pair by pair during the run
+    bool overlap = false;
+    if (direct && s->total > 0) {
+        cudaPointerAttributes a0{}, a1{};
+        overlap = cudaPointerGetAttributes(&a0, out) == cudaSuccess && a0.type == cudaMemoryTypeHost &&
+                  cudaPointerGetAttributes(&a1, out + s->total - 1) == cudaSuccess && a1.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+    }
     std::vector<esrrf_status> rs(s->shards.size(), ESRRF_OK);
     auto work = [&](size_t i) -> esrrf_status {
         Shard* sh = s->shards[i];
@@ -902,6 +961,7 @@ esrrf_status esrrf_sweep_run(esrrf_sweep* s, const void* frames, int is_u16, flo
         if (!sh->d_outbuf) SKS(cudaMalloc(&sh->d_outbuf, sizeof(float) * sh->total), "output buffer");
         SKS(cudaMemcpyAsync(sh->d_in, (const unsigned char*)frames + fbytes * sh->f0, fbytes * sh->T,
                             cudaMemcpyHostToDevice, sh->stream), "input copy");
+        if (overlap) return sh->run_device(sh->d_in, is_u16, sh->d_outbuf, out);
         esrrf_status r = sh->run_device(sh->d_in, is_u16, sh->d_outbuf);
         if (r != ESRRF_OK) return r;
         if (direct) {

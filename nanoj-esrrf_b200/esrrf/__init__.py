@@ -407,7 +407,10 @@ class Sweep:
                           for c, name in enumerate(("AVG", "VAR", "TAC2"))}
         return out
 
-    def run(self, stack):
+    def run(self, stack, out=None):
+        """Runs the sweep on host frames.  ``out``: optional flat float32 array of ``self.total``
+        floats to fill (e.g. the numpy view of a pinned torch tensor: a one-device sweep then copies
+        each (magnification, radius) pair's outputs out while the next pairs compute)."""
         a = np.asarray(stack)
         if a.dtype == np.uint16:
             a = np.ascontiguousarray(a)
@@ -415,7 +418,12 @@ class Sweep:
         else:
             a = np.ascontiguousarray(a, np.float32)
             is_u16 = 0
-        flat = np.empty(self.total, np.float32)
+        if out is None:
+            flat = np.empty(self.total, np.float32)
+        else:
+            flat = out
+            if flat.dtype != np.float32 or flat.size != self.total or not flat.flags.c_contiguous:
+                raise EsrrfError("out must be a contiguous float32 array of the sweep's total size")
         _lib.check(self._h, lib().esrrf_sweep_run(self._h, a.ctypes.data_as(ctypes.c_void_p), is_u16,
                                                   flat.ctypes.data_as(ctypes.c_void_p)), sweep=True)
         return self.unpack(flat)
