@@ -787,6 +787,10 @@ esrrf_status esrrf_set_drift(esrrf_handle* h, const float* dx, const float* dy, 
     if (!h) return ESRRF_ERR_INVALID;
     if (n != h->p.n_frame_for_srrf && !(n == 0 && !dx && !dy))
         return h->fail(ESRRF_ERR_INVALID, "drift arrays must hold n_frame_for_srrf values");
+    // the kernels turn shifts x M into integer tile offsets: finite and at most 1e6 raw pixels
+    for (int i = 0; i < n; ++i)
+        if ((dx && !(std::fabs(dx[i]) <= 1e6f)) || (dy && !(std::fabs(dy[i]) <= 1e6f)))
+            return h->fail(ESRRF_ERR_INVALID, "drift shifts must be finite and at most 1e6 pixels");
     return h->set_drift(dx, dy);
 }
 

@@ -31,6 +31,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -759,6 +760,10 @@ esrrf_status validate(const esrrf_sweep_params* sp) {
     if (sp->interp != ESRRF_INTERP_FHT && sp->interp != ESRRF_INTERP_BIC) return reject("unknown interpolation");
     if ((sp->drift_x == nullptr) != (sp->drift_y == nullptr))
         return reject("drift_x and drift_y must both be given or both be NULL");
+    if (sp->drift_x)
+        for (int t = 0; t < sp->n_frames; ++t)
+            if (!(std::fabs(sp->drift_x[t]) <= 1e6f) || !(std::fabs(sp->drift_y[t]) <= 1e6f))
+                return reject("drift shifts must be finite and at most 1e6 pixels");
     if (sp->drift_x && sp->interp == ESRRF_INTERP_BIC)
         return reject("drift correction is available in the FHT sweep only (run the bicubic engine per block)");
     if (sp->n_devices < 0 || (sp->n_devices > 0 && !sp->devices)) return reject("bad device list");

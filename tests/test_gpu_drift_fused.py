@@ -145,3 +145,24 @@ def test_rolling_with_per_block_drift(esrrf_mod, oracle_mod):
         res = esrrf_mod.rolling(raw, 4, 1.5, 2, blocks, drift=drift)
         for (st, ln), (dx, dy) in zip(blocks, drift):
             check(res[(st, ln)], ref_block(oracle_mod, interp[st:st + ln], 4, 1.5, 2, dx, dy), f"{blocks}")
+
+
+def test_non_finite_shift_is_rejected(esrrf_mod):
+    """loadDriftXYGPUbuffer with a NaN or an infinite shift is an error, and the handle keeps
+    working with valid shifts afterwards."""
+    from esrrf import EsrrfError, synth
+    raw = synth.small_stack(81, 6, 16, 16, emitters=4)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(16, 16, 2, 1.5, 1, 6, 6)
+    try:
+        for bad in (np.nan, np.inf):
+            dx = np.zeros(6, np.float32)
+            dx[2] = bad
+            with pytest.raises(EsrrfError, match="finite"):
+                eng.loadDriftXYGPUbuffer(dx, np.zeros(6, np.float32))
+        eng.resetFramePosition()
+        eng.loadDriftXYGPUbuffer(np.full(6, 0.25, np.float32), np.zeros(6, np.float32))
+        assert not eng.calculateSRRF(raw)
+        assert np.isfinite(eng.readSRRFbuffer()).all()
+    finally:
+        eng.release()

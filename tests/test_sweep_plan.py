@@ -150,3 +150,18 @@ def test_two_rank_sharded_rolling_gathers_the_single_device_layout(esrrf_mod):
     interp = O.fht_interpolate(raw, 2)
     for b, (st, ln) in enumerate(blocks):
         np.testing.assert_array_equal(full[b], O.fht_block(interp[st:st + ln], 2, 1.5, 2))
+
+
+def test_non_finite_or_huge_drift_is_rejected(esrrf_mod):
+    """Shifts become integer tile offsets in the kernels: NaN, infinite or beyond 1e6 pixels is an
+    error before any device work (validation is host arithmetic, as esrrf_sweep_plan runs it)."""
+    import ctypes
+
+    from esrrf import EsrrfError, _lib
+    for bad in (np.nan, np.inf, 2e6):
+        sw = esrrf_mod.Sweep.__new__(esrrf_mod.Sweep)
+        dx = np.zeros(10, np.float32)
+        dx[3] = bad
+        p = sw._params(16, 16, 10, [2], [1.0], [1], [(0, 10)], True, -1, "fht", (np.zeros(10), dx), None)
+        with pytest.raises(EsrrfError, match="finite"):
+            _lib.check(None, esrrf_mod.lib().esrrf_sweep_plan(ctypes.byref(p), None, None, None), sweep=True)
