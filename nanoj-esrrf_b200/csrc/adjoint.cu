@@ -822,6 +822,7 @@ esrrf_status esrrf_adjoint::forward(const float* frames, float fwhm, float sens,
     esrrf_status r = set_radius(fwhm);
     if (r != ESRRF_OK) return r;
     if (!(sigma_b > 0.f) || 4.0 * sigma_b > (kMaxGauss - 1) / 2) return fail(ESRRF_ERR_INVALID, "sigma out of range");
+    if (!(sens >= 0.f) || sens > 64.f) return fail(ESRRF_ERR_INVALID, "sensitivity must be in [0, 64]");
     const long P = (long)WM * HM, p = (long)w * h;
     frame_mean_kernel<<<(unsigned)((p + 255) / 256), 256, 0, stream>>>(frames, T, p, Fm);
     for (int t = 0; t < T; t += Fc) {
