@@ -13,6 +13,11 @@ FFT form of FourierInterpolation.java's map.
 * The fidelity-loss adjoint at M4 (the 256 x 256 x 100 workload's magnification, 18-wide tap box)
   on a 48 x 48 x 8 stack: radius, sensitivity, re-blur sigma and pixel gradients against central
   finite differences (h = 1e-3) of the float64 loss.
+* The bicubic path on 512 x 512 uint16 frames at M4, radius 1.5, S2 with MP correction (the bicubic
+  workload), 3 frames in launches of 2, against liveSRRF.cl compiled for the host.
+* The 3-D path on 9 planes of 128 x 128 at M3, radius 1.5, S1 with per-plane alignment and MP
+  correction (the 3-D workload's planes, calibration and parameters), 3 timepoints in launches of 2,
+  against live3DSRRF.cl compiled for the host.
 
 Tolerance: each slice within 1e-4 of its dynamic range; gradients within 1e-3 relative (pixel
 gradients with a floor at 20 % of the largest one checked).
@@ -93,3 +98,37 @@ def test_adjoint_at_m4_against_finite_differences(esrrf_mod):
     scale = max(abs(v) for v in fd["pixels"].values())
     for (t, y, x), v in fd["pixels"].items():
         assert abs(gf[t, y, x] - v) <= 1e-3 * max(abs(v), 0.2 * scale), ((t, y, x), gf[t, y, x], v)
+
+
+def test_bicubic_headline_frame_size_against_reference_kernels(esrrf_mod, oracle_mod):
+    from esrrf import synth
+    from test_gpu_bic3d import assert_close, run
+    raw = synth.make_stack("fht512", frames=3)
+    got, _ = run(esrrf_mod, raw, 4, 1.5, 2, mp=True, fht=False, frames_per_launch=2)
+    if oracle_mod.ref_available():
+        ref = oracle_mod.ref_bic_block(raw, 4, 1.5, 2, mp_correction=True, frames_per_load=2)
+    else:
+        ref = oracle_mod.bic_block(raw.astype(np.float32), 4, 1.5, 2, mp_correction=True)
+    assert np.abs(ref[2]).max() > 0
+    assert_close(got, ref, "bicubic 512x512 M4")
+
+
+def test_3d_workload_size_against_reference_kernels(esrrf_mod, oracle_mod):
+    from esrrf import synth
+    from test_gpu_bic3d import assert_close, calib, run, tile_planes
+    planes = synth.make_stack("mfm3d", frames=3)
+    n, P, h, w = planes.shape
+    assert (P, h, w) == (9, 128, 128)
+    roi = np.array([4, 0, 1, 2, 3, 5, 6, 7, 8], np.float32)
+    theta = np.linspace(-0.5, 0.5, P).astype(np.float32)
+    sx = np.linspace(-0.2, 0.2, P).astype(np.float32)
+    sy = np.linspace(0.1, -0.1, P).astype(np.float32)
+    got, _ = run(esrrf_mod, tile_planes(planes.astype(np.float32), roi), 3, 1.5, 1, mp=True,
+                 calib=calib(P, theta, sx, sy, roi), frames_per_launch=2)
+    if oracle_mod.ref_available():
+        ref = oracle_mod.ref_3d_block(planes, 3, 1.5, 1, theta, sx, sy, mp_correction=True,
+                                      frames_per_load=2)
+    else:
+        ref = oracle_mod.block3d(planes.astype(np.float32), 3, 1.5, 1, theta, sx, sy, mp_correction=True)
+    assert got.shape == (4 * P * 3, h * 3, w * 3)
+    assert_close(got, ref, "3-D 9 x 128 x 128 M3")
