@@ -49,3 +49,14 @@ def test_a_changed_kernel_makes_its_summary_stale(bench, monkeypatch):
     msg = bench.summary_stale("rgc_fused_fht512")
     assert msg and "re-capture" in msg
     assert bench.summary_stale("rgc_fused_bic512") is None
+
+
+@pytest.mark.parametrize("world", [1, 2, 4, 8])
+def test_ranks_take_disjoint_contiguous_runs_of_blocks(bench, esrrf_mod, world):
+    """Under torchrun each rank reconstructs its run of blocks of a world-size times longer stack
+    (weak scaling); the runs come from the library's planner, cover every block once, are
+    contiguous, and all have the length of the one-GPU workload (5 blocks of 100 frames)."""
+    runs = [bench.shard_blocks(world, r, 5, 100) for r in range(world)]
+    assert sorted(b for run in runs for b in run) == list(range(5 * world))
+    for run in runs:
+        assert len(run) == 5 and run == list(range(run[0], run[0] + 5))
