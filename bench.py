@@ -489,6 +489,94 @@ def read_traffic_summary(kernel, key="traffic_bytes_per_launch"):
     return None
 
 
+def secondary_metrics(stack, nf, M, fwhm, S, local, value):
+    """The other two figures of the headline metric, measured live on this GPU after the headline
+    line's timed regions (bounded: about 10 s): the plain per-pixel kernel on one block of the same
+    stack (fused vs plain), the batched sweep of the sweep workload (one graph replay, combos/s)
+    and the adjoint of the differentiable workload ((loss + gradients - loss) / loss).  Each is
+    timed with CUDA events on the current stream; the calls return after their own streams drained."""
+    import ctypes
+
+    import torch
+
+    import esrrf
+    from esrrf import synth
+
+    L = esrrf.lib()
+
+    def timed(fn, reps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(reps):
+            fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / 1000.0 / reps
+
+    out = {}
+    # plain kernel, one block of the headline stack
+    h, w = stack.shape[1:]
+    eng = esrrf.LiveSRRF_CL()
+    eng.initialise(w, h, M, fwhm, S, nf, nf, chosenDevice=local, kernel="plain")
+    try:
+        H = eng.handle
+        d_blk = torch.from_numpy(np.ascontiguousarray(stack[:nf]).view(np.int16)).to(f"cuda:{local}")
+        d_o = torch.empty((4, h * M, w * M), dtype=torch.float32, device=f"cuda:{local}")
+
+        def block():
+            esrrf._lib.check(H, L.esrrf_reset_frame_position(H))
+            esrrf._lib.check(H, L.esrrf_calculate_srrf_u16_device(H, ctypes.c_void_p(d_blk.data_ptr()), nf))
+            esrrf._lib.check(H, L.esrrf_read_srrf_device(H, ctypes.c_void_p(d_o.data_ptr())))
+
+        block()
+        t = timed(block, 1)
+        plain = nf * h * w / 1e6 / t
+        out["plain"] = {"value": plain, "unit": "Mpx*frames/s", "sample": f"one block of {nf} frames",
+                        "fused_over_plain": value / plain}
+    finally:
+        eng.release()
+    del d_blk, d_o
+    # batched sweep: 88 combinations x 4 uneven blocks of 256x256x200, one captured graph
+    sst = synth.make_stack("sweep256")
+    n, sh, sw_ = sst.shape
+    sw = esrrf.Sweep(sw_, sh, n, SWEEP_MAGS, SWEEP_RADII, SWEEP_SENS, SWEEP_BLOCKS, device=local)
+    try:
+        d_s = torch.from_numpy(sst.view(np.int16)).to(f"cuda:{local}")
+        d_so = torch.empty(sw.total, dtype=torch.float32, device=f"cuda:{local}")
+
+        def sweep():
+            esrrf._lib.check(sw.handle, L.esrrf_sweep_run_device(
+                sw.handle, ctypes.c_void_p(d_s.data_ptr()), 1, ctypes.c_void_p(d_so.data_ptr())), sweep=True)
+
+        sweep()  # captures the graph
+        combos = len(SWEEP_MAGS) * len(SWEEP_RADII) * len(SWEEP_SENS)
+        t = timed(sweep, 2)
+        out["sweep"] = {"value": combos / t, "unit": "combos/s", "ms_per_run": t * 1e3,
+                        "workload": "sweep256: 256x256x200, 88 combinations, blocks [0,37) [37,101) "
+                                    "[101,200) [0,100), device-resident"}
+    finally:
+        sw.release()
+    del d_s, d_so
+    # adjoint: loss + all gradients against the loss alone, 256x256x100 at M4
+    ast = synth.make_stack("adjoint256").astype(np.float32)
+    n, ah, aw = ast.shape
+    adj = esrrf.Adjoint(aw, ah, n, 4, device=local)
+    try:
+        d_a = torch.from_numpy(ast).to(f"cuda:{local}")
+        x0 = (1.5, 2.0, 1.5)
+        adj.loss(d_a, *x0)
+        adj.loss_and_grad(d_a, *x0)
+        t_f = timed(lambda: adj.loss(d_a, *x0), 3)
+        t_fb = timed(lambda: adj.loss_and_grad(d_a, *x0), 3)
+        out["adjoint"] = {"value": (t_fb - t_f) / t_f, "unit": "ratio (loss+grad - loss) / loss",
+                          "forward_ms": t_f * 1e3, "loss_and_grad_ms": t_fb * 1e3,
+                          "workload": "adjoint256: 256x256x100, M4, AVG"}
+    finally:
+        adj.release()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import ctypes
 
@@ -630,6 +718,11 @@ def run_ours(args, world, rank, local):
     achieved_tflops = ops_launch / avg_launch_s / 1e12
     cpu = (cpu_reference_sample(stack, M, fwhm, S, 2 if bic else 1, bic=bic)
            if not args.no_cpu_baseline and world == 1 else None)
+    # the headline metric's other figures (fused vs plain, sweep combos/s, adjoint / forward), on
+    # the full default workload only
+    secondary = (secondary_metrics(stack, nf, M, fwhm, S, local, value)
+                 if (world == 1 and args.workload == "fht512" and args.kernel == "fused" and not args.drift
+                     and args.frames is None and not args.block and not args.no_cpu_baseline) else None)
     summary_key = f"rgc_{args.kernel}_{args.workload}" + ("_drift" if args.drift else "")
     stale = summary_stale(summary_key)
     traffic = None if stale else read_traffic_summary(summary_key)
@@ -686,6 +779,8 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "wall_s_timed": wall,
     }
+    if secondary:
+        line["secondary"] = secondary
     print(json.dumps(line))
 
 
@@ -1205,7 +1300,8 @@ def main():
     ap.add_argument("--workload", default="fht512", choices=sorted(WORKLOADS))
     ap.add_argument("--kernel", default="fused", choices=["fused", "plain"])
     ap.add_argument("--frames-per-launch", type=int, default=0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="quick run: no CPU reference sample and no secondary metrics (profiling runs)")
     ap.add_argument("--frames", type=int, default=None,
                     help="shorter stack (profiling runs); default: the workload's length")
     ap.add_argument("--block", type=int, default=0, help="frames per block override")
