@@ -595,7 +595,7 @@ cudaError_t interp_run(const InterpPlan& p, InterpScratch& sc, const void* raw, 
             sc.vec);
     }
     if (p.tc) {
-        if (launches) *launches += 4;
+        if (launches) *launches += 5;  // sums, rank-one vectors, split operands, two passes
         cudaError_t e = cudaGetLastError();
         return e != cudaSuccess ? e : tc_interp_passes(p, sc, raw, is_u16, F, out, stream);
     }
