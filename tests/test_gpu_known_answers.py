@@ -2,7 +2,7 @@
 cosine whose period divides the frame size comes out of the Fourier interpolation (tensor-core and
 SIMT forms) exactly on the fine grid; a radially symmetric spot gives its RGC maximum at the spot
 centre and a map symmetric under x <-> y around it; TAC2 of independent frames averages to ~0 while their
-VAR does not."""
+VAR does not; a constant stack gives zero convergence on every path."""
 import numpy as np
 import pytest
 
@@ -56,3 +56,28 @@ def test_tac2_of_independent_frames_is_small(esrrf_mod):
     var, tac2 = out[1][8:-8, 8:-8], out[2][8:-8, 8:-8]
     assert var.mean() > 0
     assert abs(tac2.mean()) < 0.05 * var.mean(), (tac2.mean(), var.mean())
+
+
+def test_constant_frames_give_zero_convergence(esrrf_mod):
+    """A constant stack has a zero gradient everywhere, so no tap is inward: CGLH = 0, hence AVG,
+    VAR and TAC2 are 0, and INT is the constant -- on the FHT path (a frame that needs mirror
+    padding: the interpolation of a constant is the constant), the bicubic path with and without
+    MP correction, and the 3-D path."""
+    from test_gpu_bic3d import calib, run, tile_planes
+    c = 123.0
+    frames = np.full((5, 48, 64), c, np.float32)
+    fht = block(esrrf_mod, frames, 4, 1.5, 2)
+    assert np.abs(fht[:3]).max() == 0.0
+    np.testing.assert_allclose(fht[3], c, rtol=1e-6)
+    for mp in (False, True):
+        bic, _ = run(esrrf_mod, frames, 3, 1.5, 1, mp=mp, fht=False)
+        assert np.abs(bic[:3]).max() == 0.0, mp
+        np.testing.assert_allclose(bic[3], c, rtol=1e-5)
+    P = 5
+    planes = np.full((4, P, 24, 20), c, np.float32)
+    roi = np.array([4, 0, 8, 5, 1], np.float32)
+    zeros = np.zeros(P, np.float32)
+    v3d, _ = run(esrrf_mod, tile_planes(planes, roi), 3, 1.5, 1, mp=False, calib=calib(P, zeros, zeros, zeros, roi))
+    v3d = v3d.reshape(4, -1)
+    assert np.abs(v3d[:3]).max() == 0.0
+    np.testing.assert_allclose(v3d[3], c, rtol=1e-5)
