@@ -204,8 +204,11 @@ def dist_setup():
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        # NCCL between GPUs; ESRRF_BENCH_BACKEND=gloo runs the barrier and the max over ranks on the
+        # host (ranks sharing one GPU for a functional check: no kernel waits on another rank)
+        backend = os.environ.get("ESRRF_BENCH_BACKEND", "nccl")
+        kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
     return world, rank, local
 
 
@@ -222,7 +225,8 @@ def max_over_ranks(world, x):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
