@@ -109,7 +109,9 @@ esrrf_status esrrf_device_info(int device, char* name, size_t name_len, int* sm_
 void esrrf_default_params(esrrf_params* p);
 
 /* Replaces LiveSRRF_CL.initialise (LiveSRRF_CL.java:159-264) and its buffer/program set-up
- * (prepareBuffersFHTinterpolation :462-579, prepareBuffersBICinterpolation :266-459). */
+ * (prepareBuffersFHTinterpolation :462-579, prepareBuffersBICinterpolation :266-459).  Sizes:
+ * width, height >= 4; one output slice (widthM x heightM, in 3-D times planes x M) below 2^31
+ * pixels. */
 esrrf_status esrrf_create(const esrrf_params* params, esrrf_handle** out);
 
 /* Replaces LiveSRRF_CL.release (LiveSRRF_CL.java:939-951). */

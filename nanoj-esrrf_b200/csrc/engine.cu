@@ -63,6 +63,15 @@ esrrf_status validate(const esrrf_params& p, std::string& msg) {
     }
     if (p.interp != ESRRF_INTERP_FHT && p.interp != ESRRF_INTERP_BIC)
         return msg = "interp must be ESRRF_INTERP_FHT or ESRRF_INTERP_BIC", ESRRF_ERR_INVALID;
+    // one output slice (2-D frame, or 3-D volume of the 3 x 3 camera tiles' planes) must index in
+    // 32 bits: the kernels' per-slice offsets are ints
+    const long long M = p.magnification;
+    const long long slice = p.n_planes > 0 ? (p.width / 3) * M * ((p.height / 3) * M) * (p.n_planes * M)
+                                           : p.width * M * (p.height * M);
+    if (slice > 2147483647LL)
+        return msg = "output too large: width x height x magnification^2 (x planes x magnification in 3-D) "
+                     "must stay below 2^31 pixels per slice",
+               ESRRF_ERR_INVALID;
     return ESRRF_OK;
 }
 

@@ -751,8 +751,12 @@ esrrf_status validate(const esrrf_sweep_params* sp) {
         if (sp->block_start[b] < 0 || sp->block_length[b] < 1 ||
             sp->block_start[b] + sp->block_length[b] > sp->n_frames)
             return reject("block " + std::to_string(b) + " lies outside the stack");
-    for (int i = 0; i < sp->n_mag; ++i)
+    for (int i = 0; i < sp->n_mag; ++i) {
         if (sp->magnifications[i] < 1 || sp->magnifications[i] > 16) return reject("magnification out of range");
+        const long long M = sp->magnifications[i];
+        if ((long long)sp->width * M * ((long long)sp->height * M) > 2147483647LL)
+            return reject("output too large: width x height x magnification^2 must stay below 2^31 pixels");
+    }
     for (int i = 0; i < sp->n_radius; ++i)
         if (!(sp->radii[i] > 0.f) || sp->radii[i] > 20.f) return reject("radius out of range");
     for (int i = 0; i < sp->n_sens; ++i)

@@ -78,6 +78,9 @@ def test_invalid_parameters_are_rejected_before_device_work(esrrf_mod):
     assert L.esrrf_create(ctypes.byref(p), ctypes.byref(h)) == -1
     p.n_frame_for_srrf, p.n_planes = 10, 3  # 3-D without calibration arrays
     assert L.esrrf_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    p.n_planes, p.width, p.height, p.magnification = 0, 12000, 12000, 4  # 48000^2 output pixels
+    assert L.esrrf_create(ctypes.byref(p), ctypes.byref(h)) == -1
+    assert b"too large" in L.esrrf_last_error(None)
 
 
 def test_null_handles_are_rejected(esrrf_mod):
@@ -133,3 +136,10 @@ def test_sweep_rejects_bad_parameters_before_any_device_work(esrrf_mod):
     assert rc == invalid and "outside the stack" in msg
     rc, msg = create(n_radius=0)
     assert rc == invalid and "non-empty" in msg
+    mags[0] = 16
+    p = _lib.EsrrfSweepParams(4000, 4000, 10, 1, ctypes.cast(mags, ip), 1, ctypes.cast(radii, fp), 1,
+                              ctypes.cast(sens, ip), 1, ctypes.cast(bs, ip), ctypes.cast((ctypes.c_int * 1)(10), ip),
+                              1, -1, 0)
+    h = ctypes.c_void_p()
+    assert esrrf_mod.lib().esrrf_sweep_create(ctypes.byref(p), ctypes.byref(h)) == invalid
+    assert "too large" in esrrf_mod.lib().esrrf_sweep_last_error(None).decode()
