@@ -18,6 +18,7 @@ FFT form of FourierInterpolation.java's map.
 * The 3-D path on 9 planes of 128 x 128 at M3, radius 1.5, S1 with per-plane alignment and MP
   correction (the 3-D workload's planes, calibration and parameters), 3 timepoints in launches of 2,
   against live3DSRRF.cl compiled for the host.
+* 1024 x 1024 frames at M4 (4096 x 4096 output), the largest tested, against the reference kernels.
 
 Tolerance: each slice within 1e-4 of its dynamic range; gradients within 1e-3 relative (pixel
 gradients with a floor at 20 % of the largest one checked).
@@ -132,3 +133,26 @@ def test_3d_workload_size_against_reference_kernels(esrrf_mod, oracle_mod):
         ref = oracle_mod.block3d(planes.astype(np.float32), 3, 1.5, 1, theta, sx, sy, mp_correction=True)
     assert got.shape == (4 * P * 3, h * 3, w * 3)
     assert_close(got, ref, "3-D 9 x 128 x 128 M3")
+
+
+def test_large_frames_against_reference_kernels(esrrf_mod, oracle_mod):
+    """1024 x 1024 uint16 frames at M4 (padded size 1024, 4096 x 4096 output): the largest frames
+    of these tests, through the tensor-core interpolation and the fused kernel (2 frames in one
+    launch), against the reference kernels on the float64 FFT interpolation."""
+    from esrrf import synth
+    wl = synth.Workload("big", 1024, 1024, 2, 4, 1.5, 2, emitters=4000, filaments=30, seed=77)
+    raw = synth.make_stack(wl)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(1024, 1024, 4, 1.5, 2, 2, 2)
+    try:
+        eng.resetFramePosition()
+        assert not eng.calculateSRRF(raw)
+        got = eng.readSRRFbuffer().copy()
+    finally:
+        eng.release()
+    interp = oracle_mod.fht_interpolate_fft(raw.astype(np.float32), 4)
+    assert rel_err(got[3], interp.mean(axis=0)) < 2e-6
+    ref = _ref_block(oracle_mod, interp, 4, 1.5, 2)
+    for k in range(4):
+        e = rel_err(got[k], ref[k])
+        assert e < TOL, f"slice {k}: {e:.3g} of range"
