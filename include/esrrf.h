@@ -196,6 +196,13 @@ esrrf_status esrrf_finish_queue(esrrf_handle* h);
 /* Thread-safe cancellation (replaces the IJ.escapePressed() polling, LiveSRRF_CL.java:731-734). */
 esrrf_status esrrf_request_cancel(esrrf_handle* h);
 
+/* Diagnostic of the device-side failure detection (no counterpart in the reference, whose
+ * OpenCL waits are host-side queue.finish() calls): runs the tensor-core passes' bounded
+ * mbarrier wait, with a limit of `cycles` SM clock cycles (1 .. 1e9), on a barrier that receives
+ * its one arrival (arrive = 1: ESRRF_OK) or none (arrive = 0: the wait gives up, records it in a
+ * device flag as the passes do, and the host reads ESRRF_ERR_TIMEOUT).  The context stays usable. */
+esrrf_status esrrf_check_bounded_wait(int device, int arrive, long long cycles);
+
 /* Message of the last failure on h (or of the last failed esrrf_create when h is NULL). */
 const char* esrrf_last_error(const esrrf_handle* h);
 

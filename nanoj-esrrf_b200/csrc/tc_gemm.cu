@@ -28,6 +28,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../../include/esrrf.h"
 #include "esrrf_internal.h"
 
 namespace esrrf {
@@ -85,11 +86,12 @@ __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the completion of the mbarrier phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
+// Bounded wait for the completion of the mbarrier phase with the given parity: false once
+// `limit` SM cycles have passed without it.
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, long long limit = TC_WAIT_CYCLES) {
     if (mbar_try(addr, parity)) return true;
     const long long t0 = clock64();
-    while (clock64() - t0 < TC_WAIT_CYCLES)
+    while (clock64() - t0 < limit)
         if (mbar_try(addr, parity)) return true;
     return false;
 }
@@ -797,4 +799,50 @@ cudaError_t tc_interp_passes(const InterpPlan& p, InterpScratch& sc, const void*
     return cudaGetLastError();
 }
 
+namespace {
+
+// The GEMM roles' bounded wait and failure record on a barrier of one expected arrival: with
+// arrive = 1 the phase completes and the wait returns at once; with arrive = 0 nothing arrives, so
+// the wait gives up after `limit` cycles and records it in the flag, as a GEMM role does.
+__global__ void wait_check_kernel(long long limit, int arrive, int* __restrict__ err) {
+    __shared__ __align__(8) unsigned long long bar;
+    const uint32_t a = smem_u32(&bar);
+    mbar_init(a, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (arrive) mbar_arrive(a);
+    if (!mbar_wait(a, 0, limit)) atomicExch(err, 1);
+}
+
+}  // namespace
+
 }  // namespace esrrf
+
+extern "C" esrrf_status esrrf_check_bounded_wait(int device, int arrive, long long cycles) {
+    using namespace esrrf;
+    if (cycles < 1 || cycles > 1000000000LL) return ESRRF_ERR_INVALID;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return ESRRF_ERR_NODEVICE;
+    }
+    if (device < 0 || device >= n) return ESRRF_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return ESRRF_ERR_CUDA;
+    int* d_err = nullptr;
+    if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return ESRRF_ERR_NOMEM;
+    }
+    int flag = 0;
+    cudaError_t e = cudaMemset(d_err, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        wait_check_kernel<<<1, 1>>>(cycles, arrive ? 1 : 0, d_err);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ESRRF_ERR_CUDA;
+    }
+    return flag ? ESRRF_ERR_TIMEOUT : ESRRF_OK;
+}

@@ -71,6 +71,7 @@ SIGNATURES = {
     "esrrf_read_gradients": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_size_t]),
     "esrrf_finish_queue": (_c.c_int, [_c.c_void_p]),
     "esrrf_request_cancel": (_c.c_int, [_c.c_void_p]),
+    "esrrf_check_bounded_wait": (_c.c_int, [_c.c_int, _c.c_int, _c.c_longlong]),
     "esrrf_last_error": (_c.c_char_p, [_c.c_void_p]),
     "esrrf_set_timing": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "esrrf_set_stream": (_c.c_int, [_c.c_void_p, _c.c_void_p]),

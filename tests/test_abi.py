@@ -89,6 +89,9 @@ def test_null_handles_are_rejected(esrrf_mod):
     assert L.esrrf_reset_frame_position(None) == -1
     assert L.esrrf_read_srrf(None, None) == -1
     assert L.esrrf_request_cancel(None) == -1
+    # the bounded-wait diagnostic checks its limit before any device work
+    assert L.esrrf_check_bounded_wait(0, 0, 0) == -1
+    assert L.esrrf_check_bounded_wait(0, 0, 2_000_000_000) == -1
 
 
 def test_no_cpu_fallback_without_library(monkeypatch):
