@@ -46,6 +46,7 @@ class LiveSRRF_CL:
         self.widthS = self.heightS = 0
         self.nPlanes = self.nPlanesM = 1
         self._shape = None
+        self._frame_shape = None
 
     # -- LiveSRRF_CL.checkDevices (LiveSRRF_CL.java:111-155)
     def checkDevices(self) -> list[str]:
@@ -127,6 +128,7 @@ class LiveSRRF_CL:
         _lib.check(h, lib().esrrf_output_shape(h, ctypes.byref(wm), ctypes.byref(hm),
                                                ctypes.byref(pm)))
         self._shape = (wm.value, hm.value, pm.value)
+        self._frame_shape = (int(height), int(width))
         M = int(magnification)
         self.widthS, self.heightS = wm.value // M, hm.value // M
         self.nPlanesM = pm.value
@@ -147,6 +149,13 @@ class LiveSRRF_CL:
     # -- LiveSRRF_CL.calculateSRRF (LiveSRRF_CL.java:636-746); True if cancelled
     def calculateSRRF(self, imsRawData) -> bool:
         a = np.asarray(imsRawData)
+        if self._frame_shape is None:
+            raise EsrrfError("calculateSRRF before initialise")
+        if a.ndim == 2:  # one frame
+            a = a[None]
+        if a.ndim != 3 or tuple(a.shape[1:]) != self._frame_shape:
+            raise EsrrfError(f"frames must be [n][{self._frame_shape[0]}][{self._frame_shape[1]}] "
+                             f"(height, width of initialise), got {list(a.shape)}")
         if a.dtype == np.uint16:
             a = np.ascontiguousarray(a)
             rc = lib().esrrf_calculate_srrf_u16(self._h, a.ctypes.data_as(ctypes.c_void_p),
@@ -412,6 +421,8 @@ class Sweep:
         floats to fill (e.g. the numpy view of a pinned torch tensor: a one-device sweep then copies
         each (magnification, radius) pair's outputs out while the next pairs compute)."""
         a = np.asarray(stack)
+        if tuple(a.shape) != (self.n_frames, self.height, self.width):
+            raise EsrrfError(f"stack must be [{self.n_frames}][{self.height}][{self.width}], got {list(a.shape)}")
         if a.dtype == np.uint16:
             a = np.ascontiguousarray(a)
             is_u16 = 1

@@ -170,3 +170,26 @@ def test_small_frames_split_into_frame_groups(esrrf_mod, oracle_mod):
     assert_close(grouped, ref, what="grouped vs oracle")
     assert_close(grouped, single, tol=1e-5, what="grouped vs one group")
     assert np.abs(grouped[2]).max() > 0
+
+
+def test_frames_of_the_wrong_size_are_rejected(esrrf_mod):
+    """calculateSRRF checks the stack's frame size against initialise's (the library reads
+    n x height x width values from the pointer it is given); a single 2-D frame is one frame."""
+    from esrrf import EsrrfError, synth
+    raw = synth.small_stack(26, 4, 24, 32)
+    eng = esrrf_mod.LiveSRRF_CL()
+    eng.initialise(32, 24, 2, 1.5, 1, 4, 4)
+    try:
+        eng.resetFramePosition()
+        with pytest.raises(EsrrfError, match="frames must be"):
+            eng.calculateSRRF(raw[:, :, :16])
+        with pytest.raises(EsrrfError, match="frames must be"):
+            eng.calculateSRRF(raw.transpose(0, 2, 1))
+        for t in range(4):
+            assert not eng.calculateSRRF(raw[t])
+        one = eng.readSRRFbuffer().copy()
+    finally:
+        eng.release()
+    ref = run_engine(esrrf_mod, raw, 2, 1.5, 1)  # the same block in one push
+    for k in range(4):
+        assert rel_err(one[k], ref[k]) < 1e-6, k

@@ -163,3 +163,17 @@ def test_pinned_output_is_filled_during_the_run(esrrf_mod):
                     np.testing.assert_array_equal(got[key], ref[key], err_msg=f"{interp} {key}")
         finally:
             sw.release()
+
+
+def test_stack_of_the_wrong_shape_is_rejected(esrrf_mod):
+    from esrrf import EsrrfError, synth
+    raw = synth.small_stack(58, 10, 16, 20, emitters=4)
+    sw = esrrf_mod.Sweep(20, 16, 10, [2], [1.5], [1], [(0, 10)])
+    try:
+        with pytest.raises(EsrrfError, match="stack must be"):
+            sw.run(raw[:9])
+        with pytest.raises(EsrrfError, match="stack must be"):
+            sw.run(raw.transpose(0, 2, 1))
+        assert len(sw.run(raw)) == 1
+    finally:
+        sw.release()
