@@ -725,7 +725,8 @@ class Adjoint:
             t = frames.to(device=f"cuda:{self.device}", dtype=torch.float32).contiguous()
         else:
             t = torch.from_numpy(np.ascontiguousarray(frames, np.float32)).to(f"cuda:{self.device}")
-        assert tuple(t.shape) == self.shape, (tuple(t.shape), self.shape)
+        if tuple(t.shape) != self.shape:
+            raise EsrrfError(f"frames must be {list(self.shape)}, got {list(t.shape)}")
         return t
 
     def loss(self, frames, fwhm, sensitivity, sigma):
