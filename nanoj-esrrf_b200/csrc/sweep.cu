@@ -89,9 +89,8 @@ __global__ void __launch_bounds__(256) sweep_cumulants_kernel(CumArgs a) {
             t_lo = min(t_lo, bs[b]);
             t_hi = max(t_hi, be[b]);
         }
-    for (int t = t_lo; t < t_hi; ++t) {
-        const float c = __ldg(a.cg + (long)t * a.P + pix);
-        const float v = __ldg(a.v + (long)t * a.P + pix);
+    // one frame's CGLH and intensity into the sums of every (sensitivity, block) slot
+    auto frame = [&](int t, float c, float v) {
         const double vd = (double)v;
 #pragma unroll
         for (int s = 0; s < kSG; ++s) {
@@ -111,7 +110,22 @@ __global__ void __launch_bounds__(256) sweep_cumulants_kernel(CumArgs a) {
                 prev[s] = x;
             }
         }
+    };
+    // the planes are read once, straight from HBM: the loads of kU frames are issued before their
+    // arithmetic, so that enough of them are in flight (frames still summed in order)
+    constexpr int kU = 8;
+    int t = t_lo;
+    for (; t + kU <= t_hi; t += kU) {
+        float cu[kU], vu[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            cu[u] = __ldg(a.cg + (long)(t + u) * a.P + pix);
+            vu[u] = __ldg(a.v + (long)(t + u) * a.P + pix);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) frame(t + u, cu[u], vu[u]);
     }
+    for (; t < t_hi; ++t) frame(t, __ldg(a.cg + (long)t * a.P + pix), __ldg(a.v + (long)t * a.P + pix));
 #pragma unroll
     for (int s = 0; s < kSG; ++s) {
         if (s >= a.ns) continue;
